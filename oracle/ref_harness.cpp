@@ -1,0 +1,271 @@
+// ref_harness.cpp -- extern "C" driver of the reference SCDAT classes (TEST INFRASTRUCTURE).
+//
+// Compiled by oracle/Makefile together with the reference's own sources (read in place
+// from the reference tree) into oracle/_ref/libscdat_ref.so.  It builds identical mesh and
+// particle state from flat arrays and runs the reference code paths:
+//   CrossTetrahedron::crossTetrahedron          Tools/Particle/include/PICParticleAlgorithms.h:216-219
+//   PoissonSolver::solve(DIRECT)                Tools/FieldSolver/include/PoissonSolver.h:26-67
+//   PICCycle::setPotential (nodal LSQ field)    Tools/PICcore/include/PICCycle.h:105-120
+//   PICCycle::executeTimeStep                   Tools/PICcore/src/PICCycle.cpp:311-416
+//   Collision::executeBackgroundMccStep         Tools/Interactions/Collisions/include/CollisionPicAdapter.h:64-75
+// Only the parity tests and the CPU reference arm of the benchmark load it.
+#include "PICcore/include/PICCycle.h"
+#include "Mesh/include/MeshParsing.h"
+#include "Particle/include/ParticleManager.h"
+#include "Interactions/Collisions/include/CollisionPicAdapter.h"
+
+#include <chrono>
+#include <cstdint>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+using SCDAT::Geometry::Point3D;
+using SCDAT::Geometry::Vector3D;
+namespace SM = SCDAT::Mesh;
+namespace SP = SCDAT::Particle;
+
+namespace {
+
+struct RefMesh {
+    std::shared_ptr<SM::VolMesh> mesh;
+    std::vector<uint8_t> dirichlet;
+};
+
+SP::Particle make_particle(std::size_t id, int kind, const double* x, const double* v, double w)
+{
+    Point3D p(x[0], x[1], x[2]);
+    Vector3D u(v[0], v[1], v[2]);
+    if (kind == 0) return SP::ParticleFactory::createElectron(id, p, u, w);
+    return SP::ParticleFactory::createIon(id, p, u, 1, 1, w);
+}
+
+}  // namespace
+
+extern "C" {
+
+// Mesh from flat arrays.  nbr4 (nullable): per-tet neighbour list added through the
+// public Element::addNeighbor in row order, -1 skipped.  node_bc: 1 = Dirichlet.
+void* ref_mesh_create(int64_t N, const double* xyz, int64_t T, const int32_t* tet4, const int32_t* nbr4,
+                      const uint8_t* node_bc)
+{
+    auto* rm = new RefMesh();
+    rm->mesh = std::make_shared<SM::VolMesh>();
+    for (int64_t i = 0; i < N; ++i) rm->mesh->addNode(Point3D(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]));
+    for (int64_t t = 0; t < T; ++t) {
+        std::vector<std::size_t> ids = {(std::size_t)tet4[4 * t], (std::size_t)tet4[4 * t + 1],
+                                        (std::size_t)tet4[4 * t + 2], (std::size_t)tet4[4 * t + 3]};
+        rm->mesh->addElement(SM::ElementType::TETRAHEDRON, ids);
+    }
+    const auto& els = rm->mesh->getElements();
+    if (nbr4) {
+        for (int64_t t = 0; t < T; ++t)
+            for (int f = 0; f < 4; ++f)
+                if (nbr4[4 * t + f] >= 0) els[t]->addNeighbor(els[nbr4[4 * t + f]]);
+    }
+    rm->dirichlet.assign(node_bc, node_bc + N);
+    const auto& nodes = rm->mesh->getNodes();
+    for (int64_t i = 0; i < N; ++i)
+        nodes[i]->setBoundaryType(node_bc[i] ? SM::BoundaryType::DIRICHLET : SM::BoundaryType::INTERIOR);
+    return rm;
+}
+
+void ref_mesh_destroy(void* h) { delete static_cast<RefMesh*>(h); }
+
+// CrossTetrahedron over every particle with a frozen nodal E field.  kind[p]: 0 electron,
+// 1 H+ ion.  tet: in = hint (-1 none), out = final element.  rho accumulates.
+int ref_push(void* h, const double* Enode, int64_t P, double* x, double* v, const int32_t* kind, const double* w,
+             int32_t* tet, uint8_t* lost, double dt, int nseg, int kernel, double* rho, int64_t* substeps)
+{
+    auto* rm = static_cast<RefMesh*>(h);
+    const auto& nodes = rm->mesh->getNodes();
+    const auto& els = rm->mesh->getElements();
+    const std::size_t N = nodes.size();
+    std::vector<Vector3D> E(N), B(N, Vector3D(0, 0, 0));
+    for (std::size_t i = 0; i < N; ++i) E[i] = Vector3D(Enode[3 * i], Enode[3 * i + 1], Enode[3 * i + 2]);
+    auto interp = std::make_shared<SP::FieldInterpolator>();
+    interp->setMesh(nodes, els);
+    interp->setElectricField(E);
+    interp->setMagneticField(B);
+    auto dep = std::make_shared<SP::ChargeDepositor>();
+    dep->setMesh(nodes, els);
+    dep->setTrajectoryDepositionScheme(static_cast<SP::TrajectoryChargeDepositionKernel>(kernel),
+                                       static_cast<std::size_t>(nseg));
+    SP::CrossTetrahedron ct;
+    ct.setMesh(nodes, els);
+    ct.setFieldInterpolator(interp);
+    ct.setChargeDepositor(dep);
+    std::vector<double> rhov(rho, rho + N);
+    for (int64_t i = 0; i < P; ++i) {
+        SP::Particle p = make_particle((std::size_t)i + 1, kind[i], x + 3 * i, v + 3 * i, w[i]);
+        SP::ElementId hint = tet[i] < 0 ? static_cast<SP::ElementId>(-1) : (SP::ElementId)tet[i];
+        auto r = ct.crossTetrahedron(&p, dt, rhov, true, hint);
+        x[3 * i] = r.final_position.x(); x[3 * i + 1] = r.final_position.y(); x[3 * i + 2] = r.final_position.z();
+        v[3 * i] = r.final_velocity.x(); v[3 * i + 1] = r.final_velocity.y(); v[3 * i + 2] = r.final_velocity.z();
+        tet[i] = (int32_t)r.final_element;
+        lost[i] = r.lost_particle ? 1 : 0;
+    }
+    std::memcpy(rho, rhov.data(), sizeof(double) * N);
+    if (substeps) *substeps = ct.getStatistics().total_crossings;
+    return 0;
+}
+
+// A fresh PoissonSolver: Dirichlet nodes take phi[i], nodal charge rho; DIRECT solve.
+// phi out = node potentials, E out = node fields (PoissonSolver.cpp:387-401,452-529).
+int ref_poisson(void* h, const double* rho, double* phi, double* E)
+{
+    auto* rm = static_cast<RefMesh*>(h);
+    const auto& nodes = rm->mesh->getNodes();
+    SCDAT::FieldSolver::PoissonSolver solver(rm->mesh);
+    for (std::size_t i = 0; i < nodes.size(); ++i) {
+        solver.setChargeDensity(nodes[i]->getId(), rho[i]);
+        if (rm->dirichlet[i])
+            solver.addBoundaryCondition(nodes[i]->getId(),
+                                        std::make_shared<SCDAT::FieldSolver::BoundaryCondition>(
+                                            SCDAT::FieldSolver::BoundaryConditionType::DIRICHLET, phi[i]));
+    }
+    if (!solver.solve(SCDAT::Solver::SolverType::DIRECT)) return 1;
+    for (std::size_t i = 0; i < nodes.size(); ++i) {
+        phi[i] = nodes[i]->getPotential();
+        const auto& e = nodes[i]->getElectricField();
+        E[3 * i] = e.x(); E[3 * i + 1] = e.y(); E[3 * i + 2] = e.z();
+    }
+    return 0;
+}
+
+// Run nsteps of PICCycle::executeTimeStep (fresh PoissonSolver per step so the system is
+// re-assembled, see PoissonSolver.cpp:387-392) and optionally the background MCC step.
+// face_bc[6]: 0 none, 1 absorbing(1.0), 2 periodic over the x and y box lengths.
+// Particles come back in container order with their ids (1-based insertion order).
+int ref_cycle_run(void* h, int64_t P, double* x, double* v, const int32_t* kind, const double* w,
+                  const int32_t* hint, int nsteps, double dt, const int32_t* face_bc, const double* phi0,
+                  int64_t* P_out, int64_t* id_out, int32_t* status_out, double* rho_out, double* phi_out,
+                  double* E_out, double* ledger_out, double* stats_out, double* seconds_out)
+{
+    auto* rm = static_cast<RefMesh*>(h);
+    const auto& nodes = rm->mesh->getNodes();
+    const std::size_t N = nodes.size();
+    auto pm = std::make_shared<SP::ParticleManager>((std::size_t)P + 16);
+    std::vector<std::size_t> ids(P);
+    for (int64_t i = 0; i < P; ++i) {
+        Point3D p(x[3 * i], x[3 * i + 1], x[3 * i + 2]);
+        Vector3D u(v[3 * i], v[3 * i + 1], v[3 * i + 2]);
+        ids[i] = kind[i] == 0 ? pm->createElectron(p, u, w[i]) : pm->createIon(p, u, 1, 1, w[i]);
+    }
+    SCDAT::PICcore::PICCycle::Parameters prm;
+    prm.time_step = dt;
+    prm.max_iterations = 1 << 30;
+    prm.verbose = false;
+    SCDAT::PICcore::PICCycle cycle(prm);
+    cycle.setMesh(nodes, rm->mesh->getElements());
+    cycle.setParticleManager(pm);
+    cycle.setPoissonSolver(std::make_shared<SCDAT::FieldSolver::PoissonSolver>(rm->mesh));
+    using BF = SCDAT::PICcore::PICCycle::BoundaryFace;
+    const Point3D lo = rm->mesh->getBoundingBoxMin(), hi = rm->mesh->getBoundingBoxMax();
+    auto periodic = std::make_shared<SP::PeriodicBoundaryCondition>(
+        std::vector<Vector3D>{Vector3D(hi.x() - lo.x(), 0, 0), Vector3D(0, hi.y() - lo.y(), 0)});
+    for (int f = 0; f < 6; ++f) {
+        if (face_bc[f] == 1) cycle.setBoundaryCondition((BF)f, std::make_shared<SP::AbsorbingBoundaryCondition>(1.0));
+        else if (face_bc[f] == 2) cycle.setBoundaryCondition((BF)f, periodic);
+    }
+    if (!cycle.initialize()) return 1;
+    std::vector<double> phi(phi0, phi0 + N);
+    cycle.setPotential(phi);
+    for (int64_t i = 0; i < P; ++i)
+        if (hint[i] >= 0) cycle.addParticleLocation(pm->getParticle(ids[i]), (SP::ElementId)hint[i]);
+    auto t0 = std::chrono::steady_clock::now();
+    for (int s = 0; s < nsteps; ++s) {
+        cycle.setPoissonSolver(std::make_shared<SCDAT::FieldSolver::PoissonSolver>(rm->mesh));
+        if (!cycle.executeTimeStep()) return 2;
+    }
+    auto t1 = std::chrono::steady_clock::now();
+    if (seconds_out) *seconds_out = std::chrono::duration<double>(t1 - t0).count();
+    auto& cont = pm->getContainer();
+    int64_t k = 0;
+    for (auto& p : cont) {
+        const auto pos = p.getPosition();
+        const auto vel = p.getVelocity();
+        x[3 * k] = pos.x(); x[3 * k + 1] = pos.y(); x[3 * k + 2] = pos.z();
+        v[3 * k] = vel.x(); v[3 * k + 1] = vel.y(); v[3 * k + 2] = vel.z();
+        id_out[k] = (int64_t)p.getId();
+        status_out[k] = (int32_t)p.getStatus();
+        ++k;
+    }
+    *P_out = k;
+    const auto& rho = cycle.getChargeDensity();
+    const auto& ph = cycle.getPotential();
+    const auto& E = cycle.getElectricField();
+    for (std::size_t i = 0; i < N; ++i) {
+        rho_out[i] = rho[i];
+        phi_out[i] = ph[i];
+        E_out[3 * i] = E[i].x(); E_out[3 * i + 1] = E[i].y(); E_out[3 * i + 2] = E[i].z();
+    }
+    const auto& led = cycle.getSurfaceCurrentLedger();
+    for (int f = 0; f < 6; ++f) {
+        double* r = ledger_out + 8 * f;
+        r[0] = led[f].absorbed_electron_charge_c;
+        r[1] = led[f].absorbed_ion_charge_c;
+        r[2] = led[f].emitted_electron_charge_c;
+        r[3] = led[f].incident_energy_j;
+        r[4] = (double)led[f].absorbed_electron_particles;
+        r[5] = (double)led[f].absorbed_ion_particles;
+        r[6] = (double)led[f].emitted_electron_particles;
+        r[7] = 0.0;
+    }
+    const auto& st = cycle.getStatistics();
+    stats_out[0] = st.completed_steps;
+    stats_out[1] = st.total_charge;
+    stats_out[2] = st.total_energy;
+    stats_out[3] = st.active_particles;
+    stats_out[4] = st.surface_deposited_charge;
+    return 0;
+}
+
+// PICCycle::setPotential -> updateElectricField (LSQ with 1e-18 regularisation).
+int ref_lsq_field(void* h, const double* phi, double* E)
+{
+    auto* rm = static_cast<RefMesh*>(h);
+    const auto& nodes = rm->mesh->getNodes();
+    const std::size_t N = nodes.size();
+    auto pm = std::make_shared<SP::ParticleManager>(16);
+    SCDAT::PICcore::PICCycle cycle;
+    cycle.setMesh(nodes, rm->mesh->getElements());
+    cycle.setParticleManager(pm);
+    cycle.setPoissonSolver(std::make_shared<SCDAT::FieldSolver::PoissonSolver>(rm->mesh));
+    if (!cycle.initialize()) return 1;
+    cycle.setPotential(std::vector<double>(phi, phi + N));
+    const auto& e = cycle.getElectricField();
+    for (std::size_t i = 0; i < N; ++i) { E[3 * i] = e[i].x(); E[3 * i + 1] = e[i].y(); E[3 * i + 2] = e[i].z(); }
+    return 0;
+}
+
+// Background MCC with one constant elastic process per species (sigma, n_target), run
+// `repeats` times on copies of the same P particles; returns the total collision count
+// (reference two-draw form, CollisionAlgorithm.cpp:500-538).
+int64_t ref_mcc_count(int64_t P, const double* v, int kind, double w, double sigma, double n_target, double dt,
+                      unsigned seed, int repeats)
+{
+    using namespace SCDAT::Collision;
+    MonteCarloCollisionHandler handler(seed);
+    handler.clearCollisionProcesses();
+    CollisionParameters prm;
+    prm.energy_threshold = 0.0;
+    prm.cross_section_max = sigma;
+    prm.additional_params["reference_energy"] = 1.0;
+    prm.additional_params["power_index"] = 0.0;
+    handler.addCollisionProcess(
+        "elastic", CollisionProcessFactory::createElasticProcess(kind == 0 ? ParticleSpecies::ELECTRON : ParticleSpecies::ION,
+                                                                 ParticleSpecies::NEUTRAL, n_target, prm));
+    int64_t total = 0;
+    for (int r = 0; r < repeats; ++r) {
+        std::vector<ParticleObject> ps;
+        ps.reserve(P);
+        double z[3] = {0, 0, 0};
+        for (int64_t i = 0; i < P; ++i) ps.push_back(make_particle((std::size_t)i + 1, kind, z, v + 3 * i, w));
+        handler.processCollisions(ps, dt);
+    }
+    total = (int64_t)handler.getStatistics().total_collisions;
+    return total;
+}
+
+}  // extern "C"
