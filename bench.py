@@ -1,0 +1,386 @@
+"""Benchmark: PIC particle-steps/s of the B200 PIC-MCC step (push + deposit + boundary +
+MCC + Poisson solve + nodal field) on a synthetic Kuhn-box plasma, through the C ABI.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config NAME]
+
+Workloads (all synthetic, seeded; the reference publishes no dataset):
+  precision128  128^3 hex cells x 6 tets (12.6M tets), h = 1.6 m / 128, central 32^3-cell
+                conducting body at -10 V, outer faces 0 V, electrons + H+ at n = 1e10 m^-3,
+                Te = Ti = 1 eV, 64 particles per cell per species (~268M), dt = 2e-8 s,
+                FP32 cell-relative push, fixed-point deposit, FP32-SpMV PCG under FP64
+                refinement to 1e-10, elastic MCC (sigma 1e-19 m^2, n_n 1e14 m^-3)   [default]
+  plain32       32^3 cells, h = 0.05 m, 8^3-cell body, 20 ppc, FP64, Jacobi-PCG to 1e-8
+Every rank runs an independent replica ("replicas only": the path has no exchange step).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+QE, ME, MP = 1.602176634e-19, 9.1093837015e-31, 1.67262192369e-27
+
+CONFIGS = {
+    "precision128": dict(n=128, L=1.6, body=(48, 80), bias=-10.0, ppc=64, dt=2e-8, precision=1, rtol=1e-10,
+                         density=1e10, te=1.0, ti=1.0, sort_interval=4),
+    "plain32": dict(n=32, L=1.6, body=(12, 20), bias=-10.0, ppc=20, dt=2e-8, precision=0, rtol=1e-8, density=1e10,
+                    te=1.0, ti=1.0, sort_interval=8),
+}
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax.append(float(parts[1]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[4:8]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def build_domain(cfg, precision, capi):
+    n = cfg["n"]
+    h = cfg["L"] / n
+    body = ((cfg["body"][0], cfg["body"][1]),) * 3 if cfg["body"] else None
+    m = capi.kuhn_box_mesh((n, n, n), h, body=body, bias=cfg["bias"], wall=0.0)
+    dom = capi.Domain(m["xyz"], m["tet"], m["dirichlet"], cfg["dt"], precision=precision, face_bc=(1,) * 6,
+                      pcg_rtol=cfg["rtol"], pcg_max_iter=20000, sort_interval=cfg["sort_interval"])
+
+    class Sp:
+        def __init__(self, q, mass, w):
+            self.q, self.m, self.w = q, mass, w
+
+    w = cfg["density"] * h ** 3 / cfg["ppc"]
+    dom.set_species([Sp(-QE, ME, w), Sp(QE, MP, w)])
+    dom.seed_box(0, (n, n, n), h, body, cfg["ppc"], cfg["te"], 12345)
+    dom.seed_box(1, (n, n, n), h, body, cfg["ppc"], cfg["ti"], 12345)
+    for s in range(2):
+        dom.set_elastic(s, 1e14, 1e-19, mode=1)
+    dom.set_potential(m["phi"])
+    dom.solve_field(allow_not_converged=True)
+    return dom, m
+
+
+def alg_bytes_push(dom, precision, particles):
+    """Algorithmic bytes of one push launch (all species of a step): particle state read and
+    written once (+ the 4-byte id the fused MCC reads), the mesh read once, node E read once
+    and the fixed-point accumulators read-modify-written once."""
+    b_p = 60 if precision == 1 else 108
+    t_b = 16 + (36 if precision == 1 else 96)
+    n_b = (12 if precision == 1 else 24) + 2 * 16 * dom.nspecies
+    return particles * b_p + dom.T * t_b + dom.N * n_b
+
+
+def run_ours(args, cfg):
+    import torch
+
+    from scdat_b200 import build, capi
+
+    build.build()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    prec = cfg["precision"]
+    dom, mesh = build_domain(cfg, prec, capi)
+    stream = torch.cuda.ExternalStream(dom.stream())
+    for _ in range(args.warmup):
+        dom.step(1)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    dom.set_timing(True)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    psteps = 0
+    pcg_iters = []
+    for _ in range(args.steps):
+        before = sum(dom.count(s) for s in range(dom.nspecies))
+        dom.step(1)
+        st = dom.stats()
+        psteps += st["active_particles"]
+        pcg_iters.append(st["last_pcg_iterations"])
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    tm = dom.timing()
+    clk = clocks.stop()
+    t_local = ms / 1e3
+    if dist:
+        t = torch.tensor([t_local, float(psteps)], device="cuda", dtype=torch.float64)
+        tmax = t.clone()
+        dist.all_reduce(tmax[:1], op=dist.ReduceOp.MAX)
+        dist.all_reduce(t[1:], op=dist.ReduceOp.SUM)
+        t_max, total_psteps = float(tmax[0]), float(t[1])
+    else:
+        t_max, total_psteps = t_local, float(psteps)
+    value = total_psteps / t_max
+    # roofline of the dominant kernel (the push), timed with events on the library stream
+    push_ms = tm["push_ms"] / max(tm["push_launches"], 1)
+    parts_per_launch = tm["push_particles"] / max(tm["push_launches"], 1)
+    bytes_push = alg_bytes_push(dom, prec, parts_per_launch)
+    peak, peak_kind = load_peaks()
+    achieved = bytes_push / (push_ms / 1e3) / 1e9
+    traffic = None
+    tr_file = os.path.join(ROOT, "profiles", "push_traffic.json")
+    if os.path.exists(tr_file):
+        d = json.load(open(tr_file))
+        key = "mixed" if prec == 1 else "fp64"
+        if key in d:
+            traffic = d[key]["dram_bytes_per_particle"] * parts_per_launch
+    # end-to-end through the C ABI with host buffers: per step, Dirichlet potentials in from
+    # pinned host memory, then the ledger, statistics and the nodal potential back
+    dir_nodes = np.nonzero(mesh["dirichlet"])[0].astype(np.int64)
+    h_nodes = torch.from_numpy(dir_nodes).pin_memory()
+    h_vals = torch.from_numpy(mesh["phi"][dir_nodes].copy()).pin_memory()
+    h_phi = torch.empty(dom.N, dtype=torch.float64).pin_memory()
+    e2e_steps = max(1, min(args.steps, 3))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e2e_ps = 0
+    for _ in range(e2e_steps):
+        dom.L.scdat_set_node_potentials(dom.h, len(dir_nodes), h_nodes.data_ptr(), h_vals.data_ptr())
+        dom.step(1)
+        led = dom.ledger()
+        st = dom.stats()
+        dom.L.scdat_get_fields(dom.h, None, h_phi.data_ptr(), None)
+        e2e_ps += st["active_particles"]
+    t1 = time.perf_counter()
+    e2e_val = e2e_ps / (t1 - t0)
+    h2d = len(dir_nodes) * 16
+    d2h = dom.N * 8 + 7 * 8 * 8 + 120
+    out = {
+        "metric": "PIC particle-steps/s on 1 B200 (mixed/batched vs plain FP64 at equal error)",
+        "value": value,
+        "unit": "particle-steps/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": t_max * 1e3 / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32" if prec == 1 else "f64",
+        "data": "synthetic (seeded Kuhn-box plasma, no dataset)",
+        "config": {"workload": args.config, "cells": cfg["n"] ** 3, "tets": dom.T, "nodes": dom.N,
+                   "particles": int(sum(dom.count(s) for s in range(dom.nspecies))), "ppc_per_species": cfg["ppc"],
+                   "precision": "mixed" if prec == 1 else "fp64", "pcg_rtol": cfg["rtol"],
+                   "pcg_iterations_per_step": pcg_iters, "l2": "inputs larger than L2 (particle state > 126 MB)",
+                   "parallelism": f"replicas x{world}"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "peak_kind": peak_kind, "kernel": "push (gather+boris+relocate+deposit+mcc)",
+                     "alg_bytes_per_launch": bytes_push, "launch_ms": push_ms},
+        "stage_ms_per_step": {"push": tm["push_ms"] / args.steps, "field": tm["field_ms"] / args.steps},
+        "gpu_launches": int(tm["kernel_launches"]),
+        "clocks": clk,
+        "e2e": {"value": e2e_val, "unit": "particle-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+    }
+    dom.close()
+    if rank == 0 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(cfg, args)
+    if rank == 0 and args.fp64_compare and prec == 1:
+        out["fp64_form"] = fp64_compare(cfg, args)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out))
+
+
+def fp64_compare(cfg, args):
+    """The plain FP64 form on the same workload (the 1x of the mixed-form speed-up)."""
+    import torch
+
+    from scdat_b200 import capi
+
+    c = dict(cfg)
+    dom, _ = build_domain(c, 0, capi)
+    stream = torch.cuda.ExternalStream(dom.stream())
+    for _ in range(max(1, args.warmup)):
+        dom.step(1)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    ps = 0
+    k = max(1, min(args.steps, 3))
+    for _ in range(k):
+        dom.step(1)
+        ps += dom.stats()["active_particles"]
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    dom.close()
+    return {"value": ps / (ms / 1e3), "unit": "particle-steps/s", "steps": k, "ms_per_step": ms / k}
+
+
+def reference_sample(cfg):
+    """The reference particle path on a bounded sample of the workload: a 16^3-cell box of the
+    same cell size, plasma and particles per cell, a 4^3-cell body at the same bias."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    n = 16
+    h = cfg["L"] / cfg["n"]
+    q = n // 4
+    mesh = O.kuhn_box((n, n, n), h, body=((6, 6 + q), (6, 6 + q), (6, 6 + q)), bias=cfg["bias"])
+    sp = O.plasma_species(cfg["density"], cfg["te"], cfg["ti"], h, cfg["ppc"])
+    parts = O.seed_particles(mesh, sp, cfg["ppc"], 7)
+    o = O.Oracle()
+    A = o.assemble(mesh)
+    phi, _, _ = o.poisson(mesh, A, np.zeros(mesh.N), mesh.phi_bc, rtol=1e-10)
+    E = o.lsq(mesh, A, phi)
+    return O, mesh, sp, parts, E
+
+
+def cpu_baseline(cfg, args):
+    O, mesh, sp, parts, E = reference_sample(cfg)
+    P = parts["x"].shape[0]
+    if O.reference_available(omp=True):
+        ref = O.Reference(omp=True)
+        total, steps, nt = 0.0, 0, 1
+        cur = parts
+        while total < 10.0 and steps < 20:
+            out, secs, nt = ref.push_parallel(mesh, E, cur, sp, cfg["dt"])
+            cur = dict(parts, x=out["x"], v=out["v"], tet=np.where(out["lost"] == 1, -1, out["tet"]))
+            total += secs
+            steps += 1
+        ref.close()
+        kind, sample = "reference", (f"reference CrossTetrahedron push+deposit (OpenMP branch structure, {nt} threads) "
+                                     f"of {P} particles x {steps} steps on a 16^3-cell box at the workload's cell size, "
+                                     f"plasma and ppc; field solve excluded (dense reference solve infeasible)")
+    else:
+        o = O.Oracle()
+        t0 = time.perf_counter()
+        steps = 0
+        cur = parts
+        while time.perf_counter() - t0 < 10.0 and steps < 20:
+            out = o.push(mesh, E, cur, sp, cfg["dt"])
+            cur = dict(parts, x=out["x"], v=out["v"], tet=np.where(out["lost"] == 1, -1, out["tet"]))
+            steps += 1
+        total = time.perf_counter() - t0
+        nt = 1
+        kind, sample = "port", (f"C oracle push+deposit (1 thread) of {P} particles x {steps} steps on a 16^3-cell "
+                                f"box at the workload's cell size, plasma and ppc; field solve excluded")
+    return {"value": P * steps / total, "unit": "particle-steps/s", "cores": nt, "kind": kind, "sample": sample}
+
+
+def run_reference(args, cfg):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    cb = cpu_baseline(cfg, args)
+    out = {
+        "impl": "reference",
+        "metric": "PIC particle-steps/s on 1 B200 (mixed/batched vs plain FP64 at equal error)",
+        "value": cb["value"],
+        "unit": "particle-steps/s",
+        "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded Kuhn-box plasma, no dataset)",
+        "config": {"workload": args.config, "sample": cb["sample"]},
+        "cpu_baseline": cb,
+        "e2e": {"value": cb["value"], "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="precision128", choices=sorted(CONFIGS))
+    ap.add_argument("--n", type=int, default=0, help="override the number of cells per edge")
+    ap.add_argument("--ppc", type=int, default=0, help="override particles per cell per species")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64-compare", dest="fp64_compare", action="store_false")
+    args = ap.parse_args()
+    cfg = dict(CONFIGS[args.config])
+    if args.n:
+        f = args.n / cfg["n"]
+        cfg["body"] = (int(cfg["body"][0] * f), int(cfg["body"][1] * f))
+        cfg["n"] = args.n
+    if args.ppc:
+        cfg["ppc"] = args.ppc
+    if args.impl == "reference":
+        run_reference(args, cfg)
+    else:
+        run_ours(args, cfg)
+
+
+if __name__ == "__main__":
+    main()

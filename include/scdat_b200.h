@@ -1,0 +1,233 @@
+/*
+ * scdat_b200.h -- C ABI of the B200 PIC-MCC step and its per-step Poisson solve.
+ *
+ * Plain pointers and sizes only; every call returns SCDAT_OK (0) or a negative
+ * scdat_status, and scdat_last_error() gives a one-line reason.  No exception crosses
+ * the ABI.  Host arrays are read or written synchronously unless the name says "async".
+ *
+ * Each entry point cites the reference interface it replaces (paths inside the SCDAT
+ * tree).  The reference keeps this state in PICCycle (Tools/PICcore/include/PICCycle.h),
+ * its helpers CrossTetrahedron / FieldInterpolator / ChargeDepositor
+ * (Tools/Particle/include/PICParticleAlgorithms.h), PoissonSolver
+ * (Tools/FieldSolver/include/PoissonSolver.h) and the background MCC handler
+ * (Tools/Interactions/Collisions/include/CollisionAlgorithm.h, CollisionPicAdapter.h).
+ */
+#ifndef SCDAT_B200_H
+#define SCDAT_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SCDAT_API __attribute__((visibility("default")))
+
+typedef enum {
+    SCDAT_OK = 0,
+    SCDAT_ERR_ARG = -1,        /* bad argument (null pointer, out-of-range index, size)   */
+    SCDAT_ERR_CUDA = -2,       /* a CUDA call failed; scdat_last_error() has the message   */
+    SCDAT_ERR_STATE = -3,      /* call out of order (e.g. step before species are set)      */
+    SCDAT_ERR_CAPACITY = -4,   /* particle capacity exceeded                                */
+    SCDAT_ERR_NOT_CONVERGED = -5, /* field solve hit its iteration cap (result kept)       */
+    SCDAT_ERR_DEVICE_FLAG = -6 /* a kernel reported an error through the device flag word   */
+} scdat_status;
+
+typedef enum { SCDAT_PREC_FP64 = 0, SCDAT_PREC_MIXED = 1 } scdat_precision;
+
+/* TrajectoryChargeDepositionKernel, Tools/Particle/include/PICParticleAlgorithms.h:32-37 */
+typedef enum { SCDAT_DEP_NEAREST = 0, SCDAT_DEP_LINEAR = 1, SCDAT_DEP_GAUSS3 = 2 } scdat_deposit_kernel;
+
+/* Particle boundary condition per box face, PICCycle::setBoundaryCondition
+ * (PICCycle.h:68) with AbsorbingBoundaryCondition(1.0) / PeriodicBoundaryCondition
+ * (Tools/Boundary/include/BoundaryConditions.h). */
+typedef enum { SCDAT_BC_NONE = 0, SCDAT_BC_ABSORB = 1, SCDAT_BC_PERIODIC = 2 } scdat_face_bc;
+
+/* Particle status as stored on the device (ParticleStatus ACTIVE/ABSORBED/ESCAPED,
+ * Tools/Particle/include/ParticleDefinitions.h:161-176). */
+typedef enum { SCDAT_ACTIVE = 0, SCDAT_ABSORBED = 1, SCDAT_ESCAPED = 2 } scdat_particle_status;
+
+/* Mesh: nodes and 4-node tets, as VolMesh::addNode/addElement build them
+ * (Tools/Mesh/include/MeshParsing.h:152-155).  tet_neighbors (nullable) is the per-tet
+ * neighbour list Element::addNeighbor fills (MeshAlgorithms.h:193): the tet across the face
+ * opposite local vertex f, -1 on the boundary.  When NULL the library derives it.
+ * node_dirichlet marks Mesh::BoundaryType::DIRICHLET nodes.  tet_eps_rel (nullable): relative
+ * permittivity per tet (PoissonSolver.cpp:21-29,655-662; NULL = vacuum everywhere). */
+typedef struct {
+    int64_t n_nodes;
+    int64_t n_tets;
+    const double* node_xyz;        /* [n_nodes*3] */
+    const int32_t* tet_nodes;      /* [n_tets*4] */
+    const int32_t* tet_neighbors;  /* [n_tets*4] or NULL */
+    const uint8_t* node_dirichlet; /* [n_nodes] 1 = Dirichlet */
+    const double* tet_eps_rel;     /* [n_tets] or NULL */
+} scdat_mesh_desc;
+
+/* PICCycle::Parameters (PICCycle.h:46-58) plus the device-side choices. */
+typedef struct {
+    double dt;                    /* time_step [s] */
+    int32_t deposit_kernel;       /* scdat_deposit_kernel, default LINEAR */
+    int32_t deposit_segments;     /* trajectory_charge_deposition_segments, default 10 */
+    double adaptive_floor_ratio;  /* PIC_ADAPTIVE_FLOOR_RATIO, default 0.001 */
+    int32_t precision;            /* scdat_precision */
+    int32_t use_neighbor_lists;   /* 1: locate tries the hint's neighbour list first */
+    int32_t face_bc[6];           /* scdat_face_bc per XMin,XMax,YMin,YMax,ZMin,ZMax */
+    int32_t body_tally;           /* 1: particles lost into an interior hole go to ledger row 6 */
+    int32_t poisson_charge_sign;  /* -1: b = -rho*V/4 as PoissonSolver.cpp:356; +1: physical */
+    double pcg_rtol;              /* relative residual target of the field solve */
+    int32_t pcg_max_iter;         /* iteration cap per solve */
+    int32_t sort_interval;        /* re-sort particles by tet every N steps (0 = never) */
+    int64_t particle_capacity;    /* total device particle slots over all species */
+    uint64_t seed;                /* Philox key for MCC */
+} scdat_params;
+
+/* One species: charge [C], mass [kg], macro weight, and whether it is electron-like for the
+ * ledger (PICCycle.cpp:52-85). */
+typedef struct {
+    double charge;
+    double mass;
+    double weight;
+    int32_t electron_like;
+    int32_t pad;
+} scdat_species;
+
+/* Elastic background collision for one species: ElasticCollisionCrossSection
+ * (Tools/Interactions/Collisions/src/CollisonTypes.cpp:60-78) against a neutral background.
+ * mode 0: the reference two-draw test (CollisionAlgorithm.cpp:525-531 then :195-200);
+ * mode 1: one draw against 1-exp(-nu*dt). */
+typedef struct {
+    double target_density;  /* m^-3 */
+    double sigma_max;       /* m^2 */
+    double e_ref_ev;        /* reference_energy */
+    double alpha;           /* power_index (0 = constant cross-section) */
+    double e_threshold_ev;
+    int32_t enabled;
+    int32_t mode;
+} scdat_elastic;
+
+/* PICCycle::CycleStatistics (PICCycle.h:135-144) plus device counters. */
+typedef struct {
+    int64_t completed_steps;
+    double simulation_time;
+    double total_charge;             /* computeTotalCharge, PICParticleAlgorithms.cpp:440-448 */
+    double total_energy;             /* updateStatistics, PICCycle.cpp:941-966 */
+    int64_t active_particles;        /* active particles after the step */
+    int64_t stored_particles;        /* particles held (active + not yet compacted) */
+    double surface_deposited_charge; /* PICCycle.cpp:1271 */
+    int64_t substeps;                /* CrossTetrahedron::Statistics::total_crossings */
+    int64_t lost_events;
+    int64_t mcc_collisions;
+    int32_t last_pcg_iterations;
+    int32_t pad;
+    double last_pcg_relres;
+} scdat_stats;
+
+typedef struct scdat_ctx scdat_ctx;
+
+/* Defaults for scdat_params (dt must still be set). */
+SCDAT_API void scdat_default_params(scdat_params* p);
+
+/* PICCycle::setMesh + initialize (PICCycle.h:64-75, PICCycle.cpp:227-309) and the
+ * PoissonSolver assembly (PoissonSolver.cpp:251-385): uploads the mesh, precomputes tet
+ * geometry, the locate grid, the node graph and the Dirichlet-reduced matrix. */
+SCDAT_API int scdat_create(const scdat_mesh_desc* mesh, const scdat_params* params, scdat_ctx** out);
+SCDAT_API int scdat_destroy(scdat_ctx* ctx);
+SCDAT_API const char* scdat_last_error(const scdat_ctx* ctx);
+
+/* ParticleManager species (ParticleFactory::createElectron/createIon,
+ * Tools/Particle/src/ParticleDefinitions.cpp:374-392).  Call once before particles. */
+SCDAT_API int scdat_set_species(scdat_ctx* ctx, int32_t n_species, const scdat_species* sp);
+
+/* ParticleContainer::addParticles (ParticleManager.h:77) for one species.  tet_hint
+ * (nullable) seeds PICCycle::addParticleLocation (PICCycle.h:71); ids (nullable) key the
+ * MCC random streams (default: running index).  Replaces the species' particles. */
+SCDAT_API int scdat_set_particles(scdat_ctx* ctx, int32_t species, int64_t n, const double* x, const double* v,
+                                  const int32_t* tet_hint, const uint32_t* ids);
+
+/* Device-side seeding of a Kuhn box built by scdat_kuhn_box_mesh with the same dimensions:
+ * n_per_cell particles of the species in every meshed hex cell, uniform positions and a
+ * Maxwellian of temperature temp_ev, from Philox(seed) keyed by the particle id
+ * (cell*n_species + species)*n_per_cell + k.  Replaces the species' particles. */
+SCDAT_API int scdat_seed_box_particles(scdat_ctx* ctx, int32_t species, int32_t nx, int32_t ny, int32_t nz,
+                                       double h, const int32_t* body_lo, const int32_t* body_hi,
+                                       int32_t n_per_cell, double temp_ev, uint64_t seed);
+
+/* Builds the 6-tet Kuhn box the benchmark configurations use (the reference box mesher makes
+ * a non-conforming 5-tet split, Tools/Mesh/src/MeshParsing.cpp:1209-1260, so this replaces it
+ * for those inputs): nx*ny*nz hex cells of edge h from the origin, node id
+ * i + (nx+1)*(j + (ny+1)*k), hex cells x-fastest minus the half-open body index range
+ * [body_lo, body_hi) (both NULL: no body), 6 tets per cell.  Outer-face nodes are Dirichlet
+ * at `wall`, body nodes at `bias`.  Call with NULL output arrays to get the sizes. */
+SCDAT_API int scdat_kuhn_box_mesh(int32_t nx, int32_t ny, int32_t nz, double h, const int32_t* body_lo,
+                                  const int32_t* body_hi, double bias, double wall, int64_t* n_nodes, int64_t* n_tets,
+                                  double* node_xyz, int32_t* tet_nodes, uint8_t* node_dirichlet, double* node_phi,
+                                  int32_t* hex_ijk, int64_t* n_cells);
+
+/* ParticleContainer iteration (ParticleManager.h:113-126): copy one species back. */
+SCDAT_API int scdat_get_particle_count(scdat_ctx* ctx, int32_t species, int64_t* n);
+SCDAT_API int scdat_get_particles(scdat_ctx* ctx, int32_t species, int64_t capacity, double* x, double* v,
+                                  int32_t* tet, uint8_t* status, uint32_t* ids, int64_t* n_out);
+
+/* PICCycle::setPotential (PICCycle.h:105-120): node potentials (Dirichlet values included)
+ * and the nodal LSQ field recomputed with the 1e-18 regularisation (PICCycle.cpp:180-220). */
+SCDAT_API int scdat_set_potential(scdat_ctx* ctx, const double* phi);
+/* PICCycle::setNodePotential (PICCycle.h:122-133) for a batch of nodes. */
+SCDAT_API int scdat_set_node_potentials(scdat_ctx* ctx, int64_t n, const int64_t* nodes, const double* values);
+/* FieldInterpolator::setElectricField (PICParticleAlgorithms.h:92): freeze a nodal E. */
+SCDAT_API int scdat_set_electric_field(scdat_ctx* ctx, const double* E);
+
+/* MonteCarloCollisionHandler::addCollisionProcess (CollisionAlgorithm.h:176-226) for one
+ * species; executed once per step after the push, like executeBackgroundMccStep
+ * (CollisionPicAdapter.cpp:338-434). */
+SCDAT_API int scdat_set_elastic_mcc(scdat_ctx* ctx, int32_t species, const scdat_elastic* proc);
+
+/* PICCycle::executeTimeStep (PICCycle.cpp:311-416) followed by the background MCC step and
+ * removal of inactive particles, n_steps times, all on the device. */
+SCDAT_API int scdat_step(scdat_ctx* ctx, int32_t n_steps);
+
+/* Stages, for parity tests and callers that drive the cycle themselves:
+ *   scdat_push          -- ChargeDepositor::clearChargeDensity + pushParticles + boundary events
+ *                          (PICCycle.cpp:331, 466-629, 1331-1379) with the current field
+ *   scdat_solve_field   -- solvePoissonEquation + updateElectricField (PICCycle.cpp:645-894)
+ *   scdat_collide       -- executeBackgroundMccStep (CollisionPicAdapter.cpp:338-434)
+ *   scdat_compact       -- ParticleContainer::removeInactiveParticles (ParticleManager.cpp:157-177) */
+SCDAT_API int scdat_push(scdat_ctx* ctx);
+SCDAT_API int scdat_solve_field(scdat_ctx* ctx);
+SCDAT_API int scdat_collide(scdat_ctx* ctx);
+SCDAT_API int scdat_compact(scdat_ctx* ctx);
+
+/* PICCycle::getChargeDensity/getPotential/getElectricField (PICCycle.h:79-90); any pointer
+ * may be NULL.  rho is nodal charge [C]; E is [n_nodes*3]. */
+SCDAT_API int scdat_get_fields(scdat_ctx* ctx, double* rho, double* phi, double* E);
+/* Per-species nodal charge of the last deposit (no reference counterpart: the reference only
+ * keeps the sum). */
+SCDAT_API int scdat_get_species_charge(scdat_ctx* ctx, int32_t species, double* rho_s);
+/* PICCycle::getSurfaceCurrentLedger (PICCycle.h:175-178): 7 rows (XMin..ZMax, interior body)
+ * x 8 columns: absorbed e charge, absorbed ion charge, emitted e charge, incident energy,
+ * absorbed e count, absorbed ion count, emitted e count, 0.  Cumulative since create/reset. */
+SCDAT_API int scdat_get_ledger(scdat_ctx* ctx, double* ledger);
+SCDAT_API int scdat_reset_ledger(scdat_ctx* ctx);
+/* PICCycle::getStatistics (PICCycle.h:165-168). */
+SCDAT_API int scdat_get_statistics(scdat_ctx* ctx, scdat_stats* st);
+
+/* The CUDA stream every call of this context runs on (a cudaStream_t), for callers that
+ * order their own work or events against the library.  No reference counterpart. */
+SCDAT_API void* scdat_stream(scdat_ctx* ctx);
+
+/* Per-stage device timing with CUDA events on the context stream (no reference counterpart;
+ * the reference keeps wall-clock stage shares under PIC_PROFILE_CYCLE, PICCycle.cpp:316-408).
+ * scdat_set_timing(1) clears the counters and starts recording; scdat_get_timing returns the
+ * summed device milliseconds of the particle push launches (all species of a step count as
+ * one launch) and of the field solves since then, and how many kernels of this library were
+ * launched. */
+SCDAT_API int scdat_set_timing(scdat_ctx* ctx, int32_t enable);
+SCDAT_API int scdat_get_timing(scdat_ctx* ctx, double* push_ms, int64_t* push_launches, int64_t* push_particles,
+                               double* field_ms, int64_t* field_solves, int64_t* kernel_launches);
+
+/* Library version string. */
+SCDAT_API const char* scdat_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SCDAT_B200_H */

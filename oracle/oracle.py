@@ -286,6 +286,8 @@ class Oracle:
         L.orc_mcc.argtypes = [C.c_int64, _dp, _i32p, _u8p, _i64p, _dp, C.POINTER(Elastic), C.c_double,
                               C.c_uint64, C.c_uint32, C.c_int]
         L.orc_mcc.restype = C.c_int64
+        L.orc_boris.argtypes = [_dp, _dp, C.c_double, C.c_double, _dp]
+        L.orc_boris.restype = None
 
     # -- RNG
     def philox(self, ctr, key):
@@ -407,11 +409,14 @@ class Reference:
         L.ref_push.argtypes = [C.c_void_p, _dp, C.c_int64, _dp, _dp, _i32p, _dp, _i32p, _u8p, C.c_double, C.c_int,
                                C.c_int, _dp, C.POINTER(C.c_int64)]
         L.ref_poisson.argtypes = [C.c_void_p, _dp, _dp, _dp]
+        L.ref_push_parallel.argtypes = [C.c_void_p, _dp, C.c_int64, _dp, _dp, _i32p, _dp, _i32p, _u8p, C.c_double,
+                                        C.c_int, C.c_int, _dp, C.POINTER(C.c_int)]
+        L.ref_push_parallel.restype = C.c_double
         L.ref_lsq_field.argtypes = [C.c_void_p, _dp, _dp]
         L.ref_cycle_run.argtypes = [C.c_void_p, C.c_int64, _dp, _dp, _i32p, _dp, _i32p, C.c_int, C.c_double, _i32p,
                                     _dp, C.POINTER(C.c_int64), _i64p, _i32p, _dp, _dp, _dp, _dp, _dp, _dp]
         L.ref_mcc_count.argtypes = [C.c_int64, _dp, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
-                                    C.c_uint, C.c_int]
+                                    C.c_uint, C.c_int, C.POINTER(C.c_int64)]
         L.ref_mcc_count.restype = C.c_int64
         self._meshes = {}
 
@@ -441,6 +446,22 @@ class Reference:
         self.L.ref_push(h, np.ascontiguousarray(E, np.float64).reshape(-1), P, x.reshape(-1), v.reshape(-1), kind, w,
                         tet, lost, dt, nseg, kernel, rho, C.byref(sub))
         return dict(x=x, v=v, tet=tet, lost=lost, rho=rho, substeps=sub.value)
+
+    def push_parallel(self, mesh, E, parts, species, dt, nseg=10, kernel=1):
+        """Reference push over all host threads; returns (result dict, seconds, threads)."""
+        h = self.mesh(mesh, True)
+        P = parts["x"].shape[0]
+        x = parts["x"].copy()
+        v = parts["v"].copy()
+        kind = np.array([species[s].kind for s in parts["species"]], np.int32)
+        w = np.array([species[s].w for s in parts["species"]], np.float64)
+        tet = parts["tet"].astype(np.int32).copy()
+        lost = np.zeros(P, np.uint8)
+        rho = np.zeros(mesh.N)
+        nt = C.c_int()
+        secs = self.L.ref_push_parallel(h, np.ascontiguousarray(E, np.float64).reshape(-1), P, x.reshape(-1),
+                                        v.reshape(-1), kind, w, tet, lost, dt, nseg, kernel, rho, C.byref(nt))
+        return dict(x=x, v=v, tet=tet, lost=lost, rho=rho), float(secs), nt.value
 
     def poisson(self, mesh, rho, phi_bc):
         h = self.mesh(mesh)
@@ -480,5 +501,8 @@ class Reference:
                     ledger=ledger.reshape(6, 8), stats=stats, seconds=float(secs[0]))
 
     def mcc_count(self, v, kind, w, sigma, n_target, dt, seed, repeats):
-        return int(self.L.ref_mcc_count(v.shape[0], np.ascontiguousarray(v, np.float64).reshape(-1), kind, w, sigma,
-                                        n_target, dt, seed, repeats))
+        """(first-draw hits as the handler counts them, particles actually scattered)"""
+        sc = C.c_int64()
+        hits = int(self.L.ref_mcc_count(v.shape[0], np.ascontiguousarray(v, np.float64).reshape(-1), kind, w, sigma,
+                                        n_target, dt, seed, repeats, C.byref(sc)))
+        return hits, sc.value

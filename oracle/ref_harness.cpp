@@ -16,6 +16,9 @@
 
 #include <chrono>
 #include <cstdint>
+#ifdef USE_OPENMP
+#include <omp.h>
+#endif
 #include <cstring>
 #include <memory>
 #include <vector>
@@ -108,6 +111,62 @@ int ref_push(void* h, const double* Enode, int64_t P, double* x, double* v, cons
     std::memcpy(rho, rhov.data(), sizeof(double) * N);
     if (substeps) *substeps = ct.getStatistics().total_crossings;
     return 0;
+}
+
+// The reference particle path over all host threads, structured like the reference's own
+// OpenMP branch of PICCycle::pushParticles (PICCycle.cpp:483-563): dynamic schedule over
+// particles, thread-local charge buffers reduced at the end.  Returns wall seconds.
+double ref_push_parallel(void* h, const double* Enode, int64_t P, double* x, double* v, const int32_t* kind,
+                         const double* w, int32_t* tet, uint8_t* lost, double dt, int nseg, int kernel, double* rho,
+                         int* threads_used)
+{
+    auto* rm = static_cast<RefMesh*>(h);
+    const auto& nodes = rm->mesh->getNodes();
+    const auto& els = rm->mesh->getElements();
+    const std::size_t N = nodes.size();
+    std::vector<Vector3D> E(N), B(N, Vector3D(0, 0, 0));
+    for (std::size_t i = 0; i < N; ++i) E[i] = Vector3D(Enode[3 * i], Enode[3 * i + 1], Enode[3 * i + 2]);
+    auto interp = std::make_shared<SP::FieldInterpolator>();
+    interp->setMesh(nodes, els);
+    interp->setElectricField(E);
+    interp->setMagneticField(B);
+    auto dep = std::make_shared<SP::ChargeDepositor>();
+    dep->setMesh(nodes, els);
+    dep->setTrajectoryDepositionScheme(static_cast<SP::TrajectoryChargeDepositionKernel>(kernel),
+                                       static_cast<std::size_t>(nseg));
+    SP::CrossTetrahedron ct;
+    ct.setMesh(nodes, els);
+    ct.setFieldInterpolator(interp);
+    ct.setChargeDepositor(dep);
+    std::vector<SP::Particle> parts;
+    parts.reserve(P);
+    for (int64_t i = 0; i < P; ++i) parts.push_back(make_particle((std::size_t)i + 1, kind[i], x + 3 * i, v + 3 * i, w[i]));
+    int nt = 1;
+#ifdef USE_OPENMP
+    nt = omp_get_max_threads();
+#endif
+    std::vector<std::vector<double>> trho(nt, std::vector<double>(N, 0.0));
+    auto t0 = std::chrono::steady_clock::now();
+#ifdef USE_OPENMP
+#pragma omp parallel for schedule(dynamic, 1000)
+#endif
+    for (int64_t i = 0; i < P; ++i) {
+        int tid = 0;
+#ifdef USE_OPENMP
+        tid = omp_get_thread_num();
+#endif
+        SP::ElementId hint = tet[i] < 0 ? static_cast<SP::ElementId>(-1) : (SP::ElementId)tet[i];
+        auto r = ct.crossTetrahedron(&parts[i], dt, trho[tid], true, hint);
+        x[3 * i] = r.final_position.x(); x[3 * i + 1] = r.final_position.y(); x[3 * i + 2] = r.final_position.z();
+        v[3 * i] = r.final_velocity.x(); v[3 * i + 1] = r.final_velocity.y(); v[3 * i + 2] = r.final_velocity.z();
+        tet[i] = (int32_t)r.final_element;
+        lost[i] = r.lost_particle ? 1 : 0;
+    }
+    for (std::size_t n = 0; n < N; ++n)
+        for (int t = 0; t < nt; ++t) rho[n] += trho[t][n];
+    auto t1 = std::chrono::steady_clock::now();
+    if (threads_used) *threads_used = nt;
+    return std::chrono::duration<double>(t1 - t0).count();
 }
 
 // A fresh PoissonSolver: Dirichlet nodes take phi[i], nodal charge rho; DIRECT solve.
@@ -240,11 +299,13 @@ int ref_lsq_field(void* h, const double* phi, double* E)
 }
 
 // Background MCC with one constant elastic process per species (sigma, n_target), run
-// `repeats` times on copies of the same P particles; returns the total collision count
-// (reference two-draw form, CollisionAlgorithm.cpp:500-538).
+// `repeats` times on copies of the same P particles.  Returns the handler's collision count
+// (first-draw hits, CollisionAlgorithm.cpp:527-531) and, in *scattered, how many particles
+// actually changed velocity (second draw passed too, :195-200).
 int64_t ref_mcc_count(int64_t P, const double* v, int kind, double w, double sigma, double n_target, double dt,
-                      unsigned seed, int repeats)
+                      unsigned seed, int repeats, int64_t* scattered)
 {
+    int64_t changed = 0;
     using namespace SCDAT::Collision;
     MonteCarloCollisionHandler handler(seed);
     handler.clearCollisionProcesses();
@@ -263,8 +324,13 @@ int64_t ref_mcc_count(int64_t P, const double* v, int kind, double w, double sig
         double z[3] = {0, 0, 0};
         for (int64_t i = 0; i < P; ++i) ps.push_back(make_particle((std::size_t)i + 1, kind, z, v + 3 * i, w));
         handler.processCollisions(ps, dt);
+        for (int64_t i = 0; i < P; ++i) {
+            const auto u = ps[i].getVelocity();
+            if (u.x() != v[3 * i] || u.y() != v[3 * i + 1] || u.z() != v[3 * i + 2]) ++changed;
+        }
     }
     total = (int64_t)handler.getStatistics().total_collisions;
+    if (scattered) *scattered = changed;
     return total;
 }
 

@@ -1,0 +1,309 @@
+"""ctypes binding of the C ABI in include/scdat_b200.h.
+
+This is a thin harness for tests and the benchmark: every call goes straight through the
+shared library.  ``load()`` raises when libscdat_b200.so is missing -- there is no fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libscdat_b200.so")
+
+PREC_FP64, PREC_MIXED = 0, 1
+DEP_NEAREST, DEP_LINEAR, DEP_GAUSS3 = 0, 1, 2
+BC_NONE, BC_ABSORB, BC_PERIODIC = 0, 1, 2
+ACTIVE, ABSORBED, ESCAPED = 0, 1, 2
+ERR_NOT_CONVERGED = -5
+
+
+class MeshDesc(C.Structure):
+    _fields_ = [("n_nodes", C.c_int64), ("n_tets", C.c_int64), ("node_xyz", C.c_void_p), ("tet_nodes", C.c_void_p),
+                ("tet_neighbors", C.c_void_p), ("node_dirichlet", C.c_void_p), ("tet_eps_rel", C.c_void_p)]
+
+
+class Params(C.Structure):
+    _fields_ = [("dt", C.c_double), ("deposit_kernel", C.c_int32), ("deposit_segments", C.c_int32),
+                ("adaptive_floor_ratio", C.c_double), ("precision", C.c_int32), ("use_neighbor_lists", C.c_int32),
+                ("face_bc", C.c_int32 * 6), ("body_tally", C.c_int32), ("poisson_charge_sign", C.c_int32),
+                ("pcg_rtol", C.c_double), ("pcg_max_iter", C.c_int32), ("sort_interval", C.c_int32),
+                ("particle_capacity", C.c_int64), ("seed", C.c_uint64)]
+
+
+class SpeciesC(C.Structure):
+    _fields_ = [("charge", C.c_double), ("mass", C.c_double), ("weight", C.c_double), ("electron_like", C.c_int32),
+                ("pad", C.c_int32)]
+
+
+class ElasticC(C.Structure):
+    _fields_ = [("target_density", C.c_double), ("sigma_max", C.c_double), ("e_ref_ev", C.c_double),
+                ("alpha", C.c_double), ("e_threshold_ev", C.c_double), ("enabled", C.c_int32), ("mode", C.c_int32)]
+
+
+class StatsC(C.Structure):
+    _fields_ = [("completed_steps", C.c_int64), ("simulation_time", C.c_double), ("total_charge", C.c_double),
+                ("total_energy", C.c_double), ("active_particles", C.c_int64), ("stored_particles", C.c_int64),
+                ("surface_deposited_charge", C.c_double), ("substeps", C.c_int64), ("lost_events", C.c_int64),
+                ("mcc_collisions", C.c_int64), ("last_pcg_iterations", C.c_int32), ("pad", C.c_int32),
+                ("last_pcg_relres", C.c_double)]
+
+
+# every symbol declared in include/scdat_b200.h
+EXPORTS = ["scdat_default_params", "scdat_create", "scdat_destroy", "scdat_last_error", "scdat_set_species",
+           "scdat_set_particles", "scdat_seed_box_particles", "scdat_kuhn_box_mesh", "scdat_get_particle_count",
+           "scdat_get_particles", "scdat_set_potential", "scdat_set_node_potentials", "scdat_set_electric_field",
+           "scdat_set_elastic_mcc", "scdat_step", "scdat_push", "scdat_solve_field", "scdat_collide", "scdat_compact",
+           "scdat_get_fields", "scdat_get_species_charge", "scdat_get_ledger", "scdat_reset_ledger",
+           "scdat_get_statistics", "scdat_version", "scdat_stream", "scdat_set_timing", "scdat_get_timing"]
+
+_LIB = None
+
+
+def load():
+    """Load the shared library (raises if it has not been built)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m scdat_b200.build`")
+    L = C.CDLL(LIB_PATH)
+    vp = C.c_void_p
+    L.scdat_default_params.argtypes = [C.POINTER(Params)]
+    L.scdat_default_params.restype = None
+    L.scdat_create.argtypes = [C.POINTER(MeshDesc), C.POINTER(Params), C.POINTER(vp)]
+    L.scdat_destroy.argtypes = [vp]
+    L.scdat_last_error.argtypes = [vp]
+    L.scdat_last_error.restype = C.c_char_p
+    L.scdat_set_species.argtypes = [vp, C.c_int32, C.POINTER(SpeciesC)]
+    L.scdat_set_particles.argtypes = [vp, C.c_int32, C.c_int64, vp, vp, vp, vp]
+    L.scdat_seed_box_particles.argtypes = [vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_double, vp, vp,
+                                           C.c_int32, C.c_double, C.c_uint64]
+    L.scdat_kuhn_box_mesh.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_double, vp, vp, C.c_double, C.c_double,
+                                      C.POINTER(C.c_int64), C.POINTER(C.c_int64), vp, vp, vp, vp, vp,
+                                      C.POINTER(C.c_int64)]
+    L.scdat_get_particle_count.argtypes = [vp, C.c_int32, C.POINTER(C.c_int64)]
+    L.scdat_get_particles.argtypes = [vp, C.c_int32, C.c_int64, vp, vp, vp, vp, vp, C.POINTER(C.c_int64)]
+    L.scdat_set_potential.argtypes = [vp, vp]
+    L.scdat_set_node_potentials.argtypes = [vp, C.c_int64, vp, vp]
+    L.scdat_set_electric_field.argtypes = [vp, vp]
+    L.scdat_set_elastic_mcc.argtypes = [vp, C.c_int32, C.POINTER(ElasticC)]
+    for f in ("scdat_push", "scdat_solve_field", "scdat_collide", "scdat_compact", "scdat_reset_ledger"):
+        getattr(L, f).argtypes = [vp]
+    L.scdat_step.argtypes = [vp, C.c_int32]
+    L.scdat_get_fields.argtypes = [vp, vp, vp, vp]
+    L.scdat_get_species_charge.argtypes = [vp, C.c_int32, vp]
+    L.scdat_get_ledger.argtypes = [vp, vp]
+    L.scdat_get_statistics.argtypes = [vp, C.POINTER(StatsC)]
+    L.scdat_stream.argtypes = [vp]
+    L.scdat_stream.restype = vp
+    L.scdat_set_timing.argtypes = [vp, C.c_int32]
+    L.scdat_get_timing.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_int64), C.POINTER(C.c_int64),
+                                   C.POINTER(C.c_double), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+    L.scdat_version.argtypes = []
+    L.scdat_version.restype = C.c_char_p
+    _LIB = L
+    return L
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def kuhn_box_mesh(n, h, body=None, bias=0.0, wall=0.0):
+    """Mesh arrays of the 6-tet Kuhn box built by the library (scdat_kuhn_box_mesh)."""
+    L = load()
+    nx, ny, nz = n
+    lo = hi = None
+    if body is not None:
+        lo = np.array([body[0][0], body[1][0], body[2][0]], np.int32)
+        hi = np.array([body[0][1], body[1][1], body[2][1]], np.int32)
+    N = C.c_int64()
+    T = C.c_int64()
+    nc = C.c_int64()
+    rc = L.scdat_kuhn_box_mesh(nx, ny, nz, h, _p(lo), _p(hi), bias, wall, C.byref(N), C.byref(T), None, None, None,
+                               None, None, C.byref(nc))
+    assert rc == 0
+    xyz = np.zeros((N.value, 3))
+    tet = np.zeros((T.value, 4), np.int32)
+    dirichlet = np.zeros(N.value, np.uint8)
+    phi = np.zeros(N.value)
+    hexes = np.zeros((nc.value, 3), np.int32)
+    rc = L.scdat_kuhn_box_mesh(nx, ny, nz, h, _p(lo), _p(hi), bias, wall, C.byref(N), C.byref(T), _p(xyz), _p(tet),
+                               _p(dirichlet), _p(phi), _p(hexes), C.byref(nc))
+    assert rc == 0
+    return dict(xyz=xyz, tet=tet, dirichlet=dirichlet, phi=phi, hex_ijk=hexes)
+
+
+class ScdatError(RuntimeError):
+    def __init__(self, rc, msg):
+        super().__init__(f"scdat error {rc}: {msg}")
+        self.rc = rc
+
+
+class Domain:
+    """One device context: mesh, fields, species and their particles."""
+
+    def __init__(self, xyz, tet, dirichlet, dt, *, nbr=None, eps_rel=None, precision=PREC_FP64, face_bc=(0,) * 6,
+                 deposit_kernel=DEP_LINEAR, deposit_segments=10, use_neighbor_lists=True, pcg_rtol=1e-8,
+                 pcg_max_iter=5000, sort_interval=0, charge_sign=-1, body_tally=True, seed=0x5CDA7B200,
+                 floor_ratio=0.001):
+        self.L = load()
+        self.xyz = np.ascontiguousarray(xyz, np.float64)
+        self.tet = np.ascontiguousarray(tet, np.int32)
+        self.dirichlet = np.ascontiguousarray(dirichlet, np.uint8)
+        self.nbr = None if nbr is None else np.ascontiguousarray(nbr, np.int32)
+        self.eps_rel = None if eps_rel is None else np.ascontiguousarray(eps_rel, np.float64)
+        self.N = self.xyz.shape[0]
+        self.T = self.tet.shape[0]
+        md = MeshDesc(self.N, self.T, _p(self.xyz), _p(self.tet), _p(self.nbr), _p(self.dirichlet), _p(self.eps_rel))
+        prm = Params()
+        self.L.scdat_default_params(C.byref(prm))
+        prm.dt = dt
+        prm.precision = precision
+        for f in range(6):
+            prm.face_bc[f] = face_bc[f]
+        prm.deposit_kernel = deposit_kernel
+        prm.deposit_segments = deposit_segments
+        prm.use_neighbor_lists = 1 if use_neighbor_lists else 0
+        prm.pcg_rtol = pcg_rtol
+        prm.pcg_max_iter = pcg_max_iter
+        prm.sort_interval = sort_interval
+        prm.poisson_charge_sign = charge_sign
+        prm.body_tally = 1 if body_tally else 0
+        prm.seed = seed
+        prm.adaptive_floor_ratio = floor_ratio
+        self.params = prm
+        h = C.c_void_p()
+        rc = self.L.scdat_create(C.byref(md), C.byref(prm), C.byref(h))
+        if rc != 0:
+            raise ScdatError(rc, "scdat_create failed (bad mesh or CUDA error)")
+        self.h = h
+        self.nspecies = 0
+
+    def _ck(self, rc):
+        if rc != 0:
+            raise ScdatError(rc, self.L.scdat_last_error(self.h).decode())
+        return rc
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.scdat_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_species(self, species):
+        arr = (SpeciesC * len(species))(*[SpeciesC(s.q, s.m, s.w, 1 if s.q < 0 else 0, 0) for s in species])
+        self._ck(self.L.scdat_set_species(self.h, len(species), arr))
+        self.nspecies = len(species)
+
+    def set_particles(self, s, x, v, tet=None, ids=None):
+        x = np.ascontiguousarray(x, np.float64)
+        v = np.ascontiguousarray(v, np.float64)
+        t = None if tet is None else np.ascontiguousarray(tet, np.int32)
+        i = None if ids is None else np.ascontiguousarray(ids, np.uint32)
+        self._ck(self.L.scdat_set_particles(self.h, s, x.shape[0], _p(x), _p(v), _p(t), _p(i)))
+
+    def seed_box(self, s, n, h, body, ppc, temp_ev, seed):
+        lo = hi = None
+        if body is not None:
+            lo = np.array([body[0][0], body[1][0], body[2][0]], np.int32)
+            hi = np.array([body[0][1], body[1][1], body[2][1]], np.int32)
+        self._ck(self.L.scdat_seed_box_particles(self.h, s, n[0], n[1], n[2], h, _p(lo), _p(hi), ppc, temp_ev, seed))
+
+    def count(self, s):
+        n = C.c_int64()
+        self._ck(self.L.scdat_get_particle_count(self.h, s, C.byref(n)))
+        return n.value
+
+    def get_particles(self, s):
+        n = self.count(s)
+        x = np.zeros((n, 3))
+        v = np.zeros((n, 3))
+        t = np.zeros(n, np.int32)
+        st = np.zeros(n, np.uint8)
+        ids = np.zeros(n, np.uint32)
+        nn = C.c_int64()
+        self._ck(self.L.scdat_get_particles(self.h, s, n, _p(x), _p(v), _p(t), _p(st), _p(ids), C.byref(nn)))
+        return dict(x=x, v=v, tet=t, status=st, id=ids)
+
+    def set_potential(self, phi):
+        phi = np.ascontiguousarray(phi, np.float64)
+        self._ck(self.L.scdat_set_potential(self.h, _p(phi)))
+
+    def set_node_potentials(self, nodes, values):
+        nodes = np.ascontiguousarray(nodes, np.int64)
+        values = np.ascontiguousarray(values, np.float64)
+        self._ck(self.L.scdat_set_node_potentials(self.h, nodes.shape[0], _p(nodes), _p(values)))
+
+    def set_electric_field(self, E):
+        E = np.ascontiguousarray(E, np.float64)
+        self._ck(self.L.scdat_set_electric_field(self.h, _p(E)))
+
+    def set_elastic(self, s, n_target, sigma, mode=0, alpha=0.0, e_ref=1.0, e_th=0.0, enabled=True):
+        proc = ElasticC(n_target, sigma, e_ref, alpha, e_th, 1 if enabled else 0, mode)
+        self._ck(self.L.scdat_set_elastic_mcc(self.h, s, C.byref(proc)))
+
+    def push(self):
+        self._ck(self.L.scdat_push(self.h))
+
+    def solve_field(self, allow_not_converged=False):
+        rc = self.L.scdat_solve_field(self.h)
+        if rc == ERR_NOT_CONVERGED and allow_not_converged:
+            return rc
+        return self._ck(rc)
+
+    def collide(self):
+        self._ck(self.L.scdat_collide(self.h))
+
+    def compact(self):
+        self._ck(self.L.scdat_compact(self.h))
+
+    def step(self, n=1):
+        self._ck(self.L.scdat_step(self.h, n))
+
+    def fields(self):
+        rho = np.zeros(self.N)
+        phi = np.zeros(self.N)
+        E = np.zeros((self.N, 3))
+        self._ck(self.L.scdat_get_fields(self.h, _p(rho), _p(phi), _p(E)))
+        return rho, phi, E
+
+    def species_charge(self, s):
+        r = np.zeros(self.N)
+        self._ck(self.L.scdat_get_species_charge(self.h, s, _p(r)))
+        return r
+
+    def ledger(self):
+        led = np.zeros((7, 8))
+        self._ck(self.L.scdat_get_ledger(self.h, _p(led)))
+        return led
+
+    def reset_ledger(self):
+        self._ck(self.L.scdat_reset_ledger(self.h))
+
+    def stream(self):
+        return self.L.scdat_stream(self.h)
+
+    def set_timing(self, on=True):
+        self._ck(self.L.scdat_set_timing(self.h, 1 if on else 0))
+
+    def timing(self):
+        pm, fm = C.c_double(), C.c_double()
+        pl, pp, fs, kl = C.c_int64(), C.c_int64(), C.c_int64(), C.c_int64()
+        self._ck(self.L.scdat_get_timing(self.h, C.byref(pm), C.byref(pl), C.byref(pp), C.byref(fm), C.byref(fs),
+                                         C.byref(kl)))
+        return dict(push_ms=pm.value, push_launches=pl.value, push_particles=pp.value, field_ms=fm.value,
+                    field_solves=fs.value, kernel_launches=kl.value)
+
+    def stats(self):
+        st = StatsC()
+        self._ck(self.L.scdat_get_statistics(self.h, C.byref(st)))
+        return {k: getattr(st, k) for k, _ in StatsC._fields_ if k != "pad"}

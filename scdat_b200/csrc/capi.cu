@@ -1,0 +1,1122 @@
+// capi.cu -- the scdat_ctx object behind the C ABI in include/scdat_b200.h.
+//
+// Owns the device copies of the mesh, fields, per-species particle stores and the ledger,
+// and sequences one PIC-MCC step on a CUDA stream:
+//   clear charge -> push (gather/Boris/relocate/deposit/boundary/MCC) -> finalise charge
+//   -> RHS -> PCG -> potentials -> nodal LSQ field
+// which is the order of PICCycle::executeTimeStep (PICCycle.cpp:311-416) followed by the
+// background MCC step of the reference driver (Main/main_PICcore.cpp:487-515).
+#include "../../include/scdat_b200.h"
+#include "common.cuh"
+#include "field.cuh"
+#include "mesh_setup.h"
+#include "push.cuh"
+
+#include <cub/device/device_radix_sort.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+namespace scdat {
+void launch_push_f64(const MeshView& M, const ParticleStore& P, const SpeciesDev& S, const PushParams& pp,
+                     const double* E, unsigned long long* rlo, unsigned long long* rhi, LedgerDev* L, double* ke_part,
+                     int grid, cudaStream_t st);
+void launch_mcc_f64(const ParticleStore& P, const SpeciesDev& S, const PushParams& pp, LedgerDev* L, int grid,
+                    cudaStream_t st);
+void launch_push_mixed(const MeshView& M, const ParticleStore& P, const SpeciesDev& S, const PushParams& pp,
+                       const float* Ef, unsigned long long* rlo, unsigned long long* rhi, LedgerDev* L,
+                       double* ke_part, int grid, cudaStream_t st);
+void launch_mcc_mixed(const ParticleStore& P, const SpeciesDev& S, const PushParams& pp, LedgerDev* L, int grid,
+                      cudaStream_t st);
+void launch_to_mixed(const MeshView& M, int64_t n, const double* x, const double* y, const double* z,
+                     const double* vx, const double* vy, const double* vz, const ParticleStore& P, cudaStream_t st);
+void launch_from_mixed(const MeshView& M, int64_t n, const ParticleStore& P, double* x, double* y, double* z,
+                       double* vx, double* vy, double* vz, cudaStream_t st);
+void launch_seed_box(const int32_t* hex_ijk, int64_t ncell, int32_t ppc, int32_t S_total, int32_t s, double h,
+                     double sigma, uint64_t seed, const ParticleStore& P, bool mixed, const MeshView& M,
+                     cudaStream_t st);
+void launch_sort_keys(int64_t n, const int32_t* tet, uint32_t inactive_key, uint32_t* keys, uint32_t* vals,
+                      int64_t* active, cudaStream_t st);
+template <typename T>
+void launch_gather(int64_t n, const uint32_t* perm, const T* in, T* out, cudaStream_t st);
+void launch_scatter_values(int64_t n, const int64_t* idx, const double* v, double* dst, cudaStream_t st);
+}  // namespace scdat
+
+using namespace scdat;
+
+namespace {
+
+template <typename T>
+struct DBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    DBuf() = default;
+    DBuf(const DBuf&) = delete;
+    DBuf& operator=(const DBuf&) = delete;
+    ~DBuf() { release(); }
+    void release()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    cudaError_t alloc(size_t count)
+    {
+        release();
+        if (count == 0) return cudaSuccess;
+        cudaError_t e = cudaMalloc((void**)&p, count * sizeof(T));
+        if (e == cudaSuccess) n = count;
+        return e;
+    }
+    cudaError_t upload(const T* h, size_t count, cudaStream_t st)
+    {
+        cudaError_t e = alloc(count);
+        if (e != cudaSuccess || count == 0) return e;
+        return cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, st);
+    }
+    void swap(DBuf& o)
+    {
+        std::swap(p, o.p);
+        std::swap(n, o.n);
+    }
+};
+
+struct SpeciesState {
+    scdat_species sp{};
+    scdat_elastic mcc{};
+    int64_t cap = 0;
+    int64_t n = 0;  // host view of the stored count (updated on set/compact)
+    DBuf<double> x, y, z, vx, vy, vz;
+    DBuf<float> xf, yf, zf, vxf, vyf, vzf;
+    DBuf<int32_t> tet;
+    DBuf<uint32_t> id;
+};
+
+}  // namespace
+
+struct scdat_ctx {
+    std::string err;
+    scdat_params prm{};
+    bool mixed = false;
+    HostMesh hm;
+    HostGeometry hg;
+    HostGrid hgrid;
+    HostGraph hgr;
+    HostPoisson hps;
+    MeshView mv{};
+    PoissonView pv{};
+    // mesh
+    DBuf<double> xyz, geom;
+    DBuf<float> geomf;
+    DBuf<int4> tet, nbr;
+    DBuf<int32_t> bin_start, bin_tets, gptr, gcol;
+    // poisson
+    DBuf<int32_t> row_node, lift_ptr, lift_node, row_ptr, col;
+    DBuf<double> cv, lift_val, val, diag, dinv;
+    DBuf<float> valf;
+    DBuf<double> b, x, r, z, p, pn, q;
+    DBuf<float> xf, rf, zf, pf, pnf, qf;
+    DBuf<PcgScalars> sc;
+    DBuf<double> part;
+    // fields
+    DBuf<double> rho, phi, E, tmp_rho;
+    DBuf<float> Ef;
+    DBuf<unsigned long long> acc_lo, acc_hi, totq;
+    // particles
+    std::vector<SpeciesState> species;
+    DBuf<int64_t> counts;
+    DBuf<LedgerDev> led;
+    DBuf<double> ke_part;
+    // sort scratch
+    DBuf<uint32_t> kin, kout, vin, vout;
+    DBuf<unsigned char> cub_tmp;
+    DBuf<double> scratch64;
+    DBuf<float> scratch32;
+    DBuf<int32_t> scratchi;
+    DBuf<uint32_t> scratchu;
+    DBuf<int64_t> nact;
+    DBuf<int64_t> idx64;
+    double uq = 1.0, ue = 1.0;
+    int64_t steps = 0;
+    double sim_time = 0.0;
+    int last_pcg_iter = 0;
+    double last_pcg_rel = 0.0;
+    cudaStream_t st = nullptr;
+    int nsm = 148;
+    int grid_push = 148 * 8, grid_nodes = 148 * 4, grid_red = 148 * 2;
+    // optional per-kernel timing (CUDA events around the launches on the context stream)
+    bool timing = false;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_push, ev_field;
+    double push_ms = 0.0, field_ms = 0.0;
+    int64_t push_launches = 0, field_solves = 0;
+    int64_t push_particles = 0;
+    int64_t launches = 0;  // kernels of this library launched since scdat_set_timing
+};
+
+#define CK(call)                                                                                    \
+    do {                                                                                            \
+        cudaError_t e_ = (call);                                                                    \
+        if (e_ != cudaSuccess) {                                                                    \
+            ctx->err = std::string(#call) + ": " + cudaGetErrorString(e_);                          \
+            return SCDAT_ERR_CUDA;                                                                  \
+        }                                                                                           \
+    } while (0)
+
+#define ARG(cond, msg)                  \
+    do {                                \
+        if (!(cond)) {                  \
+            ctx->err = msg;             \
+            return SCDAT_ERR_ARG;       \
+        }                               \
+    } while (0)
+
+namespace {
+
+double pow2_ceil(double v)
+{
+    if (!(v > 0.0) || !std::isfinite(v)) return 1.0;
+    int e;
+    std::frexp(v, &e);  // v = f * 2^e, f in [0.5, 1)
+    return std::ldexp(1.0, e);
+}
+
+ParticleStore store_of(scdat_ctx* ctx, int s)
+{
+    SpeciesState& S = ctx->species[s];
+    ParticleStore P{};
+    P.x = S.x.p; P.y = S.y.p; P.z = S.z.p;
+    P.vx = S.vx.p; P.vy = S.vy.p; P.vz = S.vz.p;
+    P.xf = S.xf.p; P.yf = S.yf.p; P.zf = S.zf.p;
+    P.vxf = S.vxf.p; P.vyf = S.vyf.p; P.vzf = S.vzf.p;
+    P.tet = S.tet.p;
+    P.id = S.id.p;
+    P.count = ctx->counts.p + s;
+    return P;
+}
+
+SpeciesDev species_dev(const scdat_ctx* ctx, int s)
+{
+    const SpeciesState& S = ctx->species[s];
+    SpeciesDev d{};
+    d.q = S.sp.charge;
+    d.m = S.sp.mass;
+    d.w = S.sp.weight;
+    d.qm = S.sp.charge / S.sp.mass;
+    int nseg = std::min(std::max(ctx->prm.deposit_segments, 1), 128);
+    d.cw_seg = (S.sp.charge / (double)nseg) * S.sp.weight;
+    d.electron_like = S.sp.electron_like;
+    d.mcc_enabled = S.mcc.enabled;
+    d.mcc_mode = S.mcc.mode;
+    d.mcc_n = S.mcc.target_density;
+    d.mcc_sigma = S.mcc.sigma_max;
+    d.mcc_eref = S.mcc.e_ref_ev;
+    d.mcc_alpha = S.mcc.alpha;
+    d.mcc_eth = S.mcc.e_threshold_ev;
+    return d;
+}
+
+PushParams push_params(const scdat_ctx* ctx, bool do_mcc)
+{
+    PushParams pp{};
+    pp.dt = ctx->prm.dt;
+    pp.floor_ratio = ctx->prm.adaptive_floor_ratio;
+    pp.nseg = std::min(std::max(ctx->prm.deposit_segments, 1), 128);
+    pp.dep_kernel = ctx->prm.deposit_kernel;
+    for (int f = 0; f < 6; ++f) pp.face_bc[f] = ctx->prm.face_bc[f];
+    for (int a = 0; a < 3; ++a) {
+        bool per = (ctx->prm.face_bc[2 * a] == SCDAT_BC_PERIODIC || ctx->prm.face_bc[2 * a + 1] == SCDAT_BC_PERIODIC);
+        double span = ctx->hg.bmax[a] - ctx->hg.bmin[a];
+        // PeriodicBoundaryCondition maps every configured axis (x and y in the reference
+        // drivers, Main/main_PICcore.cpp:435-448); an axis is periodic when one of its faces is.
+        pp.period[a] = per ? span : 0.0;
+    }
+    pp.body_tally = ctx->prm.body_tally;
+    pp.do_mcc = do_mcc ? 1 : 0;
+    double sx = std::max(ctx->hg.bmax[0] - ctx->hg.bmin[0], 1e-12), sy = std::max(ctx->hg.bmax[1] - ctx->hg.bmin[1], 1e-12),
+           sz = std::max(ctx->hg.bmax[2] - ctx->hg.bmin[2], 1e-12);
+    double ms = std::max(sx, std::max(sy, sz));
+    pp.otol = std::max(1.0e-10, 1.0e-8 * ms);           // PICCycle.cpp:1238
+    pp.ntol = std::max(5.0 * pp.otol, 1.0e-9 * ms);      // PICCycle.cpp:1239
+    pp.inv_uq = 1.0 / ctx->uq;
+    pp.inv_ue = 1.0 / ctx->ue;
+    pp.seed = ctx->prm.seed;
+    pp.step = (uint32_t)ctx->steps;
+    pp.deposit = 1;
+    return pp;
+}
+
+int check_flags(scdat_ctx* ctx)
+{
+    unsigned long long f = 0;
+    CK(cudaMemcpyAsync(&f, &ctx->led.p->flags, sizeof(f), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    if (f & kFlagBadTet) {
+        ctx->err = "device flag: invalid tet index seen";
+        return SCDAT_ERR_DEVICE_FLAG;
+    }
+    return SCDAT_OK;
+}
+
+// ---- the stages ----------------------------------------------------------------------
+int do_push(scdat_ctx* ctx, bool do_mcc)
+{
+    const int S = (int)ctx->species.size();
+    if (S == 0) {
+        ctx->err = "species not set";
+        return SCDAT_ERR_STATE;
+    }
+    const int64_t N = ctx->hm.N;
+    CK(cudaMemsetAsync(ctx->acc_lo.p, 0, sizeof(unsigned long long) * S * N, ctx->st));
+    CK(cudaMemsetAsync(ctx->acc_hi.p, 0, sizeof(unsigned long long) * S * N, ctx->st));
+    CK(cudaMemsetAsync(ctx->ke_part.p, 0, sizeof(double) * ctx->grid_push, ctx->st));
+    CK(cudaMemsetAsync(&ctx->led.p->active, 0, sizeof(unsigned long long), ctx->st));
+    PushParams pp = push_params(ctx, do_mcc);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (ctx->timing) {
+        CK(cudaEventCreate(&e0));
+        CK(cudaEventCreate(&e1));
+        CK(cudaEventRecord(e0, ctx->st));
+    }
+    for (int s = 0; s < S; ++s) {
+        if (ctx->species[s].cap == 0) continue;
+        ctx->push_particles += ctx->species[s].n;
+        ParticleStore P = store_of(ctx, s);
+        SpeciesDev sd = species_dev(ctx, s);
+        if (ctx->mixed)
+            ++ctx->launches, launch_push_mixed(ctx->mv, P, sd, pp, ctx->Ef.p, ctx->acc_lo.p + s * N, ctx->acc_hi.p + s * N, ctx->led.p,
+                              ctx->ke_part.p, ctx->grid_push, ctx->st);
+        else
+            ++ctx->launches, launch_push_f64(ctx->mv, P, sd, pp, ctx->E.p, ctx->acc_lo.p + s * N, ctx->acc_hi.p + s * N, ctx->led.p,
+                            ctx->ke_part.p, ctx->grid_push, ctx->st);
+    }
+    CK(cudaGetLastError());
+    if (ctx->timing) {
+        CK(cudaEventRecord(e1, ctx->st));
+        ctx->ev_push.emplace_back(e0, e1);
+        ctx->push_launches += 1;
+    }
+    CK(cudaMemsetAsync(ctx->totq.p, 0, sizeof(unsigned long long) * 2, ctx->st));
+    ++ctx->launches;
+    launch_finalize_rho(N, S, ctx->acc_lo.p, ctx->acc_hi.p, ctx->uq, ctx->rho.p, ctx->totq.p, ctx->totq.p + 1,
+                        ctx->grid_nodes, ctx->st);
+    CK(cudaGetLastError());
+    return SCDAT_OK;
+}
+
+int do_lsq(scdat_ctx* ctx, double reg)
+{
+    CK(cudaMemsetAsync(&ctx->led.p->flags, 0, sizeof(unsigned long long), ctx->st));
+    ctx->launches += 2;
+    launch_lsq(ctx->hm.N, ctx->xyz.p, ctx->gptr.p, ctx->gcol.p, ctx->phi.p, reg, ctx->E.p, ctx->Ef.p,
+               &ctx->led.p->flags, ctx->grid_nodes, ctx->st);
+    CK(cudaGetLastError());
+    return SCDAT_OK;
+}
+
+int pcg_scalars_init(scdat_ctx* ctx, double rtol, int max_iter, double abs_thr2)
+{
+    PcgScalars h{};
+    h.rtol = rtol;
+    h.max_iter = max_iter;
+    h.abs_thr2 = abs_thr2;
+    CK(cudaMemcpyAsync(ctx->sc.p, &h, sizeof(h), cudaMemcpyHostToDevice, ctx->st));
+    return SCDAT_OK;
+}
+
+int read_scalars(scdat_ctx* ctx, PcgScalars& h)
+{
+    CK(cudaMemcpyAsync(&h, ctx->sc.p, sizeof(h), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return SCDAT_OK;
+}
+
+int run_pcg64(scdat_ctx* ctx, const double* bvec, double* xvec, double rtol, int max_iter, int& iters,
+              double& relres)
+{
+    const PoissonView& A = ctx->pv;
+    int rc = pcg_scalars_init(ctx, rtol, max_iter, 0.0);
+    if (rc) return rc;
+    ++ctx->launches;
+    launch_pcg_init64(A, bvec, xvec, ctx->r.p, ctx->z.p, ctx->sc.p, ctx->part.p, ctx->grid_red, ctx->st);
+    double* p = ctx->p.p;
+    double* pn = ctx->pn.p;
+    const int batch = 16;
+    PcgScalars h{};
+    for (int k = 0; k < max_iter; k += batch) {
+        for (int j = 0; j < batch; ++j) {
+            ctx->launches += 2;
+            launch_pcg_iter64(A, xvec, ctx->r.p, ctx->z.p, p, pn, ctx->q.p, ctx->sc.p, ctx->part.p, ctx->grid_red,
+                              ctx->st);
+            std::swap(p, pn);
+        }
+        CK(cudaGetLastError());
+        rc = read_scalars(ctx, h);
+        if (rc) return rc;
+        if (h.done) break;
+    }
+    if (max_iter <= 0) {
+        rc = read_scalars(ctx, h);
+        if (rc) return rc;
+    }
+    iters = h.iter;
+    relres = std::sqrt(h.rr / (h.bb > 0.0 ? h.bb : 1.0));
+    return SCDAT_OK;
+}
+
+// FP32-SpMV PCG inside an FP64 iterative-refinement loop (mixed form).
+int run_pcg_mixed(scdat_ctx* ctx, double rtol, int max_iter, int& iters, double& relres)
+{
+    const PoissonView& A = ctx->pv;
+    const int R = A.R;
+    iters = 0;
+    relres = 0.0;
+    PcgScalars h{};
+    for (int outer = 0; outer < 12; ++outer) {
+        ++ctx->launches;
+        launch_residual64(A, ctx->b.p, ctx->x.p, ctx->r.p, ctx->rf.p, ctx->sc.p, ctx->part.p, ctx->grid_red, ctx->st);
+        CK(cudaGetLastError());
+        int rc = read_scalars(ctx, h);
+        if (rc) return rc;
+        double bb = h.bb > 0.0 ? h.bb : 1.0;
+        relres = std::sqrt(h.rr / bb);
+        if (h.rr <= rtol * rtol * bb || iters >= max_iter) break;
+        // inner FP32 solve A e = r to 1e-4 relative, from e = 0
+        ctx->launches += 2;
+        launch_zero_f32(R, ctx->xf.p, ctx->grid_red, ctx->st);
+        rc = pcg_scalars_init(ctx, 1e-4, std::max(1, max_iter - iters), 0.0);
+        if (rc) return rc;
+        launch_pcg_init32(A, ctx->rf.p, ctx->xf.p, ctx->qf.p, ctx->zf.p, ctx->sc.p, ctx->part.p, ctx->grid_red,
+                          ctx->st);
+        // qf doubles as the inner residual vector; the direction buffers are pf/pnf, A*p goes to the
+        // inner q buffer below
+        float* p = ctx->pf.p;
+        float* pn = ctx->pnf.p;
+        float* rr = ctx->qf.p;
+        float* qq = reinterpret_cast<float*>(ctx->q.p);  // FP64 q buffer is free during the inner solve
+        const int batch = 16;
+        PcgScalars hi{};
+        for (int k = 0; k < max_iter; k += batch) {
+            for (int j = 0; j < batch; ++j) {
+                ctx->launches += 2;
+                launch_pcg_iter32(A, ctx->xf.p, rr, ctx->zf.p, p, pn, qq, ctx->sc.p, ctx->part.p, ctx->grid_red,
+                                  ctx->st);
+                std::swap(p, pn);
+            }
+            CK(cudaGetLastError());
+            rc = read_scalars(ctx, hi);
+            if (rc) return rc;
+            if (hi.done) break;
+        }
+        iters += hi.iter;
+        ++ctx->launches;
+        launch_add_correction(R, ctx->x.p, ctx->xf.p, ctx->grid_red, ctx->st);
+        CK(cudaGetLastError());
+    }
+    return SCDAT_OK;
+}
+
+int do_solve_field(scdat_ctx* ctx)
+{
+    const PoissonView& A = ctx->pv;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (ctx->timing) {
+        CK(cudaEventCreate(&e0));
+        CK(cudaEventCreate(&e1));
+        CK(cudaEventRecord(e0, ctx->st));
+    }
+    if (A.R > 0) {
+        ctx->launches += 3;
+        launch_gather_rows(A, ctx->phi.p, ctx->x.p, ctx->grid_red, ctx->st);
+        launch_rhs(A, ctx->rho.p, ctx->phi.p, (double)ctx->prm.poisson_charge_sign, ctx->b.p, ctx->grid_red, ctx->st);
+        CK(cudaGetLastError());
+        int it = 0;
+        double rel = 0.0;
+        int rc = ctx->mixed ? run_pcg_mixed(ctx, ctx->prm.pcg_rtol, ctx->prm.pcg_max_iter, it, rel)
+                            : run_pcg64(ctx, ctx->b.p, ctx->x.p, ctx->prm.pcg_rtol, ctx->prm.pcg_max_iter, it, rel);
+        if (rc) return rc;
+        ctx->last_pcg_iter = it;
+        ctx->last_pcg_rel = rel;
+        launch_scatter_rows(A, ctx->x.p, ctx->phi.p, ctx->grid_red, ctx->st);
+        CK(cudaGetLastError());
+    }
+    int rc = do_lsq(ctx, 0.0);
+    if (ctx->timing) {
+        CK(cudaEventRecord(e1, ctx->st));
+        ctx->ev_field.emplace_back(e0, e1);
+        ctx->field_solves += 1;
+    }
+    return rc;
+}
+
+int harvest_timing(scdat_ctx* ctx)
+{
+    CK(cudaStreamSynchronize(ctx->st));
+    for (auto& pr : ctx->ev_push) {
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, pr.first, pr.second));
+        ctx->push_ms += ms;
+        cudaEventDestroy(pr.first);
+        cudaEventDestroy(pr.second);
+    }
+    ctx->ev_push.clear();
+    for (auto& pr : ctx->ev_field) {
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, pr.first, pr.second));
+        ctx->field_ms += ms;
+        cudaEventDestroy(pr.first);
+        cudaEventDestroy(pr.second);
+    }
+    ctx->ev_field.clear();
+    return SCDAT_OK;
+}
+
+int do_sort(scdat_ctx* ctx, int s)
+{
+    SpeciesState& S = ctx->species[s];
+    const int64_t n = S.n;
+    if (n == 0) return SCDAT_OK;
+    const uint32_t inactive = (uint32_t)ctx->hm.T;  // keys: tet, T (no hint), T+1 (inactive)
+    int bits = 1;
+    while (((uint64_t)1 << bits) <= (uint64_t)inactive + 1) ++bits;
+    ctx->launches += 9;  // keys + 8 gathers (the radix sort itself is CUB's)
+    launch_sort_keys(n, S.tet.p, inactive, ctx->kin.p, ctx->vin.p, ctx->nact.p, ctx->st);
+    size_t tmp = 0;
+    CK(cub::DeviceRadixSort::SortPairs(nullptr, tmp, ctx->kin.p, ctx->kout.p, ctx->vin.p, ctx->vout.p, (int)n, 0, bits,
+                                       ctx->st));
+    if (tmp > ctx->cub_tmp.n) CK(ctx->cub_tmp.alloc(tmp));
+    CK(cub::DeviceRadixSort::SortPairs(ctx->cub_tmp.p, tmp, ctx->kin.p, ctx->kout.p, ctx->vin.p, ctx->vout.p, (int)n,
+                                       0, bits, ctx->st));
+    const uint32_t* perm = ctx->vout.p;
+    if (ctx->mixed) {
+        DBuf<float>* fa[6] = {&S.xf, &S.yf, &S.zf, &S.vxf, &S.vyf, &S.vzf};
+        for (auto* a : fa) {
+            if (ctx->scratch32.n < a->n) CK(ctx->scratch32.alloc(a->n));
+            launch_gather<float>(n, perm, a->p, ctx->scratch32.p, ctx->st);
+            a->swap(ctx->scratch32);
+        }
+    } else {
+        DBuf<double>* da[6] = {&S.x, &S.y, &S.z, &S.vx, &S.vy, &S.vz};
+        for (auto* a : da) {
+            if (ctx->scratch64.n < a->n) CK(ctx->scratch64.alloc(a->n));
+            launch_gather<double>(n, perm, a->p, ctx->scratch64.p, ctx->st);
+            a->swap(ctx->scratch64);
+        }
+    }
+    if (ctx->scratchi.n < S.tet.n) CK(ctx->scratchi.alloc(S.tet.n));
+    launch_gather<int32_t>(n, perm, S.tet.p, ctx->scratchi.p, ctx->st);
+    S.tet.swap(ctx->scratchi);
+    if (ctx->scratchu.n < S.id.n) CK(ctx->scratchu.alloc(S.id.n));
+    launch_gather<uint32_t>(n, perm, S.id.p, ctx->scratchu.p, ctx->st);
+    S.id.swap(ctx->scratchu);
+    CK(cudaGetLastError());
+    int64_t act = 0;
+    CK(cudaMemcpyAsync(&act, ctx->nact.p, sizeof(act), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    S.n = act;
+    CK(cudaMemcpyAsync(ctx->counts.p + s, &S.n, sizeof(int64_t), cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return SCDAT_OK;
+}
+
+}  // namespace
+
+// ======================================================================================
+// C ABI
+// ======================================================================================
+extern "C" {
+
+SCDAT_API const char* scdat_version(void) { return "scdat_b200 0.1.0 (sm_100a)"; }
+
+SCDAT_API void scdat_default_params(scdat_params* p)
+{
+    if (!p) return;
+    std::memset(p, 0, sizeof(*p));
+    p->dt = 0.0;
+    p->deposit_kernel = SCDAT_DEP_LINEAR;
+    p->deposit_segments = 10;
+    p->adaptive_floor_ratio = 0.001;
+    p->precision = SCDAT_PREC_FP64;
+    p->use_neighbor_lists = 1;
+    for (int f = 0; f < 6; ++f) p->face_bc[f] = SCDAT_BC_NONE;
+    p->body_tally = 1;
+    p->poisson_charge_sign = -1;
+    p->pcg_rtol = 1e-8;
+    p->pcg_max_iter = 5000;
+    p->sort_interval = 0;
+    p->particle_capacity = 0;
+    p->seed = 0x5CDA7B200ull;
+}
+
+SCDAT_API const char* scdat_last_error(const scdat_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+SCDAT_API int scdat_create(const scdat_mesh_desc* mesh, const scdat_params* params, scdat_ctx** out)
+{
+    if (!mesh || !params || !out) return SCDAT_ERR_ARG;
+    *out = nullptr;
+    auto holder = std::make_unique<scdat_ctx>();
+    scdat_ctx* ctx = holder.get();
+    ARG(mesh->n_nodes > 0 && mesh->n_tets > 0, "empty mesh");
+    ARG(mesh->n_nodes < (int64_t)0x7fffffff && mesh->n_tets < (int64_t)0x7fffffff, "mesh too large for int32 indices");
+    ARG(mesh->node_xyz && mesh->tet_nodes && mesh->node_dirichlet, "null mesh array");
+    ARG(params->dt > 0.0 && std::isfinite(params->dt), "dt must be positive");
+    ctx->prm = *params;
+    ctx->mixed = params->precision == SCDAT_PREC_MIXED;
+    HostMesh& m = ctx->hm;
+    m.N = mesh->n_nodes;
+    m.T = mesh->n_tets;
+    m.xyz.assign(mesh->node_xyz, mesh->node_xyz + 3 * m.N);
+    m.tet.assign(mesh->tet_nodes, mesh->tet_nodes + 4 * m.T);
+    m.dirichlet.assign(mesh->node_dirichlet, mesh->node_dirichlet + m.N);
+    if (mesh->tet_eps_rel) m.eps_rel.assign(mesh->tet_eps_rel, mesh->tet_eps_rel + m.T);
+    for (int64_t i = 0; i < 4 * m.T; ++i) ARG(m.tet[i] >= 0 && m.tet[i] < m.N, "tet node index out of range");
+    std::string e;
+    if (mesh->tet_neighbors) {
+        m.nbr.assign(mesh->tet_neighbors, mesh->tet_neighbors + 4 * m.T);
+        for (int64_t i = 0; i < 4 * m.T; ++i) ARG(m.nbr[i] >= -1 && m.nbr[i] < m.T, "tet neighbour out of range");
+    } else if (!(e = compute_face_neighbors(m, m.nbr)).empty()) {
+        ctx->err = e;
+        return SCDAT_ERR_ARG;
+    }
+    if (!(e = compute_geometry(m, ctx->hg)).empty() || !(e = build_locate_grid(m, ctx->hg, ctx->hgrid)).empty() ||
+        !(e = build_node_graph(m, ctx->hgr)).empty() || !(e = assemble_poisson(m, ctx->hgr, ctx->hps)).empty()) {
+        ctx->err = e;
+        return SCDAT_ERR_ARG;
+    }
+    CK(cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking));
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, dev));
+    ctx->grid_push = ctx->nsm * 8;
+    ctx->grid_nodes = ctx->nsm * 8;
+    ctx->grid_red = ctx->nsm * 4;
+    cudaStream_t st = ctx->st;
+    // mesh
+    CK(ctx->xyz.upload(m.xyz.data(), m.xyz.size(), st));
+    CK(ctx->geom.upload(ctx->hg.geom.data(), ctx->hg.geom.size(), st));
+    CK(ctx->geomf.upload(ctx->hg.geomf.data(), ctx->hg.geomf.size(), st));
+    CK(ctx->tet.upload(reinterpret_cast<const int4*>(m.tet.data()), (size_t)m.T, st));
+    CK(ctx->nbr.upload(reinterpret_cast<const int4*>(m.nbr.data()), (size_t)m.T, st));
+    CK(ctx->bin_start.upload(ctx->hgrid.bin_start.data(), ctx->hgrid.bin_start.size(), st));
+    CK(ctx->bin_tets.upload(ctx->hgrid.bin_tets.data(), ctx->hgrid.bin_tets.size(), st));
+    CK(ctx->gptr.upload(ctx->hgr.ptr.data(), ctx->hgr.ptr.size(), st));
+    CK(ctx->gcol.upload(ctx->hgr.col.data(), ctx->hgr.col.size(), st));
+    MeshView& mv = ctx->mv;
+    mv.N = m.N;
+    mv.T = m.T;
+    mv.xyz = ctx->xyz.p;
+    mv.tet = ctx->tet.p;
+    mv.nbr = ctx->nbr.p;
+    mv.geom = ctx->geom.p;
+    mv.geomf = ctx->geomf.p;
+    for (int a = 0; a < 3; ++a) {
+        mv.gmin[a] = ctx->hgrid.gmin[a];
+        mv.ginv[a] = ctx->hgrid.ginv[a];
+        mv.gdim[a] = ctx->hgrid.gdim[a];
+        mv.bmin[a] = ctx->hg.bmin[a];
+        mv.bmax[a] = ctx->hg.bmax[a];
+    }
+    mv.gdelta = ctx->hgrid.gdelta;
+    mv.bin_start = ctx->bin_start.p;
+    mv.bin_tets = ctx->bin_tets.p;
+    mv.use_nbr = params->use_neighbor_lists;
+    // poisson
+    HostPoisson& ps = ctx->hps;
+    CK(ctx->row_node.upload(ps.row_node.data(), ps.row_node.size(), st));
+    CK(ctx->cv.upload(ps.cv.data(), ps.cv.size(), st));
+    CK(ctx->lift_ptr.upload(ps.lift_ptr.data(), ps.lift_ptr.size(), st));
+    CK(ctx->lift_node.upload(ps.lift_node.data(), ps.lift_node.size(), st));
+    CK(ctx->lift_val.upload(ps.lift_val.data(), ps.lift_val.size(), st));
+    CK(ctx->row_ptr.upload(ps.row_ptr.data(), ps.row_ptr.size(), st));
+    CK(ctx->col.upload(ps.col.data(), ps.col.size(), st));
+    CK(ctx->val.upload(ps.val.data(), ps.val.size(), st));
+    CK(ctx->valf.upload(ps.valf.data(), ps.valf.size(), st));
+    CK(ctx->diag.upload(ps.diag.data(), ps.diag.size(), st));
+    CK(ctx->dinv.upload(ps.dinv.data(), ps.dinv.size(), st));
+    PoissonView& pv = ctx->pv;
+    pv.R = ps.R;
+    pv.row_node = ctx->row_node.p;
+    pv.cv = ctx->cv.p;
+    pv.lift_ptr = ctx->lift_ptr.p;
+    pv.lift_val = ctx->lift_val.p;
+    pv.lift_node = ctx->lift_node.p;
+    pv.row_ptr = ctx->row_ptr.p;
+    pv.col = ctx->col.p;
+    pv.val = ctx->val.p;
+    pv.valf = ctx->valf.p;
+    pv.diag = ctx->diag.p;
+    pv.dinv = ctx->dinv.p;
+    size_t R = (size_t)std::max(ps.R, 1);
+    for (DBuf<double>* v : {&ctx->b, &ctx->x, &ctx->r, &ctx->z, &ctx->p, &ctx->pn, &ctx->q}) CK(v->alloc(R));
+    for (DBuf<float>* v : {&ctx->xf, &ctx->rf, &ctx->zf, &ctx->pf, &ctx->pnf, &ctx->qf}) CK(v->alloc(R));
+    CK(ctx->sc.alloc(1));
+    CK(ctx->part.alloc((size_t)ctx->grid_red * 4));
+    // fields
+    CK(ctx->rho.alloc((size_t)m.N));
+    CK(ctx->tmp_rho.alloc((size_t)m.N));
+    CK(ctx->phi.alloc((size_t)m.N));
+    CK(ctx->E.alloc((size_t)(3 * m.N)));
+    CK(ctx->Ef.alloc((size_t)(3 * m.N)));
+    CK(cudaMemsetAsync(ctx->rho.p, 0, sizeof(double) * m.N, st));
+    CK(cudaMemsetAsync(ctx->phi.p, 0, sizeof(double) * m.N, st));
+    CK(cudaMemsetAsync(ctx->E.p, 0, sizeof(double) * 3 * m.N, st));
+    CK(cudaMemsetAsync(ctx->Ef.p, 0, sizeof(float) * 3 * m.N, st));
+    CK(ctx->totq.alloc(2));
+    CK(ctx->led.alloc(1));
+    CK(cudaMemsetAsync(ctx->led.p, 0, sizeof(LedgerDev), st));
+    CK(ctx->ke_part.alloc((size_t)ctx->grid_push));
+    CK(ctx->nact.alloc(1));
+    CK(cudaStreamSynchronize(st));
+    *out = holder.release();
+    return SCDAT_OK;
+}
+
+SCDAT_API int scdat_destroy(scdat_ctx* ctx)
+{
+    if (!ctx) return SCDAT_ERR_ARG;
+    if (ctx->st) cudaStreamSynchronize(ctx->st);
+    for (auto& pr : ctx->ev_push) { cudaEventDestroy(pr.first); cudaEventDestroy(pr.second); }
+    for (auto& pr : ctx->ev_field) { cudaEventDestroy(pr.first); cudaEventDestroy(pr.second); }
+    cudaStream_t st = ctx->st;
+    delete ctx;
+    if (st) cudaStreamDestroy(st);
+    return SCDAT_OK;
+}
+
+SCDAT_API int scdat_set_species(scdat_ctx* ctx, int32_t n_species, const scdat_species* sp)
+{
+    if (!ctx) return SCDAT_ERR_ARG;
+    ARG(n_species > 0 && n_species <= 16 && sp, "need 1..16 species");
+    ARG(ctx->species.empty(), "species are already set");
+    ctx->species = std::vector<SpeciesState>((size_t)n_species);
+    double mq = 0.0, me = 0.0;
+    const double c2 = 2.99792458e8 * 2.99792458e8;
+    for (int s = 0; s < n_species; ++s) {
+        ARG(sp[s].mass > 0.0 && std::isfinite(sp[s].charge) && sp[s].weight > 0.0, "bad species entry");
+        ctx->species[s].sp = sp[s];
+        mq = std::max(mq, std::fabs(sp[s].charge * sp[s].weight));
+        me = std::max(me, 0.5 * sp[s].mass * c2 * std::max(1.0, sp[s].weight));
+    }
+    ctx->uq = pow2_ceil(mq);
+    ctx->ue = pow2_ceil(me);
+    const int64_t N = ctx->hm.N;
+    CK(ctx->acc_lo.alloc((size_t)(n_species * N)));
+    CK(ctx->acc_hi.alloc((size_t)(n_species * N)));
+    CK(ctx->counts.alloc((size_t)n_species));
+    CK(cudaMemsetAsync(ctx->counts.p, 0, sizeof(int64_t) * n_species, ctx->st));
+    CK(cudaMemsetAsync(ctx->acc_lo.p, 0, sizeof(unsigned long long) * n_species * N, ctx->st));
+    CK(cudaMemsetAsync(ctx->acc_hi.p, 0, sizeof(unsigned long long) * n_species * N, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return SCDAT_OK;
+}
+
+static int alloc_species(scdat_ctx* ctx, int s, int64_t n)
+{
+    SpeciesState& S = ctx->species[s];
+    int64_t cap = std::max<int64_t>(n, 1);
+    if (ctx->mixed) {
+        for (DBuf<float>* a : {&S.xf, &S.yf, &S.zf, &S.vxf, &S.vyf, &S.vzf}) CK(a->alloc((size_t)cap));
+        for (DBuf<double>* a : {&S.x, &S.y, &S.z, &S.vx, &S.vy, &S.vz}) a->release();
+    } else {
+        for (DBuf<double>* a : {&S.x, &S.y, &S.z, &S.vx, &S.vy, &S.vz}) CK(a->alloc((size_t)cap));
+        for (DBuf<float>* a : {&S.xf, &S.yf, &S.zf, &S.vxf, &S.vyf, &S.vzf}) a->release();
+    }
+    CK(S.tet.alloc((size_t)cap));
+    CK(S.id.alloc((size_t)cap));
+    S.cap = cap;
+    S.n = n;
+    CK(cudaMemcpyAsync(ctx->counts.p + s, &S.n, sizeof(int64_t), cudaMemcpyHostToDevice, ctx->st));
+    // sort scratch must cover the largest species
+    size_t need = (size_t)cap;
+    if (ctx->kin.n < need) {
+        CK(ctx->kin.alloc(need));
+        CK(ctx->kout.alloc(need));
+        CK(ctx->vin.alloc(need));
+        CK(ctx->vout.alloc(need));
+    }
+    return SCDAT_OK;
+}
+
+SCDAT_API int scdat_set_particles(scdat_ctx* ctx, int32_t species, int64_t n, const double* x, const double* v,
+                                  const int32_t* tet_hint, const uint32_t* ids)
+{
+    if (!ctx) return SCDAT_ERR_ARG;
+    ARG(species >= 0 && species < (int)ctx->species.size(), "bad species index");
+    ARG(n >= 0 && (n == 0 || (x && v)), "bad particle arrays");
+    ARG(n < (int64_t)0xffffffffLL, "too many particles for 32-bit ids");
+    int rc = alloc_species(ctx, species, n);
+    if (rc) return rc;
+    if (n == 0) return SCDAT_OK;
+    SpeciesState& S = ctx->species[species];
+    std::vector<double> cx((size_t)n), cy((size_t)n), cz((size_t)n), wx((size_t)n), wy((size_t)n), wz((size_t)n);
+    for (int64_t i = 0; i < n; ++i) {
+        cx[i] = x[3 * i]; cy[i] = x[3 * i + 1]; cz[i] = x[3 * i + 2];
+        wx[i] = v[3 * i]; wy[i] = v[3 * i + 1]; wz[i] = v[3 * i + 2];
+    }
+    std::vector<int32_t> t((size_t)n, kTetNoHint);
+    if (tet_hint)
+        for (int64_t i = 0; i < n; ++i) t[i] = (tet_hint[i] >= 0 && tet_hint[i] < ctx->hm.T) ? tet_hint[i] : kTetNoHint;
+    std::vector<uint32_t> id((size_t)n);
+    for (int64_t i = 0; i < n; ++i) id[i] = ids ? ids[i] : (uint32_t)i;
+    CK(cudaMemcpyAsync(S.tet.p, t.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(S.id.p, id.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice, ctx->st));
+    if (!ctx->mixed) {
+        CK(cudaMemcpyAsync(S.x.p, cx.data(), sizeof(double) * n, cudaMemcpyHostToDevice, ctx->st));
+        CK(cudaMemcpyAsync(S.y.p, cy.data(), sizeof(double) * n, cudaMemcpyHostToDevice, ctx->st));
+        CK(cudaMemcpyAsync(S.z.p, cz.data(), sizeof(double) * n, cudaMemcpyHostToDevice, ctx->st));
+        CK(cudaMemcpyAsync(S.vx.p, wx.data(), sizeof(double) * n, cudaMemcpyHostToDevice, ctx->st));
+        CK(cudaMemcpyAsync(S.vy.p, wy.data(), sizeof(double) * n, cudaMemcpyHostToDevice, ctx->st));
+        CK(cudaMemcpyAsync(S.vz.p, wz.data(), sizeof(double) * n, cudaMemcpyHostToDevice, ctx->st));
+    } else {
+        DBuf<double> dx, dy, dz, dvx, dvy, dvz;
+        CK(dx.upload(cx.data(), n, ctx->st));
+        CK(dy.upload(cy.data(), n, ctx->st));
+        CK(dz.upload(cz.data(), n, ctx->st));
+        CK(dvx.upload(wx.data(), n, ctx->st));
+        CK(dvy.upload(wy.data(), n, ctx->st));
+        CK(dvz.upload(wz.data(), n, ctx->st));
+        launch_to_mixed(ctx->mv, n, dx.p, dy.p, dz.p, dvx.p, dvy.p, dvz.p, store_of(ctx, species), ctx->st);
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(ctx->st));
+    }
+    CK(cudaStreamSynchronize(ctx->st));
+    return SCDAT_OK;
+}
+
+SCDAT_API int scdat_get_particle_count(scdat_ctx* ctx, int32_t species, int64_t* n)
+{
+    if (!ctx || !n) return SCDAT_ERR_ARG;
+    ARG(species >= 0 && species < (int)ctx->species.size(), "bad species index");
+    *n = ctx->species[species].n;
+    return SCDAT_OK;
+}
+
+SCDAT_API int scdat_get_particles(scdat_ctx* ctx, int32_t species, int64_t capacity, double* x, double* v,
+                                  int32_t* tet, uint8_t* status, uint32_t* ids, int64_t* n_out)
+{
+    if (!ctx) return SCDAT_ERR_ARG;
+    ARG(species >= 0 && species < (int)ctx->species.size(), "bad species index");
+    SpeciesState& S = ctx->species[species];
+    const int64_t n = S.n;
+    if (n_out) *n_out = n;
+    ARG(capacity >= n, "capacity smaller than the particle count");
+    if (n == 0) return SCDAT_OK;
+    std::vector<double> cx((size_t)n), cy((size_t)n), cz((size_t)n), wx((size_t)n), wy((size_t)n), wz((size_t)n);
+    std::vector<int32_t> t((size_t)n);
+    std::vector<uint32_t> id((size_t)n);
+    if (ctx->mixed) {
+        DBuf<double> dx, dy, dz, dvx, dvy, dvz;
+        for (DBuf<double>* a : {&dx, &dy, &dz, &dvx, &dvy, &dvz}) CK(a->alloc((size_t)n));
+        launch_from_mixed(ctx->mv, n, store_of(ctx, species), dx.p, dy.p, dz.p, dvx.p, dvy.p, dvz.p, ctx->st);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(cx.data(), dx.p, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaMemcpyAsync(cy.data(), dy.p, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaMemcpyAsync(cz.data(), dz.p, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaMemcpyAsync(wx.data(), dvx.p, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaMemcpyAsync(wy.data(), dvy.p, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaMemcpyAsync(wz.data(), dvz.p, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+    } else {
+        CK(cudaMemcpyAsync(cx.data(), S.x.p, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaMemcpyAsync(cy.data(), S.y.p, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaMemcpyAsync(cz.data(), S.z.p, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaMemcpyAsync(wx.data(), S.vx.p, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaMemcpyAsync(wy.data(), S.vy.p, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaMemcpyAsync(wz.data(), S.vz.p, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->st));
+    }
+    CK(cudaMemcpyAsync(t.data(), S.tet.p, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaMemcpyAsync(id.data(), S.id.p, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    for (int64_t i = 0; i < n; ++i) {
+        if (x) { x[3 * i] = cx[i]; x[3 * i + 1] = cy[i]; x[3 * i + 2] = cz[i]; }
+        if (v) { v[3 * i] = wx[i]; v[3 * i + 1] = wy[i]; v[3 * i + 2] = wz[i]; }
+        if (tet) tet[i] = t[i];
+        if (status) status[i] = t[i] >= kTetNoHint ? SCDAT_ACTIVE : (t[i] == kTetAbsorbed ? SCDAT_ABSORBED : SCDAT_ESCAPED);
+        if (ids) ids[i] = id[i];
+    }
+    return SCDAT_OK;
+}
+
+SCDAT_API int scdat_kuhn_box_mesh(int32_t nx, int32_t ny, int32_t nz, double h, const int32_t* body_lo,
+                                  const int32_t* body_hi, double bias, double wall, int64_t* n_nodes, int64_t* n_tets,
+                                  double* node_xyz, int32_t* tet_nodes, uint8_t* node_dirichlet, double* node_phi,
+                                  int32_t* hex_ijk, int64_t* n_cells)
+{
+    if (nx <= 0 || ny <= 0 || nz <= 0 || !(h > 0.0) || !n_nodes || !n_tets) return SCDAT_ERR_ARG;
+    std::vector<double> xyz, phi;
+    std::vector<int32_t> tet, hex;
+    std::vector<uint8_t> dir;
+    build_kuhn_box(nx, ny, nz, h, body_lo, body_hi, bias, wall, xyz, tet, dir, phi, hex);
+    *n_nodes = (int64_t)dir.size();
+    *n_tets = (int64_t)(tet.size() / 4);
+    if (n_cells) *n_cells = (int64_t)(hex.size() / 3);
+    if (node_xyz) std::memcpy(node_xyz, xyz.data(), sizeof(double) * xyz.size());
+    if (tet_nodes) std::memcpy(tet_nodes, tet.data(), sizeof(int32_t) * tet.size());
+    if (node_dirichlet) std::memcpy(node_dirichlet, dir.data(), dir.size());
+    if (node_phi) std::memcpy(node_phi, phi.data(), sizeof(double) * phi.size());
+    if (hex_ijk) std::memcpy(hex_ijk, hex.data(), sizeof(int32_t) * hex.size());
+    return SCDAT_OK;
+}
+
+SCDAT_API int scdat_seed_box_particles(scdat_ctx* ctx, int32_t species, int32_t nx, int32_t ny, int32_t nz, double h,
+                                       const int32_t* body_lo, const int32_t* body_hi, int32_t n_per_cell,
+                                       double temp_ev, uint64_t seed)
+{
+    if (!ctx) return SCDAT_ERR_ARG;
+    ARG(species >= 0 && species < (int)ctx->species.size(), "bad species index");
+    ARG(n_per_cell > 0 && temp_ev >= 0.0, "bad seeding parameters");
+    std::vector<double> xyz, phi;
+    std::vector<int32_t> tet, hex;
+    std::vector<uint8_t> dir;
+    build_kuhn_box(nx, ny, nz, h, body_lo, body_hi, 0.0, 0.0, xyz, tet, dir, phi, hex);
+    ARG((int64_t)(tet.size() / 4) == ctx->hm.T && (int64_t)dir.size() == ctx->hm.N,
+        "mesh is not the Kuhn box of these dimensions");
+    const int64_t ncell = (int64_t)(hex.size() / 3);
+    const int64_t n = ncell * n_per_cell;
+    ARG(n < (int64_t)0xffffffffLL, "too many particles for 32-bit ids");
+    int rc = alloc_species(ctx, species, n);
+    if (rc) return rc;
+    DBuf<int32_t> dh;
+    CK(dh.upload(hex.data(), hex.size(), ctx->st));
+    const SpeciesState& S = ctx->species[species];
+    double sigma = std::sqrt(temp_ev * 1.602176634e-19 / S.sp.mass);
+    launch_seed_box(dh.p, ncell, n_per_cell, (int32_t)ctx->species.size(), species, h, sigma, seed,
+                    store_of(ctx, species), ctx->mixed, ctx->mv, ctx->st);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(ctx->st));
+    return SCDAT_OK;
+}
+
+SCDAT_API int scdat_set_potential(scdat_ctx* ctx, const double* phi)
+{
+    if (!ctx) return SCDAT_ERR_ARG;
+    ARG(phi, "null potential");
+    CK(cudaMemcpyAsync(ctx->phi.p, phi, sizeof(double) * ctx->hm.N, cudaMemcpyHostToDevice, ctx->st));
+    int rc = do_lsq(ctx, 1.0e-18);  // PICCycle's own LSQ regularisation (PICCycle.cpp:208)
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(ctx->st));
+    return SCDAT_OK;
+}
+
+SCDAT_API int scdat_set_node_potentials(scdat_ctx* ctx, int64_t n, const int64_t* nodes, const double* values)
+{
+    if (!ctx) return SCDAT_ERR_ARG;
+    ARG(n >= 0 && (n == 0 || (nodes && values)), "bad node arrays");
+    if (n == 0) return SCDAT_OK;
+    for (int64_t i = 0; i < n; ++i) ARG(nodes[i] >= 0 && nodes[i] < ctx->hm.N, "node index out of range");
+    DBuf<int64_t> di;
+    DBuf<double> dv;
+    CK(di.upload(nodes, (size_t)n, ctx->st));
+    CK(dv.upload(values, (size_t)n, ctx->st));
+    launch_scatter_values(n, di.p, dv.p, ctx->phi.p, ctx->st);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(ctx->st));
+    return SCDAT_OK;
+}
+
+SCDAT_API int scdat_set_electric_field(scdat_ctx* ctx, const double* E)
+{
+    if (!ctx) return SCDAT_ERR_ARG;
+    ARG(E, "null field");
+    const int64_t n3 = 3 * ctx->hm.N;
+    CK(cudaMemcpyAsync(ctx->E.p, E, sizeof(double) * n3, cudaMemcpyHostToDevice, ctx->st));
+    std::vector<float> f((size_t)n3);
+    for (int64_t i = 0; i < n3; ++i) f[i] = (float)E[i];
+    CK(cudaMemcpyAsync(ctx->Ef.p, f.data(), sizeof(float) * n3, cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return SCDAT_OK;
+}
+
+SCDAT_API int scdat_set_elastic_mcc(scdat_ctx* ctx, int32_t species, const scdat_elastic* proc)
+{
+    if (!ctx) return SCDAT_ERR_ARG;
+    ARG(species >= 0 && species < (int)ctx->species.size(), "bad species index");
+    ARG(proc && proc->target_density >= 0.0 && proc->sigma_max >= 0.0, "bad collision process");
+    ctx->species[species].mcc = *proc;
+    return SCDAT_OK;
+}
+
+SCDAT_API int scdat_push(scdat_ctx* ctx)
+{
+    if (!ctx) return SCDAT_ERR_ARG;
+    int rc = do_push(ctx, false);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(ctx->st));
+    return check_flags(ctx);
+}
+
+SCDAT_API int scdat_solve_field(scdat_ctx* ctx)
+{
+    if (!ctx) return SCDAT_ERR_ARG;
+    int rc = do_solve_field(ctx);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(ctx->st));
+    if (ctx->last_pcg_iter >= ctx->prm.pcg_max_iter && ctx->last_pcg_rel > ctx->prm.pcg_rtol) {
+        ctx->err = "field solve reached its iteration cap";
+        return SCDAT_ERR_NOT_CONVERGED;
+    }
+    return SCDAT_OK;
+}
+
+SCDAT_API int scdat_collide(scdat_ctx* ctx)
+{
+    if (!ctx) return SCDAT_ERR_ARG;
+    PushParams pp = push_params(ctx, true);
+    for (int s = 0; s < (int)ctx->species.size(); ++s) {
+        if (!ctx->species[s].mcc.enabled || ctx->species[s].cap == 0) continue;
+        if (ctx->mixed)
+            launch_mcc_mixed(store_of(ctx, s), species_dev(ctx, s), pp, ctx->led.p, ctx->grid_push, ctx->st);
+        else
+            launch_mcc_f64(store_of(ctx, s), species_dev(ctx, s), pp, ctx->led.p, ctx->grid_push, ctx->st);
+    }
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(ctx->st));
+    return SCDAT_OK;
+}
+
+SCDAT_API int scdat_compact(scdat_ctx* ctx)
+{
+    if (!ctx) return SCDAT_ERR_ARG;
+    for (int s = 0; s < (int)ctx->species.size(); ++s) {
+        int rc = do_sort(ctx, s);
+        if (rc) return rc;
+    }
+    return SCDAT_OK;
+}
+
+SCDAT_API int scdat_step(scdat_ctx* ctx, int32_t n_steps)
+{
+    if (!ctx) return SCDAT_ERR_ARG;
+    ARG(n_steps >= 0, "negative step count");
+    for (int k = 0; k < n_steps; ++k) {
+        int rc = do_push(ctx, true);
+        if (rc) return rc;
+        rc = do_solve_field(ctx);
+        if (rc) return rc;
+        ctx->steps += 1;
+        ctx->sim_time += ctx->prm.dt;
+        if (ctx->prm.sort_interval > 0 && ctx->steps % ctx->prm.sort_interval == 0) {
+            rc = scdat_compact(ctx);
+            if (rc) return rc;
+        }
+    }
+    CK(cudaStreamSynchronize(ctx->st));
+    return check_flags(ctx);
+}
+
+SCDAT_API int scdat_get_fields(scdat_ctx* ctx, double* rho, double* phi, double* E)
+{
+    if (!ctx) return SCDAT_ERR_ARG;
+    const int64_t N = ctx->hm.N;
+    if (rho) CK(cudaMemcpyAsync(rho, ctx->rho.p, sizeof(double) * N, cudaMemcpyDeviceToHost, ctx->st));
+    if (phi) CK(cudaMemcpyAsync(phi, ctx->phi.p, sizeof(double) * N, cudaMemcpyDeviceToHost, ctx->st));
+    if (E) CK(cudaMemcpyAsync(E, ctx->E.p, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return SCDAT_OK;
+}
+
+SCDAT_API int scdat_get_species_charge(scdat_ctx* ctx, int32_t species, double* rho_s)
+{
+    if (!ctx) return SCDAT_ERR_ARG;
+    ARG(species >= 0 && species < (int)ctx->species.size() && rho_s, "bad species index");
+    const int64_t N = ctx->hm.N;
+    launch_species_rho(N, ctx->acc_lo.p + species * N, ctx->acc_hi.p + species * N, ctx->uq, ctx->tmp_rho.p,
+                       ctx->grid_nodes, ctx->st);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(rho_s, ctx->tmp_rho.p, sizeof(double) * N, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return SCDAT_OK;
+}
+
+SCDAT_API int scdat_get_ledger(scdat_ctx* ctx, double* ledger)
+{
+    if (!ctx || !ledger) return SCDAT_ERR_ARG;
+    LedgerDev h{};
+    CK(cudaMemcpyAsync(&h, ctx->led.p, sizeof(h), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    for (int f = 0; f < 7; ++f) {
+        double* r = ledger + 8 * f;
+        r[0] = fx_to_double(h.row[f][0], (long long)h.row[f][1], ctx->uq);
+        r[1] = fx_to_double(h.row[f][2], (long long)h.row[f][3], ctx->uq);
+        r[2] = 0.0;
+        r[3] = fx_to_double(h.row[f][4], (long long)h.row[f][5], ctx->ue);
+        r[4] = (double)h.row[f][6];
+        r[5] = (double)h.row[f][7];
+        r[6] = 0.0;
+        r[7] = 0.0;
+    }
+    return SCDAT_OK;
+}
+
+SCDAT_API int scdat_reset_ledger(scdat_ctx* ctx)
+{
+    if (!ctx) return SCDAT_ERR_ARG;
+    CK(cudaMemsetAsync(ctx->led.p->row, 0, sizeof(ctx->led.p->row), ctx->st));
+    CK(cudaMemsetAsync(&ctx->led.p->surf_lo, 0, 2 * sizeof(unsigned long long), ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return SCDAT_OK;
+}
+
+SCDAT_API void* scdat_stream(scdat_ctx* ctx) { return ctx ? (void*)ctx->st : nullptr; }
+
+SCDAT_API int scdat_set_timing(scdat_ctx* ctx, int32_t enable)
+{
+    if (!ctx) return SCDAT_ERR_ARG;
+    int rc = harvest_timing(ctx);
+    if (rc) return rc;
+    ctx->timing = enable != 0;
+    ctx->push_ms = ctx->field_ms = 0.0;
+    ctx->push_launches = ctx->field_solves = ctx->push_particles = ctx->launches = 0;
+    return SCDAT_OK;
+}
+
+SCDAT_API int scdat_get_timing(scdat_ctx* ctx, double* push_ms, int64_t* push_launches, int64_t* push_particles,
+                               double* field_ms, int64_t* field_solves, int64_t* kernel_launches)
+{
+    if (!ctx) return SCDAT_ERR_ARG;
+    int rc = harvest_timing(ctx);
+    if (rc) return rc;
+    if (push_ms) *push_ms = ctx->push_ms;
+    if (push_launches) *push_launches = ctx->push_launches;
+    if (push_particles) *push_particles = ctx->push_particles;
+    if (field_ms) *field_ms = ctx->field_ms;
+    if (field_solves) *field_solves = ctx->field_solves;
+    if (kernel_launches) *kernel_launches = ctx->launches;
+    return SCDAT_OK;
+}
+
+SCDAT_API int scdat_get_statistics(scdat_ctx* ctx, scdat_stats* st)
+{
+    if (!ctx || !st) return SCDAT_ERR_ARG;
+    LedgerDev h{};
+    std::vector<double> ke((size_t)ctx->grid_push);
+    unsigned long long tq[2] = {0, 0};
+    CK(cudaMemcpyAsync(&h, ctx->led.p, sizeof(h), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaMemcpyAsync(ke.data(), ctx->ke_part.p, sizeof(double) * ke.size(), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaMemcpyAsync(tq, ctx->totq.p, sizeof(tq), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    std::memset(st, 0, sizeof(*st));
+    st->completed_steps = ctx->steps;
+    st->simulation_time = ctx->sim_time;
+    st->total_charge = fx_to_double(tq[0], (long long)tq[1], ctx->uq);
+    double e = 0.0;
+    for (double k : ke) e += k;
+    st->total_energy = e;
+    st->active_particles = (int64_t)h.active;
+    int64_t stored = 0;
+    for (auto& S : ctx->species) stored += S.n;
+    st->stored_particles = stored;
+    st->surface_deposited_charge = fx_to_double(h.surf_lo, (long long)h.surf_hi, ctx->uq);
+    st->substeps = (int64_t)h.substeps;
+    st->lost_events = (int64_t)h.lost_events;
+    st->mcc_collisions = (int64_t)h.mcc_hits;
+    st->last_pcg_iterations = ctx->last_pcg_iter;
+    st->last_pcg_relres = ctx->last_pcg_rel;
+    return SCDAT_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,164 @@
+// common.cuh -- device-side building blocks shared by the PIC-MCC kernels.
+//
+//  * 128-bit two's-complement fixed point accumulated with two 64-bit integer atomics, so
+//    charge and ledger sums are exact and independent of thread order (deterministic).
+//  * Philox4x32-10 counter-based RNG (Salmon et al., SC'11), keyed by (seed) with counter
+//    (particle id, step, purpose): every particle owns its random stream.
+//  * Flat views of the mesh, fields and particle store that the kernels take by value.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace scdat {
+
+// ------------------------------------------------------------------------------------
+// Fixed point: value = (hi * 2^64 + lo) * 2^-64 * unit, hi signed, lo unsigned.
+// ------------------------------------------------------------------------------------
+struct Fx128 {
+    unsigned long long lo;
+    long long hi;
+};
+
+__host__ __device__ inline Fx128 fx_from_double(double v)
+{
+    // v is already divided by the unit (a power of two, so the division is exact).
+    double fl = floor(v);
+    Fx128 r;
+    r.hi = (long long)fl;
+    double frac = v - fl;  // exact, in [0, 1)
+#ifdef __CUDA_ARCH__
+    r.lo = __double2ull_rz(frac * 18446744073709551616.0);
+#else
+    r.lo = (unsigned long long)(frac * 18446744073709551616.0);
+#endif
+    return r;
+}
+
+__host__ __device__ inline void fx_add(Fx128& a, const Fx128& b)
+{
+    unsigned long long lo = a.lo + b.lo;
+    a.hi += b.hi + (lo < a.lo ? 1 : 0);
+    a.lo = lo;
+}
+
+__host__ __device__ inline double fx_to_double(unsigned long long lo, long long hi, double unit)
+{
+    return (double)hi * unit + (double)lo * (unit * 5.421010862427522170037264e-20);  // 2^-64
+}
+
+__device__ inline void fx_atomic_add(unsigned long long* lo_acc, unsigned long long* hi_acc, const Fx128& v)
+{
+    if (v.lo == 0ull && v.hi == 0ll) return;
+    unsigned long long old = atomicAdd(lo_acc, v.lo);
+    unsigned long long carry = (old + v.lo < old) ? 1ull : 0ull;
+    unsigned long long h = (unsigned long long)v.hi + carry;
+    if (h) atomicAdd(hi_acc, h);
+}
+
+// ------------------------------------------------------------------------------------
+// Philox4x32-10
+// ------------------------------------------------------------------------------------
+__host__ __device__ inline void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1)
+{
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        if (r > 0) {
+            k0 += 0x9E3779B9u;
+            k1 += 0xBB67AE85u;
+        }
+        uint64_t p0 = (uint64_t)0xD2511F53u * c[0];
+        uint64_t p1 = (uint64_t)0xCD9E8D57u * c[2];
+        uint32_t n0 = (uint32_t)(p1 >> 32) ^ c[1] ^ k0;
+        uint32_t n1 = (uint32_t)p1;
+        uint32_t n2 = (uint32_t)(p0 >> 32) ^ c[3] ^ k1;
+        uint32_t n3 = (uint32_t)p0;
+        c[0] = n0; c[1] = n1; c[2] = n2; c[3] = n3;
+    }
+}
+
+// Two (0,1) doubles with 53-bit resolution for (seed; id, step, purpose).
+__host__ __device__ inline void uniform2(uint64_t seed, uint64_t id, uint32_t step, uint32_t purpose, double& u0,
+                                         double& u1)
+{
+    uint32_t c[4] = {(uint32_t)id, (uint32_t)(id >> 32), step, purpose};
+    philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+    uint64_t m0 = (((uint64_t)c[0] << 21) ^ (uint64_t)(c[1] >> 11)) & ((1ull << 53) - 1);
+    uint64_t m1 = (((uint64_t)c[2] << 21) ^ (uint64_t)(c[3] >> 11)) & ((1ull << 53) - 1);
+    u0 = ((double)m0 + 0.5) * (1.0 / 9007199254740992.0);
+    u1 = ((double)m1 + 0.5) * (1.0 / 9007199254740992.0);
+}
+
+// ------------------------------------------------------------------------------------
+// Device views
+// ------------------------------------------------------------------------------------
+constexpr double kBaryEps = 1e-8;        // PICParticleAlgorithms.cpp:286
+constexpr double kMinTimeStep = 1e-20;   // PICParticleAlgorithms.cpp:583
+constexpr int kMaxSubsteps = 100000;     // PICParticleAlgorithms.cpp:584
+constexpr int kWalkSteps = 64;           // neighbour-walk cap before the grid lookup
+
+// tet[] encoding of particle state: >= 0 active with that tet as location hint,
+// -1 active without a hint, kTetAbsorbed / kTetEscaped inactive.
+constexpr int32_t kTetNoHint = -1;
+constexpr int32_t kTetAbsorbed = -2;
+constexpr int32_t kTetEscaped = -3;
+
+struct MeshView {
+    int64_t N, T;
+    const double* xyz;       // [N*3]
+    const int4* tet;         // [T]
+    const int4* nbr;         // [T] neighbour across the face opposite local vertex f
+    const double* geom;      // [T*12] inverse Jacobian (row-major 3x3) then origin node xyz
+    const float* geomf;      // [T*12] the same in FP32 (mixed form), origin-relative
+    // locate grid: uniform bins over the bounding box, tets listed by ascending id
+    double gmin[3];
+    double ginv[3];
+    int32_t gdim[3];
+    double gdelta;           // query half-width covering the containment tolerance
+    const int32_t* bin_start;
+    const int32_t* bin_tets;
+    double bmin[3], bmax[3];  // domain bounds (PICCycle.cpp:1039-1066)
+    int32_t use_nbr;
+};
+
+struct LedgerDev {
+    // 7 rows x {qe_lo, qe_hi, qi_lo, qi_hi, en_lo, en_hi, n_e, n_i}
+    unsigned long long row[7][8];
+    unsigned long long surf_lo, surf_hi;     // surface_deposited_charge
+    unsigned long long substeps, lost_events, mcc_hits, active;
+    unsigned long long flags;                // device error flag word
+    unsigned long long pad[5];
+};
+
+enum DeviceFlag : unsigned long long {
+    kFlagBadTet = 1ull << 0,
+    kFlagPcgNotConverged = 1ull << 1,
+};
+
+struct SpeciesDev {
+    double q, m, w, qm;
+    double cw_seg;       // (q / nseg) * w, the reference's per-point charge weight
+    int32_t electron_like;
+    int32_t mcc_enabled;
+    int32_t mcc_mode;
+    int32_t pad;
+    double mcc_n, mcc_sigma, mcc_eref, mcc_alpha, mcc_eth;
+};
+
+struct PushParams {
+    double dt;
+    double floor_ratio;
+    int32_t nseg;
+    int32_t dep_kernel;
+    int32_t face_bc[6];
+    double period[3];
+    int32_t body_tally;
+    int32_t do_mcc;
+    double otol, ntol;
+    double inv_uq, inv_ue;   // 1 / fixed-point units for charge and energy
+    uint64_t seed;
+    uint32_t step;
+    int32_t deposit;
+};
+
+}  // namespace scdat

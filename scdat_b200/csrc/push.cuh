@@ -1,0 +1,263 @@
+// push.cuh -- device functions of the particle path: barycentric containment, locate,
+// boundary events, MCC.  Shared by the FP64 and the mixed-precision push kernels.
+#pragma once
+
+#include "common.cuh"
+
+namespace scdat {
+
+struct ParticleStore {
+    // FP64 form: absolute positions.  Mixed form: xf/yf/zf hold float offsets from the
+    // origin node of the particle's tet and vxf/vyf/vzf float velocities.
+    double *x, *y, *z, *vx, *vy, *vz;
+    float *xf, *yf, *zf, *vxf, *vyf, *vzf;
+    int32_t* tet;
+    uint32_t* id;
+    const int64_t* count;  // device-resident particle count of this species
+};
+
+__device__ __forceinline__ bool bary_inside(const double lam[4])
+{
+    bool ok = true;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) ok = ok && (lam[i] >= -kBaryEps) && (lam[i] <= 1.0 + kBaryEps);
+    return ok;  // false for NaN (degenerate tets store NaN geometry)
+}
+
+// Barycentric coordinates of p in tet t from the precomputed inverse Jacobian
+// (equivalent, up to rounding, to the signed-volume ratios of
+// FieldInterpolator::isPointInTetrahedron, PICParticleAlgorithms.cpp:247-296).
+__device__ __forceinline__ bool bary64(const MeshView& M, int t, double px, double py, double pz, double lam[4])
+{
+    const double2* g2 = reinterpret_cast<const double2*>(M.geom + 12 * (int64_t)t);
+    double2 a = __ldg(g2 + 0), b = __ldg(g2 + 1), c = __ldg(g2 + 2), d = __ldg(g2 + 3), e = __ldg(g2 + 4),
+            f = __ldg(g2 + 5);
+    double dx = px - e.y, dy = py - f.x, dz = pz - f.y;
+    lam[1] = a.x * dx + a.y * dy + b.x * dz;
+    lam[2] = b.y * dx + c.x * dy + c.y * dz;
+    lam[3] = d.x * dx + d.y * dy + e.x * dz;
+    lam[0] = 1.0 - lam[1] - lam[2] - lam[3];
+    return bary_inside(lam);
+}
+
+// Lowest-id tet containing p among the grid candidates (exactly the result of the
+// reference's linear scan, PICParticleAlgorithms.cpp:882-888), or -1.
+__device__ inline int grid_lookup(const MeshView& M, double px, double py, double pz)
+{
+    double p[3] = {px, py, pz};
+    int lo[3], hi[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        double l = (p[a] - M.gdelta - M.gmin[a]) * M.ginv[a];
+        double h = (p[a] + M.gdelta - M.gmin[a]) * M.ginv[a];
+        if (!(h >= 0.0) || !(l < (double)M.gdim[a])) return -1;  // outside the grid (or NaN)
+        lo[a] = l < 0.0 ? 0 : (int)l;
+        hi[a] = h >= (double)M.gdim[a] ? M.gdim[a] - 1 : (int)h;
+    }
+    int best = 0x7fffffff;
+    double lam[4];
+    for (int k = lo[2]; k <= hi[2]; ++k)
+        for (int j = lo[1]; j <= hi[1]; ++j)
+            for (int i = lo[0]; i <= hi[0]; ++i) {
+                int b = i + M.gdim[0] * (j + M.gdim[1] * k);
+                int s = __ldg(M.bin_start + b), e = __ldg(M.bin_start + b + 1);
+                for (int q = s; q < e; ++q) {
+                    int t = __ldg(M.bin_tets + q);
+                    if (t >= best) break;
+                    if (bary64(M, t, px, py, pz, lam)) {
+                        best = t;
+                        break;
+                    }
+                }
+            }
+    return best == 0x7fffffff ? -1 : best;
+}
+
+// After the hint and its neighbour list fail: walk across the most violated face from
+// `start`; accept a tet whose barycentrics all clear 1e-6 (no other tet can hold the point
+// within the 1e-8 tolerance then), otherwise fall back to the exact grid lookup.
+__device__ inline int locate_far(const MeshView& M, double px, double py, double pz, int start)
+{
+    double lam[4];
+    int t = start;
+    if (t >= 0) {
+        for (int k = 0; k < kWalkSteps; ++k) {
+            bool in = bary64(M, t, px, py, pz, lam);
+            double mn = fmin(fmin(lam[0], lam[1]), fmin(lam[2], lam[3]));
+            if (in) {
+                if (mn >= 1e-6) return t;
+                break;
+            }
+            if (!(mn == mn)) break;  // NaN: degenerate tet
+            int f = 0;
+#pragma unroll
+            for (int i = 1; i < 4; ++i)
+                if (lam[i] < lam[f]) f = i;
+            int4 nb = __ldg(M.nbr + t);
+            int nt = f == 0 ? nb.x : (f == 1 ? nb.y : (f == 2 ? nb.z : nb.w));
+            if (nt < 0) break;
+            t = nt;
+        }
+    }
+    return grid_lookup(M, px, py, pz);
+}
+
+// CrossTetrahedron::locateParticle semantics (PICParticleAlgorithms.cpp:853-891).
+__device__ __forceinline__ int locate(const MeshView& M, double px, double py, double pz, int hint)
+{
+    double lam[4];
+    if (hint >= 0) {
+        if (bary64(M, hint, px, py, pz, lam)) return hint;
+        if (M.use_nbr) {
+            int4 nb = __ldg(M.nbr + hint);
+            if (nb.x >= 0 && bary64(M, nb.x, px, py, pz, lam)) return nb.x;
+            if (nb.y >= 0 && bary64(M, nb.y, px, py, pz, lam)) return nb.y;
+            if (nb.z >= 0 && bary64(M, nb.z, px, py, pz, lam)) return nb.z;
+            if (nb.w >= 0 && bary64(M, nb.w, px, py, pz, lam)) return nb.w;
+        }
+    }
+    return locate_far(M, px, py, pz, hint);
+}
+
+// PICCycle::detectBoundaryFace, PICCycle.cpp:1074-1133.
+__device__ inline int detect_face(const MeshView& M, double px, double py, double pz, double otol, bool near,
+                                  double ntol)
+{
+    if (px < M.bmin[0] - otol) return 0;
+    if (px > M.bmax[0] + otol) return 1;
+    if (py < M.bmin[1] - otol) return 2;
+    if (py > M.bmax[1] + otol) return 3;
+    if (pz < M.bmin[2] - otol) return 4;
+    if (pz > M.bmax[2] + otol) return 5;
+    if (!near) return -1;
+    double d[6] = {fabs(px - M.bmin[0]), fabs(px - M.bmax[0]), fabs(py - M.bmin[1]),
+                   fabs(py - M.bmax[1]), fabs(pz - M.bmin[2]), fabs(pz - M.bmax[2])};
+    int best = -1;
+    double bd = 1.79769313486231570815e+308;
+#pragma unroll
+    for (int f = 0; f < 6; ++f)
+        if (d[f] <= ntol && d[f] < bd) {
+            best = f;
+            bd = d[f];
+        }
+    return best;
+}
+
+__device__ inline void ledger_tally(LedgerDev* L, int row, const SpeciesDev& S, const PushParams& pp, double ke,
+                                    bool surface)
+{
+    double qw = S.q * S.w;
+    double en = ke * fmax(1.0, S.w);
+    Fx128 fq = fx_from_double(qw * pp.inv_uq);
+    Fx128 fe = fx_from_double(en * pp.inv_ue);
+    fx_atomic_add(&L->row[row][4], &L->row[row][5], fe);
+    if (S.electron_like) {
+        fx_atomic_add(&L->row[row][0], &L->row[row][1], fq);
+        atomicAdd(&L->row[row][6], 1ull);
+    } else if (S.q > 0.0) {
+        fx_atomic_add(&L->row[row][2], &L->row[row][3], fq);
+        atomicAdd(&L->row[row][7], 1ull);
+    }
+    if (surface) fx_atomic_add(&L->surf_lo, &L->surf_hi, fq);
+}
+
+// PICCycle::applyRuntimeBoundaryCondition + processRuntimeBoundaryEvents for one lost
+// particle (PICCycle.cpp:1221-1379).  Updates position (periodic wrap) and returns the new
+// tet code (>= 0 active, kTetAbsorbed, kTetEscaped).
+__device__ inline int resolve_lost(const MeshView& M, const SpeciesDev& S, const PushParams& pp, LedgerDev* L, double& px,
+                            double& py, double& pz, double ke, int hint)
+{
+    int resolved = -1;
+    int status = 0;  // 0 active, 1 absorbed, 2 escaped
+    bool ok = false, done = false;
+    for (int pass = 0; pass < 6 && !done; ++pass) {
+        int f = detect_face(M, px, py, pz, pp.otol, pass == 0, pp.ntol);
+        if (f < 0) {
+            resolved = locate(M, px, py, pz, hint);
+            ok = resolved >= 0;
+            done = true;
+            break;
+        }
+        int bc = pp.face_bc[f];
+        if (bc == 0) {
+            ok = false;
+            done = true;
+            break;
+        }
+        if (bc == 1) {
+            status = 1;
+            ledger_tally(L, f, S, pp, ke, true);
+            ok = true;
+            done = true;
+            break;
+        }
+        // periodic: PeriodicBoundaryCondition::mapPeriodicPosition (BoundaryConditions.cpp:93-140)
+        double c[3] = {px, py, pz};
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            double Lp = pp.period[a];
+            if (Lp <= 1e-12) continue;
+            c[a] = fmod(c[a], Lp);
+            if (c[a] < 0.0) c[a] += Lp;
+        }
+        px = c[0]; py = c[1]; pz = c[2];
+        int h2 = locate(M, px, py, pz, hint);
+        hint = h2;
+        if (h2 >= 0) resolved = h2;
+    }
+    if (!done) {
+        resolved = locate(M, px, py, pz, hint);
+        ok = resolved >= 0;
+    }
+    if (!ok) status = 2;
+    if (status == 0 && resolved < 0) status = 2;
+    if (status == 2 && pp.body_tally) {
+        if (detect_face(M, px, py, pz, pp.otol, false, 0.0) < 0) ledger_tally(L, 6, S, pp, ke, false);
+    }
+    if (status == 1) return kTetAbsorbed;
+    if (status == 2) return kTetEscaped;
+    return resolved;
+}
+
+// ElasticCollisionCrossSection::calculateCrossSection, CollisonTypes.cpp:60-78.
+__device__ inline double sigma_elastic(const SpeciesDev& S, double e_ev)
+{
+    if (!(e_ev >= S.mcc_eth)) return 0.0;
+    double eref = S.mcc_eref > 1e-6 ? S.mcc_eref : 1e-6;
+    double s = S.mcc_alpha == 0.0 ? S.mcc_sigma : S.mcc_sigma * pow(eref / e_ev, S.mcc_alpha);
+    s = fmin(s, S.mcc_sigma);
+    return s > 0.0 ? s : 0.0;
+}
+
+// MonteCarloCollisionHandler::processCollisions for one elastic process
+// (CollisionAlgorithm.cpp:500-538, 189-210) with Philox streams (seed; id, step, 2|3).
+__device__ inline bool mcc_elastic(const SpeciesDev& S, const PushParams& pp, uint32_t pid, double& vx, double& vy,
+                                   double& vz)
+{
+    const double qe = 1.602176634e-19;
+    double speed = sqrt(vx * vx + vy * vy + vz * vz);
+    double e_ev = 0.5 * S.m * speed * speed / qe;
+    double nu = S.mcc_n * sigma_elastic(S, e_ev) * speed;
+    double u0, u1;
+    uniform2(pp.seed, pid, pp.step, 2u, u0, u1);
+    bool hit;
+    if (S.mcc_mode == 0) {
+        double p = fmin(fmax(nu * pp.dt, 0.0), 1.0);
+        hit = (u0 < p) && !(u1 >= p);
+    } else {
+        double p = 1.0 - exp(-nu * pp.dt);
+        hit = u0 < p;
+    }
+    if (!hit) return false;
+    double w0, w1;
+    uniform2(pp.seed, pid, pp.step, 3u, w0, w1);
+    double theta = acos(-1.0 + 2.0 * w0);
+    double phi = 6.283185307179586476925286766559 * w1;
+    double st = sin(theta);
+    vx = speed * st * cos(phi);
+    vy = speed * st * sin(phi);
+    vz = speed * cos(theta);
+    return true;
+}
+
+}  // namespace scdat

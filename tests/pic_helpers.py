@@ -1,0 +1,71 @@
+"""Shared drivers for the parity tests: the oracle's PIC cycle in the reference's order
+(PICCycle::executeTimeStep, Tools/PICcore/src/PICCycle.cpp:311-416) and the same cycle on
+the CUDA library through its C ABI."""
+import numpy as np
+
+import oracle as O
+
+
+def oracle_cycle(o, mesh, sp, parts, nsteps, dt, face_bc, phi0, neighbors=True, rtol=1e-15, body_tally=False):
+    A = o.assemble(mesh)
+    E = o.lsq(mesh, A, phi0, reg=1e-18)
+    L = mesh.xyz.max(axis=0) - mesh.xyz.min(axis=0)
+    period = tuple(L[a] if (face_bc[2 * a] == 2 or face_bc[2 * a + 1] == 2) else 0.0 for a in range(3))
+    st = dict(x=parts["x"].copy(), v=parts["v"].copy(), tet=parts["tet"].copy(),
+              status=np.zeros(len(parts["tet"]), np.uint8))
+    phi = phi0.copy()
+    ledger = np.zeros((7, 8))
+    sc = 0.0
+    rho = np.zeros(mesh.N)
+    substeps = 0
+    for _ in range(nsteps):
+        out = o.push(mesh, E, dict(parts, x=st["x"], v=st["v"], tet=st["tet"]), sp, dt, status=st["status"],
+                     neighbors=neighbors)
+        out = o.boundary(mesh, out, parts, sp, face_bc, period=period, neighbors=neighbors, body_tally=body_tally)
+        ledger += out["ledger"]
+        sc += out["surface_charge"]
+        substeps += out["substeps"]
+        st = dict(x=out["x"], v=out["v"], tet=out["tet"], status=out["status"])
+        rho = out["rho"]
+        phi, _, _ = o.poisson(mesh, A, rho, mesh.phi_bc, rtol=rtol, phi0=phi)
+        E = o.lsq(mesh, A, phi)
+    return dict(st, rho=rho, phi=phi, E=E, ledger=ledger, surface_charge=sc, substeps=substeps)
+
+
+def species_split(parts, s):
+    m = parts["species"] == s
+    return {k: (v[m] if isinstance(v, np.ndarray) and v.shape[:1] == m.shape else v) for k, v in parts.items()}
+
+
+def gpu_domain(mesh, dt, face_bc=(0,) * 6, precision=0, neighbors=True, **kw):
+    from scdat_b200 import capi
+
+    return capi.Domain(mesh.xyz, mesh.tet, mesh.dirichlet, dt, nbr=mesh.nbr, precision=precision, face_bc=face_bc,
+                       use_neighbor_lists=neighbors, **kw)
+
+
+def gpu_load_particles(dom, sp, parts):
+    """Species-major upload; returns the index map (device order -> oracle particle index)."""
+    dom.set_species(sp)
+    order = []
+    for s in range(len(sp)):
+        idx = np.nonzero(parts["species"] == s)[0]
+        dom.set_particles(s, parts["x"][idx], parts["v"][idx], parts["tet"][idx], parts["id"][idx].astype(np.uint32))
+        order.append(idx)
+    return order
+
+
+def gpu_state(dom, nspecies, nparts):
+    """Device particles scattered back into oracle particle order (by id)."""
+    x = np.full((nparts, 3), np.nan)
+    v = np.full((nparts, 3), np.nan)
+    tet = np.full(nparts, -9, np.int32)
+    status = np.full(nparts, 255, np.uint8)
+    for s in range(nspecies):
+        g = dom.get_particles(s)
+        ids = g["id"].astype(np.int64)
+        x[ids] = g["x"]
+        v[ids] = g["v"]
+        tet[ids] = g["tet"]
+        status[ids] = g["status"]
+    return dict(x=x, v=v, tet=tet, status=status)

@@ -1,0 +1,236 @@
+"""CUDA library (through its C ABI) against the reference fixtures and the C oracle.
+
+FP64 form: per-particle state and nodal fields within 1e-12 relative of the reference;
+tets, status and counters exact.  Mixed form: error against the FP64 form reported and
+bounded.  All inputs are the seeded small cases of tests/golden."""
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import rel_err
+from golden.make_golden import CASES, make_inputs
+from pic_helpers import gpu_domain, gpu_load_particles, gpu_state, oracle_cycle
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+TOL = 1e-12
+
+
+@pytest.fixture(params=sorted(CASES))
+def case(request, lib):
+    return request.param, np.load(os.path.join(GOLDEN, f"{request.param}.npz"))
+
+
+def test_push_matches_reference(case):
+    name, g = case
+    mesh, sp, parts, dt, nsteps, face_bc = make_inputs(name)
+    dom = gpu_domain(mesh, dt)
+    gpu_load_particles(dom, sp, parts)
+    dom.set_electric_field(g["E_laplace"])
+    dom.push()
+    st = gpu_state(dom, len(sp), len(parts["tet"]))
+    lost = g["push_lost"] == 1
+    assert np.array_equal(st["status"] != O.ACTIVE, lost)
+    assert np.array_equal(st["tet"][~lost], g["push_tet"][~lost])
+    assert np.abs(st["x"] - g["push_x"]).max() <= TOL * np.abs(g["push_x"]).max()
+    assert rel_err(st["v"], g["push_v"]) < TOL
+    rho, _, _ = dom.fields()
+    assert rel_err(rho, g["push_rho"]) < TOL
+    assert dom.stats()["substeps"] == int(g["push_substeps"])
+    dom.close()
+
+
+def test_push_species_charge_matches_oracle(case, orc):
+    name, g = case
+    mesh, sp, parts, dt, nsteps, face_bc = make_inputs(name)
+    dom = gpu_domain(mesh, dt)
+    gpu_load_particles(dom, sp, parts)
+    dom.set_electric_field(g["E_laplace"])
+    dom.push()
+    for s in range(len(sp)):
+        sub = {k: v[parts["species"] == s] for k, v in parts.items()}
+        ref_s = orc.push(mesh, g["E_laplace"], sub, sp, dt)["rho"]
+        assert rel_err(dom.species_charge(s), ref_s) < TOL
+    dom.close()
+
+
+def test_poisson_matches_reference(case):
+    name, g = case
+    mesh, sp, parts, dt, nsteps, face_bc = make_inputs(name)
+    dom = gpu_domain(mesh, dt, pcg_rtol=1e-15, pcg_max_iter=20000)
+    dom.set_species(sp)
+    dom.set_potential(mesh.phi_bc)
+    dom.solve_field(allow_not_converged=True)
+    _, phi, E = dom.fields()
+    assert rel_err(phi, g["phi_laplace"]) < TOL
+    assert rel_err(E, g["E_laplace"]) < TOL
+    dom.close()
+
+
+def test_full_cycle_matches_reference(case):
+    name, g = case
+    mesh, sp, parts, dt, nsteps, face_bc = make_inputs(name)
+    dom = gpu_domain(mesh, dt, face_bc=face_bc, pcg_rtol=1e-15, pcg_max_iter=20000, body_tally=False)
+    gpu_load_particles(dom, sp, parts)
+    dom.set_potential(g["phi_laplace"])
+    for _ in range(nsteps):
+        dom.step(1)
+    st = gpu_state(dom, len(sp), len(parts["tet"]))
+    ids = g["cyc_id"]
+    smap = {10: O.ACTIVE, 20: O.ABSORBED, 21: O.ESCAPED}
+    assert np.array_equal(st["status"][ids], np.array([smap[s] for s in g["cyc_status"]]))
+    act = g["cyc_status"] == 10
+    assert np.abs(st["x"][ids][act] - g["cyc_x"][act]).max() <= TOL * np.abs(g["cyc_x"]).max()
+    assert rel_err(st["v"][ids][act], g["cyc_v"][act]) < TOL
+    rho, phi, E = dom.fields()
+    assert rel_err(rho, g["cyc_rho"]) < TOL
+    assert rel_err(phi, g["cyc_phi"]) < TOL
+    assert rel_err(E, g["cyc_E"]) < TOL
+    led = dom.ledger()
+    assert np.array_equal(led[:6, 4:6], g["cyc_ledger"][:, 4:6])
+    np.testing.assert_allclose(led[:6, [0, 1, 3]], g["cyc_ledger"][:, [0, 1, 3]], rtol=TOL, atol=1e-30)
+    stt = dom.stats()
+    np.testing.assert_allclose(stt["surface_deposited_charge"], g["cyc_stats"][4], rtol=TOL, atol=1e-30)
+    np.testing.assert_allclose(stt["total_charge"], g["cyc_stats"][1], rtol=1e-9, atol=1e-12 * np.abs(g["cyc_rho"]).sum())
+    np.testing.assert_allclose(stt["total_energy"], g["cyc_stats"][2], rtol=1e-12)
+    dom.close()
+
+
+@pytest.mark.parametrize("neighbors", [True, False])
+@pytest.mark.parametrize("kernel", [0, 1, 2])
+def test_push_variants_match_oracle(lib, orc, neighbors, kernel):
+    mesh, sp, parts, dt, _, _ = make_inputs("box6_body")
+    g = np.load(os.path.join(GOLDEN, "box6_body.npz"))
+    dom = gpu_domain(mesh, 3e-8, neighbors=neighbors, deposit_kernel=kernel)
+    gpu_load_particles(dom, sp, parts)
+    dom.set_electric_field(g["E_laplace"] * 5.0)
+    dom.push()
+    o = orc.push(mesh, g["E_laplace"] * 5.0, parts, sp, 3e-8, kernel=kernel, neighbors=neighbors)
+    st = gpu_state(dom, len(sp), len(parts["tet"]))
+    lost = o["lost"] == 1
+    assert np.array_equal(st["status"] != O.ACTIVE, lost)
+    assert np.array_equal(st["tet"][~lost], o["tet"][~lost])
+    assert rel_err(st["v"], o["v"]) < TOL
+    rho, _, _ = dom.fields()
+    assert rel_err(rho, o["rho"]) < TOL
+    dom.close()
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_mcc_matches_oracle_streams(lib, orc, mode):
+    """Same Philox streams on both sides: identical collision sets, velocities to 1e-12."""
+    mesh = O.kuhn_box((4, 4, 4), 0.05)
+    sp = O.plasma_species(1e10, 3.0, 3.0, 0.05, 8)
+    parts = O.seed_particles(mesh, sp, 8, 21)
+    dom = gpu_domain(mesh, 2e-8, seed=4242)
+    gpu_load_particles(dom, sp, parts)
+    n_t, sigma = 4e20, 1e-19
+    for s in range(2):
+        dom.set_elastic(s, n_t, sigma, mode=mode)
+    dom.collide()
+    st = gpu_state(dom, len(sp), len(parts["tet"]))
+    procs = [O.Elastic(n_t, sigma, 1.0, 0.0, 0.0, 1, 0) for _ in sp]
+    v, hits = orc.mcc(parts["v"], parts["species"], np.zeros(len(parts["tet"]), np.uint8), parts["id"], sp, procs,
+                      2e-8, 4242, 0, mode=mode)
+    assert dom.stats()["mcc_collisions"] == hits and hits > 50
+    changed_g = np.any(st["v"] != parts["v"], axis=1)
+    changed_o = np.any(v != parts["v"], axis=1)
+    assert np.array_equal(changed_g, changed_o)
+    assert rel_err(st["v"], v) < TOL
+    dom.close()
+
+
+def test_picycle_boundary_scenarios(lib):
+    """Tools/PICcore/test/PICCycleBoundary_test.cpp:121-221 on the device."""
+    mesh = O.kuhn_box((1, 1, 6), 1.0, body=None)
+    mesh.xyz[:, 2] /= 6.0
+    z = mesh.xyz[:, 2]
+    mesh.dirichlet[:] = ((z < 1e-12) | (z > z.max() - 1e-12)).astype(np.uint8)
+    sp = [O.Species(-O.QE, O.ME, 1.0, 0, 1.0)]
+    cent = mesh.xyz[mesh.tet].mean(axis=1)
+    for scen in ("periodic", "absorbing", "far_escape"):
+        axis = 0 if scen == "periodic" else 2
+        t = int(np.argmax(cent[:, axis]))
+        vel = {"periodic": [2e9, 0, 0], "absorbing": [0, 0, 2e9], "far_escape": [0, 0, 5e12]}[scen]
+        bc = (0,) * 6 if scen == "far_escape" else (2, 2, 2, 2, 1, 1)
+        dom = gpu_domain(mesh, 1e-9, face_bc=bc)
+        dom.set_species(sp)
+        dom.set_particles(0, cent[t][None, :], np.array([vel], float), np.array([t], np.int32))
+        dom.set_potential(np.zeros(mesh.N))
+        dom.step(1)
+        p = dom.get_particles(0)
+        st = dom.stats()
+        if scen == "periodic":
+            assert p["status"][0] == O.ACTIVE and -1e-9 <= p["x"][0, 0] <= 1.0 + 1e-9
+        elif scen == "absorbing":
+            led = dom.ledger()
+            assert p["status"][0] == O.ABSORBED and st["surface_deposited_charge"] < 0
+            assert led[5, 0] < 0 and led[5, 4] == 1
+        else:
+            assert p["status"][0] != O.ACTIVE and abs(st["surface_deposited_charge"]) < 1e-20
+        dom.close()
+
+
+def test_edge_cases(lib):
+    mesh = O.kuhn_box((3, 3, 3), 0.05)
+    sp = O.plasma_species(1e10, 1.0, 1.0, 0.05, 2)
+    dom = gpu_domain(mesh, 2e-8, face_bc=(1,) * 6)
+    dom.set_species(sp)
+    # empty species, one particle outside the mesh (lost at start -> absorbed at XMax)
+    dom.set_particles(0, np.zeros((0, 3)), np.zeros((0, 3)))
+    dom.set_particles(1, np.array([[0.2, 0.05, 0.05]]), np.array([[1.0, 0.0, 0.0]]))
+    dom.set_potential(mesh.phi_bc)
+    dom.step(2)
+    p = dom.get_particles(1)
+    assert p["status"][0] == O.ABSORBED and dom.ledger()[1, 5] == 1
+    assert dom.count(0) == 0
+    with pytest.raises(Exception):
+        dom.set_particles(5, np.zeros((1, 3)), np.zeros((1, 3)))
+    dom.close()
+
+
+def test_deterministic_and_sort_invariant(lib):
+    mesh = O.kuhn_box((8, 8, 8), 0.05, body=((3, 5), (3, 5), (3, 5)), bias=-10.0)
+    sp = O.plasma_species(1e10, 1.0, 1.0, 0.05, 6)
+    parts = O.seed_particles(mesh, sp, 6, 99)
+    out = []
+    for sort_interval in (0, 0, 1):
+        dom = gpu_domain(mesh, 2e-8, face_bc=(2, 2, 2, 2, 1, 1), sort_interval=sort_interval)
+        gpu_load_particles(dom, sp, parts)
+        dom.set_potential(mesh.phi_bc)
+        dom.solve_field()
+        dom.step(4)
+        rho, phi, E = dom.fields()
+        st = gpu_state(dom, len(sp), len(parts["tet"]))
+        out.append((rho, phi, E, st, dom.ledger()))
+        dom.close()
+    for k in (1, 2):
+        assert np.array_equal(out[0][0], out[k][0])  # fixed-point deposit: bitwise
+        assert np.array_equal(out[0][4], out[k][4])
+        act = out[0][3]["status"] == O.ACTIVE
+        assert np.array_equal(out[0][3]["x"][act], out[k][3]["x"][act])
+    assert np.array_equal(out[0][1], out[1][1]) and np.array_equal(out[0][2], out[1][2])
+
+
+def test_mixed_precision_error_bounded(lib):
+    """Precision form against the FP64 form on the same inputs (errors reported and bounded)."""
+    mesh, sp, parts, dt, nsteps, face_bc = make_inputs("box6_body")
+    res = {}
+    for prec in (0, 1):
+        dom = gpu_domain(mesh, dt, face_bc=face_bc, precision=prec, pcg_rtol=1e-10)
+        gpu_load_particles(dom, sp, parts)
+        dom.set_potential(mesh.phi_bc)
+        dom.solve_field()
+        dom.step(3)
+        res[prec] = (dom.fields(), gpu_state(dom, len(sp), len(parts["tet"])))
+        dom.close()
+    (r0, p0, e0), s0 = res[0]
+    (r1, p1, e1), s1 = res[1]
+    assert rel_err(p1, p0) < 1e-6
+    assert rel_err(e1, e0) < 1e-4
+    both = (s0["status"] == O.ACTIVE) & (s1["status"] == O.ACTIVE)
+    assert both.mean() > 0.95
+    assert np.abs(s1["x"][both] - s0["x"][both]).max() < 1e-4
+    assert (s0["status"] != s1["status"]).mean() < 0.02

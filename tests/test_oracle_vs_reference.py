@@ -1,0 +1,174 @@
+"""Pin the C oracle against the reference's own classes, compiled from its sources into
+oracle/_ref (skipped where that library was not built), on identical seeded state."""
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import rel_err
+from pic_helpers import oracle_cycle
+
+
+def _setup(n=(5, 5, 5), body=((2, 3), (2, 3), (2, 3)), bias=-10.0, ppc=3, seed=5):
+    mesh = O.kuhn_box(n, 0.05, body=body, bias=bias)
+    sp = O.plasma_species(1e10, 1.0, 1.0, 0.05, ppc)
+    parts = O.seed_particles(mesh, sp, ppc, seed)
+    return mesh, sp, parts
+
+
+def test_philox_known_answers(orc):
+    # Random123 known-answer vectors for Philox4x32-10
+    assert list(orc.philox([0, 0, 0, 0], [0, 0])) == [0x6627E8D5, 0xE169C58D, 0xBC57AC4C, 0x9B00DBD8]
+    assert list(orc.philox([0xFFFFFFFF] * 4, [0xFFFFFFFF] * 2)) == [0x408F276D, 0x41C83B0E, 0xA20BC7C6, 0x6D5451FD]
+    assert list(orc.philox([0x243F6A88, 0x85A308D3, 0x13198A2E, 0x03707344], [0xA4093822, 0x299F31D0])) == [
+        0xD16CFE09, 0x94FDCCEB, 0x5001E420, 0x24126EA1]
+    ctr = np.array([[1, 2, 3, 4], [0, 0, 0, 0]], np.uint32)
+    key = np.array([[5, 6], [0, 0]], np.uint32)
+    vec = O.philox4x32_10(ctr, key)
+    assert list(vec[1]) == [0x6627E8D5, 0xE169C58D, 0xBC57AC4C, 0x9B00DBD8]
+    assert list(vec[0]) == list(orc.philox([1, 2, 3, 4], [5, 6]))
+
+
+def test_boris_known_answer(orc):
+    # Tools/Particle/test/ParticleDefinitions_test.cpp:72-91: q/m = 1, E = 2 x, dt = 0.5 -> v = 1
+    out = np.zeros(3)
+    orc.L.orc_boris(np.zeros(3), np.array([2.0, 0.0, 0.0]), 1.0, 0.5, out)
+    assert abs(out[0] - 1.0) < 1e-12 and out[1] == 0.0 and out[2] == 0.0
+
+
+@pytest.mark.parametrize("neighbors", [True, False])
+@pytest.mark.parametrize("kernel", [0, 1, 2])
+def test_push_variants(orc, ref, neighbors, kernel):
+    mesh, sp, parts = _setup()
+    phi, E = ref.poisson(mesh, np.zeros(mesh.N), mesh.phi_bc)
+    a = orc.push(mesh, E, parts, sp, 3e-8, kernel=kernel, neighbors=neighbors)
+    b = ref.push(mesh, E, parts, sp, 3e-8, kernel=kernel, neighbors=neighbors)
+    assert np.array_equal(a["tet"], b["tet"]) and np.array_equal(a["lost"], b["lost"])
+    assert a["substeps"] == b["substeps"]
+    assert rel_err(a["x"], b["x"]) < 1e-12
+    assert rel_err(a["v"], b["v"]) < 1e-12
+    assert rel_err(a["rho"], b["rho"]) < 1e-12
+
+
+def test_push_without_hints(orc, ref):
+    # no location hints: the reference falls back to its linear scan (lowest containing id)
+    mesh, sp, parts = _setup(n=(4, 4, 4), body=None, ppc=2)
+    parts = dict(parts, tet=np.full_like(parts["tet"], -1))
+    E = np.zeros((mesh.N, 3))
+    a = orc.push(mesh, E, parts, sp, 2e-8)
+    b = ref.push(mesh, E, parts, sp, 2e-8)
+    assert np.array_equal(a["tet"], b["tet"]) and rel_err(a["rho"], b["rho"]) < 1e-12
+
+
+def test_lsq_set_potential(orc, ref):
+    # PICCycle::setPotential -> updateElectricField (PICCycle.cpp:769-894), 1e-18 regularisation
+    mesh, _, _ = _setup(body=None)
+    phi = 12.0 * mesh.xyz[:, 2] + 3.0 * mesh.xyz[:, 0] ** 2
+    A = orc.assemble(mesh)
+    assert rel_err(orc.lsq(mesh, A, phi, reg=1e-18), ref.lsq(mesh, phi)) < 1e-12
+
+
+def test_poisson_plate_reference_test(orc, ref):
+    # Tools/FieldSolver/test/PoissonSolver_test.cpp:48-117: 10 V / 0 V plates, interior in [0,10]
+    mesh = O.kuhn_box((1, 1, 6), 0.01, body=None)
+    z = mesh.xyz[:, 2]
+    dir_ = ((z < 1e-12) | (z > z.max() - 1e-12)).astype(np.uint8)
+    phi_bc = np.where(z < 1e-12, 10.0, 0.0)
+    mesh.dirichlet[:] = dir_
+    mesh.phi_bc[:] = phi_bc
+    A = orc.assemble(mesh)
+    phi, _, _ = orc.poisson(mesh, A, np.zeros(mesh.N), phi_bc)
+    inner = dir_ == 0
+    assert np.all(phi[inner] >= -1e-8) and np.all(phi[inner] <= 10 + 1e-8)
+    assert np.allclose(phi[z < 1e-12], 10.0, atol=1e-8)
+    pr, Er = ref.poisson(mesh, np.zeros(mesh.N), phi_bc)
+    assert rel_err(phi, pr) < 1e-12
+    E = orc.lsq(mesh, A, phi)
+    assert np.all(np.isfinite(E)) and np.abs(E).max() > 0 and rel_err(E, Er) < 1e-12
+
+
+@pytest.mark.parametrize("face_bc", [(2, 2, 2, 2, 1, 1), (1, 1, 1, 1, 1, 1), (0, 0, 0, 0, 1, 1)])
+def test_cycle_boundaries(orc, ref, face_bc):
+    mesh, sp, parts = _setup(ppc=3)
+    phi0, _ = ref.poisson(mesh, np.zeros(mesh.N), mesh.phi_bc)
+    a = oracle_cycle(orc, mesh, sp, parts, 3, 4e-8, face_bc, phi0)
+    b = ref.cycle(mesh, parts, sp, 3, 4e-8, face_bc, phi0)
+    ids = b["id"]
+    st = {10: O.ACTIVE, 20: O.ABSORBED, 21: O.ESCAPED}
+    assert np.array_equal(a["status"][ids], np.array([st[s] for s in b["status"]]))
+    act = b["status"] == 10
+    assert rel_err(a["x"][ids][act], b["x"][act]) < 1e-12
+    assert rel_err(a["rho"], b["rho"]) < 1e-12
+    assert rel_err(a["phi"], b["phi"]) < 1e-12
+    np.testing.assert_allclose(a["ledger"][:6], b["ledger"], rtol=1e-12, atol=1e-30)
+
+
+def _plate():
+    # the 1 x 1 x 6 plate of Tools/PICcore/test/PICCycleBoundary_test.cpp:32-65 (Kuhn split)
+    mesh = O.kuhn_box((1, 1, 6), 1.0 / 1.0, body=None)
+    mesh.xyz[:, 2] /= 6.0
+    z = mesh.xyz[:, 2]
+    mesh.dirichlet[:] = ((z < 1e-12) | (z > z.max() - 1e-12)).astype(np.uint8)
+    mesh.phi_bc[:] = 0.0
+    return mesh
+
+
+def _single(mesh, tet, vel, w=1.0):
+    c = mesh.xyz[mesh.tet[tet]].mean(axis=0)
+    return dict(x=c[None, :].copy(), v=np.array([vel], np.float64), species=np.zeros(1, np.int32),
+                tet=np.array([tet], np.int32), id=np.zeros(1, np.int64))
+
+
+@pytest.mark.parametrize("scenario", ["periodic", "absorbing", "far_escape"])
+def test_picycle_boundary_reference_tests(orc, ref, scenario):
+    """PICCycleBoundary_test.cpp:121-221 re-hosted: dt 1e-9, one electron of weight 1."""
+    mesh = _plate()
+    sp = [O.Species(-O.QE, O.ME, 1.0, 0, 1.0)]
+    cent = mesh.xyz[mesh.tet].mean(axis=1)
+    if scenario == "periodic":
+        t = int(np.argmax(cent[:, 0]))
+        parts, bc = _single(mesh, t, [2.0e9, 0, 0]), (2, 2, 2, 2, 1, 1)
+    elif scenario == "absorbing":
+        t = int(np.argmax(cent[:, 2]))
+        parts, bc = _single(mesh, t, [0, 0, 2.0e9]), (2, 2, 2, 2, 1, 1)
+    else:
+        t = int(np.argmax(cent[:, 2]))
+        parts, bc = _single(mesh, t, [0, 0, 5.0e12]), (0, 0, 0, 0, 0, 0)
+    phi0 = np.zeros(mesh.N)
+    a = oracle_cycle(orc, mesh, sp, parts, 1, 1e-9, bc, phi0)
+    b = ref.cycle(mesh, parts, sp, 1, 1e-9, bc, phi0)
+    st = {10: O.ACTIVE, 20: O.ABSORBED, 21: O.ESCAPED}
+    assert a["status"][0] == st[b["status"][0]]
+    if scenario == "periodic":
+        assert a["status"][0] == O.ACTIVE
+        assert -1e-9 <= a["x"][0, 0] <= 1.0 + 1e-9
+        assert rel_err(a["x"], b["x"]) < 1e-12
+    elif scenario == "absorbing":
+        assert a["status"][0] == O.ABSORBED
+        assert a["surface_charge"] < 0 and a["ledger"][5, 0] < 0 and a["ledger"][5, 4] == 1
+        np.testing.assert_allclose(a["ledger"][:6], b["ledger"], rtol=1e-12, atol=1e-40)
+    else:
+        assert a["status"][0] != O.ACTIVE and abs(a["surface_charge"]) < 1e-20
+
+
+def test_mcc_statistics_match_reference(orc, ref):
+    """Reference mt19937 stream vs oracle Philox streams: the same collision law within a
+    5-sigma band (the streams themselves cannot match).  The reference handler counts
+    first-draw hits (probability p) while a particle scatters only when its second draw
+    passes too (probability p^2)."""
+    rng = np.random.default_rng(3)
+    P = 20000
+    v = rng.normal(size=(P, 3)) * 4.2e5
+    sigma, n_t, dt, reps = 1e-19, 3e20, 2e-8, 5
+    ref_hits, ref_scat = ref.mcc_count(v, 0, 1.0, sigma, n_t, dt, 7, reps)
+    sp = [O.Species(-O.QE, O.ME, 1.0, 0, 1.0)]
+    proc = [O.Elastic(n_t, sigma, 1.0, 0.0, 0.0, 1, 0)]
+    hits = 0
+    for r in range(reps):
+        _, h = orc.mcc(v, np.zeros(P, np.int32), np.zeros(P, np.uint8), np.arange(P), sp, proc, dt, 99, r, mode=0)
+        hits += h
+    p = np.clip(n_t * sigma * np.linalg.norm(v, axis=1) * dt, 0, 1)
+    m1, s1 = reps * p.sum(), np.sqrt(reps * np.sum(p * (1 - p)))
+    m2, s2 = reps * np.sum(p * p), np.sqrt(reps * np.sum(p * p * (1 - p * p)))
+    assert abs(ref_hits - m1) < 5 * s1, (ref_hits, m1, s1)
+    assert abs(ref_scat - m2) < 5 * s2, (ref_scat, m2, s2)
+    assert abs(hits - m2) < 5 * s2, (hits, m2, s2)
