@@ -24,15 +24,17 @@
 
 namespace scdat {
 void launch_push_f64(const MeshView& M, const ParticleStore& P, const SpeciesDev& S, const PushParams& pp,
-                     const double* E, unsigned long long* rlo, unsigned long long* rhi, LedgerDev* L, double* ke_part,
-                     int grid, cudaStream_t st);
+                     const DeferList& D1, const DeferList& D2, unsigned long long* rlo, unsigned long long* rhi,
+                     LedgerDev* L, double* ke_part, int grid, cudaStream_t st);
 void launch_mcc_f64(const ParticleStore& P, const SpeciesDev& S, const PushParams& pp, LedgerDev* L, int grid,
                     cudaStream_t st);
 void launch_push_mixed(const MeshView& M, const ParticleStore& P, const SpeciesDev& S, const PushParams& pp,
-                       const float* Ef, unsigned long long* rlo, unsigned long long* rhi, LedgerDev* L,
-                       double* ke_part, int grid, cudaStream_t st);
+                       const DeferList& D1, const DeferList& D2, unsigned long long* rlo, unsigned long long* rhi,
+                       LedgerDev* L, double* ke_part, int grid, cudaStream_t st);
 void launch_mcc_mixed(const ParticleStore& P, const SpeciesDev& S, const PushParams& pp, LedgerDev* L, int grid,
                       cudaStream_t st);
+void launch_refresh_erec(int64_t T, const int4* tet, const double* E, double* erec, cudaStream_t st);
+void launch_refresh_trec(int64_t T, const int4* tet, const double* E, float* trec, cudaStream_t st);
 void launch_to_mixed(const MeshView& M, int64_t n, const double* x, const double* y, const double* z,
                      const double* vx, const double* vy, const double* vz, const ParticleStore& P, cudaStream_t st);
 void launch_from_mixed(const MeshView& M, int64_t n, const ParticleStore& P, double* x, double* y, double* z,
@@ -111,8 +113,8 @@ struct scdat_ctx {
     MeshView mv{};
     PoissonView pv{};
     // mesh
-    DBuf<double> xyz, geom;
-    DBuf<float> geomf;
+    DBuf<double> xyz, geom, erec;
+    DBuf<float> geomf, trec;
     DBuf<int4> tet, nbr;
     DBuf<int32_t> bin_start, bin_tets, gptr, gcol;
     // poisson
@@ -141,6 +143,12 @@ struct scdat_ctx {
     DBuf<uint32_t> scratchu;
     DBuf<int64_t> nact;
     DBuf<int64_t> idx64;
+    // deferred-particle lists of the multi-pass push
+    DBuf<unsigned> dcount;
+    DBuf<uint32_t> d1idx, d2idx;
+    DBuf<int> d1it, d2it;
+    DBuf<double> d1rem, d2rem, d1vs, d2vs;
+    unsigned dcap = 0;
     double uq = 1.0, ue = 1.0;
     int64_t steps = 0;
     double sim_time = 0.0;
@@ -287,11 +295,15 @@ int do_push(scdat_ctx* ctx, bool do_mcc)
         ctx->push_particles += ctx->species[s].n;
         ParticleStore P = store_of(ctx, s);
         SpeciesDev sd = species_dev(ctx, s);
+        CK(cudaMemsetAsync(ctx->dcount.p, 0, 2 * sizeof(unsigned), ctx->st));
+        DeferList d1{ctx->dcount.p, ctx->dcap, ctx->d1idx.p, ctx->d1it.p, ctx->d1rem.p, ctx->d1vs.p};
+        DeferList d2{ctx->dcount.p + 1, ctx->dcap, ctx->d2idx.p, ctx->d2it.p, ctx->d2rem.p, ctx->d2vs.p};
+        ctx->launches += 3;
         if (ctx->mixed)
-            ++ctx->launches, launch_push_mixed(ctx->mv, P, sd, pp, ctx->Ef.p, ctx->acc_lo.p + s * N, ctx->acc_hi.p + s * N, ctx->led.p,
+            launch_push_mixed(ctx->mv, P, sd, pp, d1, d2, ctx->acc_lo.p + s * N, ctx->acc_hi.p + s * N, ctx->led.p,
                               ctx->ke_part.p, ctx->grid_push, ctx->st);
         else
-            ++ctx->launches, launch_push_f64(ctx->mv, P, sd, pp, ctx->E.p, ctx->acc_lo.p + s * N, ctx->acc_hi.p + s * N, ctx->led.p,
+            launch_push_f64(ctx->mv, P, sd, pp, d1, d2, ctx->acc_lo.p + s * N, ctx->acc_hi.p + s * N, ctx->led.p,
                             ctx->ke_part.p, ctx->grid_push, ctx->st);
     }
     CK(cudaGetLastError());
@@ -308,6 +320,18 @@ int do_push(scdat_ctx* ctx, bool do_mcc)
     return SCDAT_OK;
 }
 
+// copy the nodal field into the per-tet records the push kernels read
+int refresh_tet_field(scdat_ctx* ctx)
+{
+    ++ctx->launches;
+    if (ctx->mixed)
+        launch_refresh_trec(ctx->hm.T, ctx->tet.p, ctx->E.p, ctx->trec.p, ctx->st);
+    else
+        launch_refresh_erec(ctx->hm.T, ctx->tet.p, ctx->E.p, ctx->erec.p, ctx->st);
+    CK(cudaGetLastError());
+    return SCDAT_OK;
+}
+
 int do_lsq(scdat_ctx* ctx, double reg)
 {
     CK(cudaMemsetAsync(&ctx->led.p->flags, 0, sizeof(unsigned long long), ctx->st));
@@ -315,7 +339,7 @@ int do_lsq(scdat_ctx* ctx, double reg)
     launch_lsq(ctx->hm.N, ctx->xyz.p, ctx->gptr.p, ctx->gcol.p, ctx->phi.p, reg, ctx->E.p, ctx->Ef.p,
                &ctx->led.p->flags, ctx->grid_nodes, ctx->st);
     CK(cudaGetLastError());
-    return SCDAT_OK;
+    return refresh_tet_field(ctx);
 }
 
 int pcg_scalars_init(scdat_ctx* ctx, double rtol, int max_iter, double abs_thr2)
@@ -611,8 +635,31 @@ SCDAT_API int scdat_create(const scdat_mesh_desc* mesh, const scdat_params* para
     mv.xyz = ctx->xyz.p;
     mv.tet = ctx->tet.p;
     mv.nbr = ctx->nbr.p;
+    if (ctx->mixed) {
+        // static words of the 128-byte tet records: J^-1 and node ids (E refreshed later)
+        std::vector<float> rec((size_t)(64 * m.T), 0.0f);
+        for (int64_t t = 0; t < m.T; ++t) {
+            float* r = &rec[64 * t];
+            for (int k = 0; k < 9; ++k) r[k] = ctx->hg.geomf[12 * t + k];
+            for (int k = 0; k < 4; ++k) std::memcpy(&r[21 + k], &m.tet[4 * t + k], sizeof(int32_t));
+            for (int k = 0; k < 4; ++k) std::memcpy(&r[25 + k], &m.nbr[4 * t + k], sizeof(int32_t));
+            const int64_t o = m.tet[4 * t];
+            for (int k = 0; k < 4; ++k) {
+                int32_t nb = m.nbr[4 * t + k];
+                if (nb < 0) continue;
+                const int64_t on = m.tet[4 * (int64_t)nb];
+                for (int a = 0; a < 3; ++a) r[32 + 3 * k + a] = (float)(m.xyz[3 * o + a] - m.xyz[3 * on + a]);
+            }
+        }
+        CK(ctx->trec.upload(rec.data(), rec.size(), st));
+    } else {
+        CK(ctx->erec.alloc((size_t)(12 * m.T)));
+        CK(cudaMemsetAsync(ctx->erec.p, 0, sizeof(double) * 12 * m.T, st));
+    }
     mv.geom = ctx->geom.p;
     mv.geomf = ctx->geomf.p;
+    mv.trec = ctx->trec.p;
+    mv.erec = ctx->erec.p;
     for (int a = 0; a < 3; ++a) {
         mv.gmin[a] = ctx->hgrid.gmin[a];
         mv.ginv[a] = ctx->hgrid.ginv[a];
@@ -693,13 +740,14 @@ SCDAT_API int scdat_set_species(scdat_ctx* ctx, int32_t n_species, const scdat_s
     ARG(n_species > 0 && n_species <= 16 && sp, "need 1..16 species");
     ARG(ctx->species.empty(), "species are already set");
     ctx->species = std::vector<SpeciesState>((size_t)n_species);
+    // fixed-point units: one macro-particle charge, and the energy of a 1 MeV macro-particle
+    // (resolution 2^-64 of that, range 2^63 of it)
     double mq = 0.0, me = 0.0;
-    const double c2 = 2.99792458e8 * 2.99792458e8;
     for (int s = 0; s < n_species; ++s) {
         ARG(sp[s].mass > 0.0 && std::isfinite(sp[s].charge) && sp[s].weight > 0.0, "bad species entry");
         ctx->species[s].sp = sp[s];
         mq = std::max(mq, std::fabs(sp[s].charge * sp[s].weight));
-        me = std::max(me, 0.5 * sp[s].mass * c2 * std::max(1.0, sp[s].weight));
+        me = std::max(me, 1.602176634e-13 * std::max(1.0, sp[s].weight));
     }
     ctx->uq = pow2_ceil(mq);
     ctx->ue = pow2_ceil(me);
@@ -730,6 +778,21 @@ static int alloc_species(scdat_ctx* ctx, int s, int64_t n)
     S.cap = cap;
     S.n = n;
     CK(cudaMemcpyAsync(ctx->counts.p + s, &S.n, sizeof(int64_t), cudaMemcpyHostToDevice, ctx->st));
+    // deferred lists of the multi-pass push: a quarter of the largest species (a full list
+    // only means the overflow finishes in the earlier pass)
+    unsigned want = (unsigned)std::min<int64_t>(cap / 4 + 4096, 0x7fffffff);
+    if (want > ctx->dcap) {
+        CK(ctx->dcount.alloc(2));
+        CK(ctx->d1idx.alloc(want));
+        CK(ctx->d2idx.alloc(want));
+        CK(ctx->d1it.alloc(want));
+        CK(ctx->d2it.alloc(want));
+        CK(ctx->d1rem.alloc(want));
+        CK(ctx->d2rem.alloc(want));
+        CK(ctx->d1vs.alloc(want));
+        CK(ctx->d2vs.alloc(want));
+        ctx->dcap = want;
+    }
     // sort scratch must cover the largest species
     size_t need = (size_t)cap;
     if (ctx->kin.n < need) {
@@ -927,6 +990,8 @@ SCDAT_API int scdat_set_electric_field(scdat_ctx* ctx, const double* E)
     std::vector<float> f((size_t)n3);
     for (int64_t i = 0; i < n3; ++i) f[i] = (float)E[i];
     CK(cudaMemcpyAsync(ctx->Ef.p, f.data(), sizeof(float) * n3, cudaMemcpyHostToDevice, ctx->st));
+    int rc = refresh_tet_field(ctx);
+    if (rc) return rc;
     CK(cudaStreamSynchronize(ctx->st));
     return SCDAT_OK;
 }

@@ -108,8 +108,12 @@ struct MeshView {
     const double* xyz;       // [N*3]
     const int4* tet;         // [T]
     const int4* nbr;         // [T] neighbour across the face opposite local vertex f
-    const double* geom;      // [T*12] inverse Jacobian (row-major 3x3) then origin node xyz
+    const double* geom;      // [T*16] 128-byte records: J^-1 (row-major), origin xyz, 4 face
+                             // neighbours and 4 node ids as int32
     const float* geomf;      // [T*12] the same in FP32 (mixed form), origin-relative
+    const float* trec;       // [T*64] mixed-form 256-byte records (FP32 J^-1, nodal E, node ids,
+                             // neighbours | FP32 origin offsets to the 4 neighbours)
+    const double* erec;      // [T*12] FP64 nodal E of each tet's 4 nodes (refreshed per solve)
     // locate grid: uniform bins over the bounding box, tets listed by ascending id
     double gmin[3];
     double ginv[3];

@@ -59,7 +59,7 @@ std::string compute_face_neighbors(const HostMesh& m, std::vector<int32_t>& nbr)
 std::string compute_geometry(const HostMesh& m, HostGeometry& g)
 {
     const int64_t T = m.T;
-    g.geom.assign((size_t)(12 * T), 0.0);
+    g.geom.assign((size_t)(16 * T), 0.0);
     g.geomf.assign((size_t)(12 * T), 0.0f);
     for (int a = 0; a < 3; ++a) {
         g.bmin[a] = std::numeric_limits<double>::infinity();
@@ -94,7 +94,7 @@ std::string compute_geometry(const HostMesh& m, HostGeometry& g)
                v3[3] = {J[0][2], J[1][2], J[2][2]};
         double cx = v2[1] * v3[2] - v2[2] * v3[1], cy = v2[2] * v3[0] - v2[0] * v3[2], cz = v2[0] * v3[1] - v2[1] * v3[0];
         double V6 = v1[0] * cx + v1[1] * cy + v1[2] * cz;
-        double* G = &g.geom[12 * t];
+        double* G = &g.geom[16 * t];
         float* Gf = &g.geomf[12 * t];
         if (std::fabs(V6) < 1e-15) {  // degenerate: never contains a point
             for (int k = 0; k < 9; ++k) {
@@ -124,6 +124,13 @@ std::string compute_geometry(const HostMesh& m, HostGeometry& g)
         G[9] = p[0][0];
         G[10] = p[0][1];
         G[11] = p[0][2];
+        // words 12..15 hold the 4 face neighbours and the 4 node ids as int32
+        int32_t ids[8];
+        for (int k = 0; k < 4; ++k) {
+            ids[k] = m.nbr.empty() ? -1 : m.nbr[4 * t + k];
+            ids[4 + k] = m.tet[4 * t + k];
+        }
+        std::memcpy(&G[12], ids, sizeof(ids));
     }
     g.max_edge = max_edge;
     return "";

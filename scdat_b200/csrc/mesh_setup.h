@@ -19,7 +19,7 @@ struct HostMesh {
 };
 
 struct HostGeometry {
-    std::vector<double> geom;   // [T*12] inverse Jacobian row-major, origin xyz
+    std::vector<double> geom;   // [T*16] inverse Jacobian row-major, origin xyz, face neighbours + node ids (int32)
     std::vector<float> geomf;   // [T*12] FP32 inverse Jacobian, 3 unused
     double bmin[3], bmax[3];
     double max_edge = 0.0;

@@ -29,7 +29,7 @@ __device__ __forceinline__ bool bary_inside(const double lam[4])
 // FieldInterpolator::isPointInTetrahedron, PICParticleAlgorithms.cpp:247-296).
 __device__ __forceinline__ bool bary64(const MeshView& M, int t, double px, double py, double pz, double lam[4])
 {
-    const double2* g2 = reinterpret_cast<const double2*>(M.geom + 12 * (int64_t)t);
+    const double2* g2 = reinterpret_cast<const double2*>(M.geom + 16 * (int64_t)t);
     double2 a = __ldg(g2 + 0), b = __ldg(g2 + 1), c = __ldg(g2 + 2), d = __ldg(g2 + 3), e = __ldg(g2 + 4),
             f = __ldg(g2 + 5);
     double dx = px - e.y, dy = py - f.x, dz = pz - f.y;
@@ -42,7 +42,7 @@ __device__ __forceinline__ bool bary64(const MeshView& M, int t, double px, doub
 
 // Lowest-id tet containing p among the grid candidates (exactly the result of the
 // reference's linear scan, PICParticleAlgorithms.cpp:882-888), or -1.
-__device__ inline int grid_lookup(const MeshView& M, double px, double py, double pz)
+static __device__ __noinline__ int grid_lookup(const MeshView& M, double px, double py, double pz)
 {
     double p[3] = {px, py, pz};
     int lo[3], hi[3];
@@ -73,50 +73,88 @@ __device__ inline int grid_lookup(const MeshView& M, double px, double py, doubl
     return best == 0x7fffffff ? -1 : best;
 }
 
-// After the hint and its neighbour list fail: walk across the most violated face from
-// `start`; accept a tet whose barycentrics all clear 1e-6 (no other tet can hold the point
-// within the 1e-8 tolerance then), otherwise fall back to the exact grid lookup.
-__device__ inline int locate_far(const MeshView& M, double px, double py, double pz, int start)
+__device__ __forceinline__ int4 rec_nbr(const MeshView& M, int t)
 {
-    double lam[4];
+    return __ldg(reinterpret_cast<const int4*>(M.geom + 16 * (int64_t)t + 12));
+}
+
+__device__ __forceinline__ int4 rec_nodes(const MeshView& M, int t)
+{
+    return __ldg(reinterpret_cast<const int4*>(M.geom + 16 * (int64_t)t + 14));
+}
+
+// Straight walk from `start` across the most violated face (lam holds start's barycentrics).
+// Returns the tet reached that contains p, or -1 at a boundary face, a degenerate tet or the
+// step cap.  *unique is set when every barycentric clears 1e-6: no other tet can then hold
+// the point within the 1e-8 containment tolerance, so the reference's search order
+// (hint, neighbour list, lowest id) cannot pick a different tet.
+__device__ __forceinline__ int walk64(const MeshView& M, double px, double py, double pz, int start, double lam[4],
+                                      bool* unique)
+{
     int t = start;
-    if (t >= 0) {
-        for (int k = 0; k < kWalkSteps; ++k) {
-            bool in = bary64(M, t, px, py, pz, lam);
-            double mn = fmin(fmin(lam[0], lam[1]), fmin(lam[2], lam[3]));
-            if (in) {
-                if (mn >= 1e-6) return t;
-                break;
-            }
-            if (!(mn == mn)) break;  // NaN: degenerate tet
-            int f = 0;
-#pragma unroll
-            for (int i = 1; i < 4; ++i)
-                if (lam[i] < lam[f]) f = i;
-            int4 nb = __ldg(M.nbr + t);
-            int nt = f == 0 ? nb.x : (f == 1 ? nb.y : (f == 2 ? nb.z : nb.w));
-            if (nt < 0) break;
-            t = nt;
+    for (int k = 0; k < kWalkSteps; ++k) {
+        double mn = fmin(fmin(lam[0], lam[1]), fmin(lam[2], lam[3]));
+        if (!(mn == mn)) return -1;  // NaN: degenerate tet
+        if (bary_inside(lam)) {
+            *unique = mn >= 1e-6;
+            return t;
         }
+        int f = 0;
+#pragma unroll
+        for (int i = 1; i < 4; ++i)
+            if (lam[i] < lam[f]) f = i;
+        int4 nb = rec_nbr(M, t);
+        int nt = f == 0 ? nb.x : (f == 1 ? nb.y : (f == 2 ? nb.z : nb.w));
+        if (nt < 0) return -1;
+        t = nt;
+        bary64(M, t, px, py, pz, lam);
+    }
+    return -1;
+}
+
+// Without a usable hint: walk from `start` when given, else (or when the walk cannot decide)
+// the exact grid lookup of the lowest containing id.
+static __device__ __noinline__ int locate_far(const MeshView& M, double px, double py, double pz, int start)
+{
+    if (start >= 0) {
+        double lam[4];
+        bary64(M, start, px, py, pz, lam);
+        bool uniq = false;
+        int t = walk64(M, px, py, pz, start, lam, &uniq);
+        if (t >= 0 && uniq) return t;
     }
     return grid_lookup(M, px, py, pz);
 }
 
-// CrossTetrahedron::locateParticle semantics (PICParticleAlgorithms.cpp:853-891).
+// CrossTetrahedron::locateParticle (PICParticleAlgorithms.cpp:853-891): the hint if it holds
+// the point; otherwise the unique holder found by the walk; only for points within the
+// tolerance band of several tets, the reference order itself (neighbour list, then the
+// lowest id over all tets, which the grid lookup reproduces).
+static __device__ __noinline__ int locate_slow(const MeshView& M, double px, double py, double pz, int hint,
+                                               double lam[4])
+{
+    bool uniq = false;
+    int t = walk64(M, px, py, pz, hint, lam, &uniq);
+    if (t >= 0 && uniq) return t;
+    if (M.use_nbr) {
+        int4 nb = rec_nbr(M, hint);
+        double l2[4];
+        if (nb.x >= 0 && bary64(M, nb.x, px, py, pz, l2)) return nb.x;
+        if (nb.y >= 0 && bary64(M, nb.y, px, py, pz, l2)) return nb.y;
+        if (nb.z >= 0 && bary64(M, nb.z, px, py, pz, l2)) return nb.z;
+        if (nb.w >= 0 && bary64(M, nb.w, px, py, pz, l2)) return nb.w;
+    }
+    return grid_lookup(M, px, py, pz);
+}
+
 __device__ __forceinline__ int locate(const MeshView& M, double px, double py, double pz, int hint)
 {
     double lam[4];
     if (hint >= 0) {
         if (bary64(M, hint, px, py, pz, lam)) return hint;
-        if (M.use_nbr) {
-            int4 nb = __ldg(M.nbr + hint);
-            if (nb.x >= 0 && bary64(M, nb.x, px, py, pz, lam)) return nb.x;
-            if (nb.y >= 0 && bary64(M, nb.y, px, py, pz, lam)) return nb.y;
-            if (nb.z >= 0 && bary64(M, nb.z, px, py, pz, lam)) return nb.z;
-            if (nb.w >= 0 && bary64(M, nb.w, px, py, pz, lam)) return nb.w;
-        }
+        return locate_slow(M, px, py, pz, hint, lam);
     }
-    return locate_far(M, px, py, pz, hint);
+    return grid_lookup(M, px, py, pz);
 }
 
 // PICCycle::detectBoundaryFace, PICCycle.cpp:1074-1133.
@@ -164,7 +202,7 @@ __device__ inline void ledger_tally(LedgerDev* L, int row, const SpeciesDev& S, 
 // PICCycle::applyRuntimeBoundaryCondition + processRuntimeBoundaryEvents for one lost
 // particle (PICCycle.cpp:1221-1379).  Updates position (periodic wrap) and returns the new
 // tet code (>= 0 active, kTetAbsorbed, kTetEscaped).
-__device__ inline int resolve_lost(const MeshView& M, const SpeciesDev& S, const PushParams& pp, LedgerDev* L, double& px,
+static __device__ __noinline__ int resolve_lost(const MeshView& M, const SpeciesDev& S, const PushParams& pp, LedgerDev* L, double& px,
                             double& py, double& pz, double ke, int hint)
 {
     int resolved = -1;
@@ -259,5 +297,79 @@ __device__ inline bool mcc_elastic(const SpeciesDev& S, const PushParams& pp, ui
     vz = speed * cos(theta);
     return true;
 }
+
+}  // namespace scdat
+
+namespace scdat {
+
+// Particles that still have time left after a pass: index, sub-steps used, remaining time
+// and the step-start speed (adaptiveTimeStep keeps using it, PICParticleAlgorithms.cpp:762).
+struct DeferList {
+    unsigned* count;
+    unsigned cap;
+    uint32_t* idx;
+    int* it;
+    double* rem;
+    double* vstart;
+};
+
+enum { kDone = 0, kCapped = 1, kLost = 2 };
+
+struct PushStats {
+    double ke_sum;
+    unsigned long long nsub, nlost, nhit, nact;
+};
+
+// warp-aggregated append to a deferred list; every lane of the warp calls it
+__device__ __forceinline__ unsigned warp_append(bool want, unsigned* cnt)
+{
+    const int lane = threadIdx.x & 31;
+    unsigned m = __ballot_sync(0xffffffffu, want);
+    unsigned base = 0;
+    if (m) {
+        int leader = __ffs(m) - 1;
+        if (lane == leader) base = atomicAdd(cnt, (unsigned)__popc(m));
+        base = __shfl_sync(0xffffffffu, base, leader);
+    }
+    return base + (unsigned)__popc(m & ((1u << lane) - 1u));
+}
+
+// block reduction of the push statistics in a fixed order (deterministic)
+__device__ __forceinline__ void block_stats(const PushStats& c, LedgerDev* L, double* ke_part)
+{
+    __shared__ double sk[8];
+    __shared__ unsigned long long sc[4][8];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double ke = c.ke_sum;
+    unsigned long long v[4] = {c.nsub, c.nlost, c.nhit, c.nact};
+    for (int o = 16; o > 0; o >>= 1) {
+        ke += __shfl_down_sync(0xffffffffu, ke, o);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+    }
+    if (lane == 0) {
+        sk[warp] = ke;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) sc[k][warp] = v[k];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        unsigned long long a[4] = {0, 0, 0, 0};
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+            s += sk[w];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) a[k] += sc[k][w];
+        }
+        ke_part[blockIdx.x] += s;
+        if (a[0]) atomicAdd(&L->substeps, a[0]);
+        if (a[1]) atomicAdd(&L->lost_events, a[1]);
+        if (a[2]) atomicAdd(&L->mcc_hits, a[2]);
+        if (a[3]) atomicAdd(&L->active, a[3]);
+    }
+}
+
+constexpr int kCap1 = 2;   // sub-steps every particle gets in pass 1
+constexpr int kCap2 = 16;  // further sub-steps in pass 2; pass 3 runs to the end
 
 }  // namespace scdat

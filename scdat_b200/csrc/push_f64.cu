@@ -4,9 +4,11 @@
 // per-sub-step trajectory deposit (:371-433), then the runtime boundary events
 // (PICCycle.cpp:1221-1379) and, when enabled, the elastic background MCC.
 //
-// Charge goes into per-species 128-bit fixed-point node accumulators: the 10 sample points
-// of a sub-step are summed exactly in registers, then each of the tet's 4 nodes takes one
-// 64-bit atomic (plus one on carry), so the deposit is exact and order independent.
+// Charge goes into per-species 128-bit fixed-point node accumulators staged per warp in
+// shared memory, so the deposit is exact and independent of thread order.  The nodal E of
+// each tet's 4 nodes is kept per tet (refreshed after every field solve), so the gather is
+// one load beside the tet's geometry.  Sub-steps run in passes (see push_mixed.cu) to keep
+// warps converged.
 #include "push.cuh"
 
 namespace scdat {
@@ -28,9 +30,9 @@ __device__ __forceinline__ void dep_point(DepositAcc& acc, const double lam[4], 
 
 // ChargeDepositor::depositChargeAlongTrajectory into the post-move tet t
 // (PICParticleAlgorithms.cpp:371-433); each sample point counts only when it lies in t.
-__device__ __forceinline__ void deposit_traj(const MeshView& M, const SpeciesDev& S, const PushParams& pp, int t,
-                                             double sx, double sy, double sz, double ex, double ey, double ez,
-                                             unsigned long long* rlo, unsigned long long* rhi)
+static __device__ __noinline__ void deposit_traj(const MeshView& M, const SpeciesDev& S, const PushParams& pp, int t,
+                                                 double sx, double sy, double sz, double ex, double ey, double ez,
+                                                 unsigned long long* rlo, unsigned long long* rhi)
 {
     DepositAcc acc;
 #pragma unroll
@@ -45,7 +47,7 @@ __device__ __forceinline__ void deposit_traj(const MeshView& M, const SpeciesDev
         if (bary64(M, t, ex, ey, ez, lam)) dep_point(acc, lam, qw, pp.inv_uq);
     } else {
         // barycentrics are affine along the segment: lam(s + tau*tr) = lam_s + tau*dlam
-        const double* g = M.geom + 12 * (int64_t)t;
+        const double* g = M.geom + 16 * (int64_t)t;
         double ls[4], dl[4];
         bary64(M, t, sx, sy, sz, ls);
         dl[1] = __ldg(g + 0) * tx + __ldg(g + 1) * ty + __ldg(g + 2) * tz;
@@ -59,7 +61,6 @@ __device__ __forceinline__ void deposit_traj(const MeshView& M, const SpeciesDev
             for (int sg = 0; sg < nseg; ++sg) {
                 double t0 = (double)sg / (double)nseg, t1 = (double)(sg + 1) / (double)nseg;
                 double tc = 0.5 * (t0 + t1), th = 0.5 * (t1 - t0);
-#pragma unroll
                 for (int q = 0; q < 3; ++q) {
                     double tau = tc + th * gn[q];
                     double l[4] = {ls[0] + tau * dl[0], ls[1] + tau * dl[1], ls[2] + tau * dl[2], ls[3] + tau * dl[3]};
@@ -75,135 +76,209 @@ __device__ __forceinline__ void deposit_traj(const MeshView& M, const SpeciesDev
         }
     }
     if (!acc.any) return;
-    int4 tn = __ldg(M.tet + t);
+    int4 tn = rec_nodes(M, t);
     fx_atomic_add(rlo + tn.x, rhi + tn.x, acc.n[0]);
     fx_atomic_add(rlo + tn.y, rhi + tn.y, acc.n[1]);
     fx_atomic_add(rlo + tn.z, rhi + tn.z, acc.n[2]);
     fx_atomic_add(rlo + tn.w, rhi + tn.w, acc.n[3]);
 }
 
-__device__ __forceinline__ void gather_e(const MeshView& M, const double* __restrict__ E, int t, double px, double py,
-                                         double pz, double& Ex, double& Ey, double& Ez)
+struct FlightD {
+    double px, py, pz, vx, vy, vz;
+    double rem, vstart;
+    int cur, it;
+};
+
+// Run sub-steps until the step's time is used up, the particle is lost, or `cap` sub-steps
+// ran in this call.
+__device__ __forceinline__ int advance_d(const MeshView& M, const SpeciesDev& S, const PushParams& pp, FlightD& f,
+                                         int cap, unsigned long long* rlo, unsigned long long* rhi,
+                                         unsigned long long& nsub)
 {
+    const double qm = S.qm;
+    const double qw = S.q * S.w;
     double lam[4];
-    Ex = Ey = Ez = 0.0;
-    if (!bary64(M, t, px, py, pz, lam)) return;  // interpolateVectorField returns 0 outside
-    int4 tn = __ldg(M.tet + t);
-    int nd[4] = {tn.x, tn.y, tn.z, tn.w};
+    bool in = bary64(M, f.cur, f.px, f.py, f.pz, lam);  // reused as the next gather's weights
+    int k = 0;
+    while (f.rem > kMinTimeStep && f.it < kMaxSubsteps) {
+        if (k == cap) return kCapped;
+        ++k;
+        ++f.it;
+        double Ex = 0.0, Ey = 0.0, Ez = 0.0;
+        if (in) {
+            const double* e = M.erec + 12 * (int64_t)f.cur;
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        const double* e = E + 3 * (int64_t)nd[i];
-        Ex = Ex + __ldg(e) * lam[i];
-        Ey = Ey + __ldg(e + 1) * lam[i];
-        Ez = Ez + __ldg(e + 2) * lam[i];
+            for (int q = 0; q < 4; ++q) {
+                Ex = Ex + __ldg(e + 3 * q) * lam[q];
+                Ey = Ey + __ldg(e + 3 * q + 1) * lam[q];
+                Ez = Ez + __ldg(e + 3 * q + 2) * lam[q];
+            }
+        }
+        // CrossTetrahedron::adaptiveTimeStep with |B| = 0
+        double adt = f.rem;
+        double Em = sqrt(Ex * Ex + Ey * Ey + Ez * Ez);
+        if (Em > 1e-10) {
+            double acc = Em * fabs(qm);
+            if (acc > 1e-10 && f.vstart > 1.0) adt = fmin(adt, 0.1 * f.vstart / acc);
+        }
+        adt = fmax(adt, f.rem * pp.floor_ratio);
+        adt = fmin(adt, f.rem);
+        const double sx = f.px, sy = f.py, sz = f.pz;
+        if (fabs(qm) > 1e-20) {
+            double h = qm * (0.5 * adt);
+            f.vx = f.vx + Ex * h; f.vy = f.vy + Ey * h; f.vz = f.vz + Ez * h;
+            f.vx = f.vx + Ex * h; f.vy = f.vy + Ey * h; f.vz = f.vz + Ez * h;
+        }
+        f.px = f.px + f.vx * adt;
+        f.py = f.py + f.vy * adt;
+        f.pz = f.pz + f.vz * adt;
+        double le[4];
+        if (bary64(M, f.cur, f.px, f.py, f.pz, le)) {
+            if (pp.deposit) {
+                if (in) {
+                    // the segment stayed in the tet: the symmetric sample points sum to
+                    // q*w*lambda(midpoint) for the segment-cloud and Gauss-3 kernels
+                    double tx = f.px - sx, ty = f.py - sy, tz = f.pz - sz;
+                    bool tiny = sqrt(tx * tx + ty * ty + tz * tz) < 1e-15;
+                    int4 tn = rec_nodes(M, f.cur);
+                    int nd[4] = {tn.x, tn.y, tn.z, tn.w};
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        double lk = tiny ? lam[q] : (pp.dep_kernel == 0 ? le[q] : 0.5 * (lam[q] + le[q]));
+                        fx_atomic_add(rlo + nd[q], rhi + nd[q], fx_from_double((qw * lk) * pp.inv_uq));
+                    }
+                } else {
+                    deposit_traj(M, S, pp, f.cur, sx, sy, sz, f.px, f.py, f.pz, rlo, rhi);
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q) lam[q] = le[q];
+            in = true;
+        } else {
+            int nt = locate(M, f.px, f.py, f.pz, f.cur);
+            if (nt < 0) return kLost;
+            f.cur = nt;
+            if (pp.deposit) deposit_traj(M, S, pp, nt, sx, sy, sz, f.px, f.py, f.pz, rlo, rhi);
+            in = bary64(M, nt, f.px, f.py, f.pz, lam);
+        }
+        f.rem -= adt;
+        ++nsub;
     }
+    return f.it >= kMaxSubsteps ? kLost : kDone;
 }
 
+__device__ __forceinline__ void finish_d(const MeshView& M, const ParticleStore& P, const SpeciesDev& S,
+                                         const PushParams& pp, LedgerDev* L, int64_t i, FlightD& f, int st,
+                                         PushStats& c)
+{
+    const double ke = 0.5 * S.m * (f.vx * f.vx + f.vy * f.vy + f.vz * f.vz);
+    int tet_out = f.cur;
+    if (st == kLost) {
+        ++c.nlost;
+        tet_out = resolve_lost(M, S, pp, L, f.px, f.py, f.pz, ke, f.cur);
+    }
+    c.ke_sum += ke;  // updateStatistics counts every stored particle (PICCycle.cpp:941-966)
+    if (tet_out >= 0) {
+        ++c.nact;
+        if (pp.do_mcc && S.mcc_enabled && mcc_elastic(S, pp, P.id[i], f.vx, f.vy, f.vz)) ++c.nhit;
+    }
+    P.x[i] = f.px; P.y[i] = f.py; P.z[i] = f.pz;
+    P.vx[i] = f.vx; P.vy[i] = f.vy; P.vz[i] = f.vz;
+    P.tet[i] = tet_out;
+}
+
+__device__ __forceinline__ void defer_store_d(const ParticleStore& P, const DeferList& D, unsigned slot, int64_t i,
+                                              const FlightD& f)
+{
+    D.idx[slot] = (uint32_t)i;
+    D.it[slot] = f.it;
+    D.rem[slot] = f.rem;
+    D.vstart[slot] = f.vstart;
+    P.x[i] = f.px; P.y[i] = f.py; P.z[i] = f.pz;
+    P.vx[i] = f.vx; P.vy[i] = f.vy; P.vz[i] = f.vz;
+    P.tet[i] = f.cur;
+}
+
+// Pass 1: every stored particle, at most kCap1 sub-steps.
 __global__ void __launch_bounds__(256) k_push_f64(MeshView M, ParticleStore P, SpeciesDev S, PushParams pp,
-                                                  const double* __restrict__ E, unsigned long long* rlo,
-                                                  unsigned long long* rhi, LedgerDev* L, double* ke_part)
+                                                  DeferList D, unsigned long long* rlo, unsigned long long* rhi,
+                                                  LedgerDev* L, double* ke_part)
 {
     const int64_t n = *P.count;
-    double ke_sum = 0.0;
-    unsigned long long nsub = 0, nlost = 0, nhit = 0, nact = 0;
-    const double qm = S.qm;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        int t0 = P.tet[i];
-        if (t0 <= kTetAbsorbed) continue;
-        double px = P.x[i], py = P.y[i], pz = P.z[i];
-        double vx = P.vx[i], vy = P.vy[i], vz = P.vz[i];
-        const double vstart = sqrt(vx * vx + vy * vy + vz * vz);
-        int cur = locate(M, px, py, pz, t0);
-        bool lost = false;
-        int tet_out;
-        if (cur < 0) {
-            lost = true;
-            cur = 0;  // result.final_element stays 0 (PICParticleAlgorithms.cpp:543,577)
-        } else {
-            double remaining = pp.dt;
-            int it = 0;
-            while (remaining > kMinTimeStep && it < kMaxSubsteps) {
-                ++it;
-                double Ex, Ey, Ez;
-                gather_e(M, E, cur, px, py, pz, Ex, Ey, Ez);
-                // CrossTetrahedron::adaptiveTimeStep with |B| = 0
-                double adt = remaining;
-                double Em = sqrt(Ex * Ex + Ey * Ey + Ez * Ez);
-                if (Em > 1e-10) {
-                    double acc = Em * fabs(qm);
-                    if (acc > 1e-10 && vstart > 1.0) adt = fmin(adt, 0.1 * vstart / acc);
+    PushStats c{0.0, 0ull, 0ull, 0ull, 0ull};
+    const int lane = threadIdx.x & 31;
+    const int64_t gwarp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t base = gwarp * 32; base < n; base += nwarps * 32) {
+        const int64_t i = base + lane;
+        int st = -1;
+        FlightD f;
+        if (i < n) {
+            int t0 = P.tet[i];
+            f.vx = P.vx[i]; f.vy = P.vy[i]; f.vz = P.vz[i];
+            if (t0 <= kTetAbsorbed) {
+                // updateStatistics sums every particle the container still holds (PICCycle.cpp:941-966)
+                c.ke_sum += 0.5 * S.m * (f.vx * f.vx + f.vy * f.vy + f.vz * f.vz);
+            } else {
+                f.px = P.x[i]; f.py = P.y[i]; f.pz = P.z[i];
+                f.vstart = sqrt(f.vx * f.vx + f.vy * f.vy + f.vz * f.vz);
+                f.rem = pp.dt;
+                f.it = 0;
+                f.cur = locate(M, f.px, f.py, f.pz, t0);
+                if (f.cur < 0) {
+                    f.cur = 0;  // result.final_element stays 0 (PICParticleAlgorithms.cpp:543,577)
+                    st = kLost;
+                } else {
+                    st = advance_d(M, S, pp, f, kCap1, rlo, rhi, c.nsub);
                 }
-                adt = fmax(adt, remaining * pp.floor_ratio);
-                adt = fmin(adt, remaining);
-                const double sx = px, sy = py, sz = pz;
-                if (fabs(qm) > 1e-20) {
-                    double f = qm * (0.5 * adt);
-                    vx = vx + Ex * f; vy = vy + Ey * f; vz = vz + Ez * f;
-                    vx = vx + Ex * f; vy = vy + Ey * f; vz = vz + Ez * f;
-                }
-                px = px + vx * adt;
-                py = py + vy * adt;
-                pz = pz + vz * adt;
-                double lam[4];
-                if (!bary64(M, cur, px, py, pz, lam)) {
-                    int nt = locate(M, px, py, pz, cur);
-                    if (nt < 0) {
-                        lost = true;
-                        break;
-                    }
-                    cur = nt;
-                }
-                if (pp.deposit) deposit_traj(M, S, pp, cur, sx, sy, sz, px, py, pz, rlo, rhi);
-                remaining -= adt;
-                ++nsub;
             }
-            if (it >= kMaxSubsteps) lost = true;
         }
-        tet_out = cur;
-        const double ke = 0.5 * S.m * (vx * vx + vy * vy + vz * vz);
-        if (lost) {
-            ++nlost;
-            tet_out = resolve_lost(M, S, pp, L, px, py, pz, ke, cur);
+        unsigned slot = warp_append(st == kCapped, D.count);
+        if (st == kCapped && slot < D.cap) {
+            defer_store_d(P, D, slot, i, f);
+        } else if (st >= 0) {
+            if (st == kCapped) st = advance_d(M, S, pp, f, 0x7fffffff, rlo, rhi, c.nsub);
+            finish_d(M, P, S, pp, L, i, f, st, c);
         }
-        ke_sum += ke;  // updateStatistics counts every stored particle (PICCycle.cpp:941-966)
-        if (tet_out >= 0) {
-            ++nact;
-            if (pp.do_mcc && S.mcc_enabled && mcc_elastic(S, pp, P.id[i], vx, vy, vz)) ++nhit;
+    }
+    block_stats(c, L, ke_part);
+}
+
+// Passes 2 and 3 over a deferred list (see k_push_mixed_more).
+__global__ void __launch_bounds__(256) k_push_f64_more(MeshView M, ParticleStore P, SpeciesDev S, PushParams pp,
+                                                       DeferList Din, DeferList Dout, int cap, unsigned long long* rlo,
+                                                       unsigned long long* rhi, LedgerDev* L, double* ke_part)
+{
+    const int64_t n = (int64_t)min(*Din.count, Din.cap);
+    PushStats c{0.0, 0ull, 0ull, 0ull, 0ull};
+    const int lane = threadIdx.x & 31;
+    const int64_t gwarp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const bool chain = Dout.count != nullptr;
+    for (int64_t base = gwarp * 32; base < n; base += nwarps * 32) {
+        const int64_t e = base + lane;
+        int st = -1;
+        FlightD f;
+        int64_t i = 0;
+        if (e < n) {
+            i = Din.idx[e];
+            f.cur = P.tet[i];
+            f.px = P.x[i]; f.py = P.y[i]; f.pz = P.z[i];
+            f.vx = P.vx[i]; f.vy = P.vy[i]; f.vz = P.vz[i];
+            f.it = Din.it[e];
+            f.rem = Din.rem[e];
+            f.vstart = Din.vstart[e];
+            st = advance_d(M, S, pp, f, chain ? cap : 0x7fffffff, rlo, rhi, c.nsub);
         }
-        P.x[i] = px; P.y[i] = py; P.z[i] = pz;
-        P.vx[i] = vx; P.vy[i] = vy; P.vz[i] = vz;
-        P.tet[i] = tet_out;
-    }
-    // block reduction of the statistics (fixed order -> deterministic)
-    __shared__ double sk[256];
-    __shared__ unsigned long long sc[4][8];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int o = 16; o > 0; o >>= 1) {
-        nsub += __shfl_down_sync(0xffffffffu, nsub, o);
-        nlost += __shfl_down_sync(0xffffffffu, nlost, o);
-        nhit += __shfl_down_sync(0xffffffffu, nhit, o);
-        nact += __shfl_down_sync(0xffffffffu, nact, o);
-    }
-    if (lane == 0) {
-        sc[0][warp] = nsub; sc[1][warp] = nlost; sc[2][warp] = nhit; sc[3][warp] = nact;
-    }
-    sk[threadIdx.x] = ke_sum;
-    __syncthreads();
-    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-        if (threadIdx.x < s) sk[threadIdx.x] += sk[threadIdx.x + s];
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) {
-        ke_part[blockIdx.x] += sk[0];
-        unsigned long long a = 0, b = 0, c = 0, d = 0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
-            a += sc[0][w]; b += sc[1][w]; c += sc[2][w]; d += sc[3][w];
+        unsigned slot = chain ? warp_append(st == kCapped, Dout.count) : 0xffffffffu;
+        if (st == kCapped && chain && slot < Dout.cap) {
+            defer_store_d(P, Dout, slot, i, f);
+        } else if (st >= 0) {
+            if (st == kCapped) st = advance_d(M, S, pp, f, 0x7fffffff, rlo, rhi, c.nsub);
+            finish_d(M, P, S, pp, L, i, f, st, c);
         }
-        if (a) atomicAdd(&L->substeps, a);
-        if (b) atomicAdd(&L->lost_events, b);
-        if (c) atomicAdd(&L->mcc_hits, c);
-        if (d) atomicAdd(&L->active, d);
     }
+    block_stats(c, L, ke_part);
 }
 
 // Standalone MCC pass (executeBackgroundMccStep, CollisionPicAdapter.cpp:338-434).
@@ -222,17 +297,41 @@ __global__ void k_mcc_f64(ParticleStore P, SpeciesDev S, PushParams pp, LedgerDe
     if (nhit) atomicAdd(&L->mcc_hits, nhit);
 }
 
-void launch_push_f64(const MeshView& M, const ParticleStore& P, const SpeciesDev& S, const PushParams& pp,
-                     const double* E, unsigned long long* rlo, unsigned long long* rhi, LedgerDev* L, double* ke_part,
-                     int grid, cudaStream_t st)
+// Per-tet copy of the nodal E of its 4 nodes.
+__global__ void k_refresh_erec(int64_t T, const int4* __restrict__ tet, const double* __restrict__ E, double* erec)
 {
-    k_push_f64<<<grid, 256, 0, st>>>(M, P, S, pp, E, rlo, rhi, L, ke_part);
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < T; t += (int64_t)gridDim.x * blockDim.x) {
+        int4 tn = tet[t];
+        int nd[4] = {tn.x, tn.y, tn.z, tn.w};
+        double* r = erec + 12 * t;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            r[3 * q] = E[3 * (int64_t)nd[q]];
+            r[3 * q + 1] = E[3 * (int64_t)nd[q] + 1];
+            r[3 * q + 2] = E[3 * (int64_t)nd[q] + 2];
+        }
+    }
+}
+
+void launch_push_f64(const MeshView& M, const ParticleStore& P, const SpeciesDev& S, const PushParams& pp,
+                     const DeferList& D1, const DeferList& D2, unsigned long long* rlo, unsigned long long* rhi,
+                     LedgerDev* L, double* ke_part, int grid, cudaStream_t st)
+{
+    k_push_f64<<<grid, 256, 0, st>>>(M, P, S, pp, D1, rlo, rhi, L, ke_part);
+    k_push_f64_more<<<grid, 256, 0, st>>>(M, P, S, pp, D1, D2, kCap2, rlo, rhi, L, ke_part);
+    DeferList none{};
+    k_push_f64_more<<<grid, 256, 0, st>>>(M, P, S, pp, D2, none, 0, rlo, rhi, L, ke_part);
 }
 
 void launch_mcc_f64(const ParticleStore& P, const SpeciesDev& S, const PushParams& pp, LedgerDev* L, int grid,
                     cudaStream_t st)
 {
     k_mcc_f64<<<grid, 256, 0, st>>>(P, S, pp, L);
+}
+
+void launch_refresh_erec(int64_t T, const int4* tet, const double* E, double* erec, cudaStream_t st)
+{
+    k_refresh_erec<<<148 * 8, 256, 0, st>>>(T, tet, E, erec);
 }
 
 }  // namespace scdat

@@ -1,12 +1,18 @@
 // push_mixed.cu -- the precision form of the particle step.
 //
 // Particles store FP32 positions relative to the origin node (local vertex 0) of their tet
-// and FP32 velocities (28 bytes with the tet id, against 52 in FP64).  Gather, adaptive
-// sub-step, Boris and the in-tet test run in FP32 on the FP32 inverse Jacobians and FP32
-// nodal E; a move into a face neighbour is re-based in FP32 from the FP64 node difference;
-// anything farther (walk, grid lookup, boundary events) reconstructs the FP64 absolute
-// position and uses the FP64 locate.  Deposit weights are FP32 barycentrics promoted to
-// FP64 before the exact fixed-point accumulation.  The step structure is the reference's
+// and FP32 velocities (28 bytes with the tet id, against 52 in FP64).  Every tet has one
+// 128-byte record: FP32 inverse Jacobian, the nodal E of its 4 nodes as E0 and three
+// differences (refreshed after every field solve) and its node ids, so a sub-step reads one
+// cache line.  Gather, adaptive sub-step, Boris and the in-tet test run in FP32; a move into
+// a face neighbour is re-based in FP32 from the FP64 node difference; anything farther (walk,
+// grid lookup, boundary events) reconstructs the FP64 absolute position and uses the FP64
+// locate.  Deposit weights are FP32 barycentrics promoted to FP64 before the exact
+// fixed-point accumulation.
+//
+// Sub-steps run in passes so that warps stay converged: pass 1 gives every particle at most
+// kCap1 sub-steps and appends the unfinished ones to a list; pass 2 gives those up to kCap2
+// more; pass 3 finishes the rest.  The step structure is the reference's
 // CrossTetrahedron::integrateTrajectory (PICParticleAlgorithms.cpp:536-740).
 #include "push.cuh"
 
@@ -21,27 +27,47 @@ __device__ __forceinline__ bool inside_f(const float l[4])
     return ok;
 }
 
-struct GeomF {
+// record layout (64 words): [0..8] J^-1, [9..11] E0, [12..20] E1-E0, E2-E0, E3-E0,
+// [21..24] node ids, [25..28] face neighbours, [29..31] unused | [32..43] origin minus the
+// origin of each face neighbour (FP32), [44..63] unused
+struct TetRec {
     float j[9];
+    float e0[3];
+    float d[9];
+    int nd[4];
 };
 
-__device__ __forceinline__ GeomF load_geomf(const MeshView& M, int t)
+__device__ __forceinline__ TetRec load_rec(const MeshView& M, int t)
 {
-    const float4* g = reinterpret_cast<const float4*>(M.geomf + 12 * (int64_t)t);
-    float4 a = __ldg(g), b = __ldg(g + 1);
-    float c = __ldg(M.geomf + 12 * (int64_t)t + 8);
-    GeomF G;
-    G.j[0] = a.x; G.j[1] = a.y; G.j[2] = a.z; G.j[3] = a.w;
-    G.j[4] = b.x; G.j[5] = b.y; G.j[6] = b.z; G.j[7] = b.w; G.j[8] = c;
-    return G;
+    const float4* g = reinterpret_cast<const float4*>(M.trec + 64 * (int64_t)t);
+    float4 a = __ldg(g), b = __ldg(g + 1), c = __ldg(g + 2), d = __ldg(g + 3), e = __ldg(g + 4), f = __ldg(g + 5),
+           h = __ldg(g + 6);
+    TetRec R;
+    R.j[0] = a.x; R.j[1] = a.y; R.j[2] = a.z; R.j[3] = a.w;
+    R.j[4] = b.x; R.j[5] = b.y; R.j[6] = b.z; R.j[7] = b.w;
+    R.j[8] = c.x; R.e0[0] = c.y; R.e0[1] = c.z; R.e0[2] = c.w;
+    R.d[0] = d.x; R.d[1] = d.y; R.d[2] = d.z; R.d[3] = d.w;
+    R.d[4] = e.x; R.d[5] = e.y; R.d[6] = e.z; R.d[7] = e.w;
+    R.d[8] = f.x;
+    R.nd[0] = __float_as_int(f.y); R.nd[1] = __float_as_int(f.z); R.nd[2] = __float_as_int(f.w);
+    R.nd[3] = __float_as_int(h.x);
+    return R;
 }
 
-__device__ __forceinline__ void baryf(const GeomF& G, float rx, float ry, float rz, float l[4])
+__device__ __forceinline__ void baryj(const float* j, float rx, float ry, float rz, float l[4])
 {
-    l[1] = G.j[0] * rx + G.j[1] * ry + G.j[2] * rz;
-    l[2] = G.j[3] * rx + G.j[4] * ry + G.j[5] * rz;
-    l[3] = G.j[6] * rx + G.j[7] * ry + G.j[8] * rz;
+    l[1] = j[0] * rx + j[1] * ry + j[2] * rz;
+    l[2] = j[3] * rx + j[4] * ry + j[5] * rz;
+    l[3] = j[6] * rx + j[7] * ry + j[8] * rz;
     l[0] = 1.0f - l[1] - l[2] - l[3];
+}
+
+__device__ __forceinline__ void load_j(const MeshView& M, int t, float j[9])
+{
+    const float4* g = reinterpret_cast<const float4*>(M.trec + 64 * (int64_t)t);
+    float4 a = __ldg(g), b = __ldg(g + 1);
+    j[0] = a.x; j[1] = a.y; j[2] = a.z; j[3] = a.w; j[4] = b.x; j[5] = b.y; j[6] = b.z; j[7] = b.w;
+    j[8] = __ldg(M.trec + 64 * (int64_t)t + 8);
 }
 
 __device__ __forceinline__ double3 origin(const MeshView& M, int t)
@@ -60,237 +86,339 @@ __device__ __forceinline__ void dep_point_f(Fx128 acc[4], bool& any, const float
     any = true;
 }
 
-// Relocate the FP32 offset r (relative to origin of `cur`): neighbour list first in FP32,
-// then the FP64 walk / grid lookup.  Returns the new tet or -1; r and the carried start
-// offset s are re-based to the new origin.
-__device__ __forceinline__ int relocate_f(const MeshView& M, int cur, float& rx, float& ry, float& rz, float& sx,
-                                          float& sy, float& sz)
+// Relocate the FP32 offset r (relative to the origin of `cur`) by a straight walk across the
+// most violated face, re-basing r (and the carried start offset s) with each neighbour's
+// stored origin shift; a walk that meets a boundary face or runs long falls back to the FP64
+// locate on the absolute position.  Returns the new tet or -1.
+static __device__ __noinline__ int relocate_f(const MeshView& M, int cur, float& rx, float& ry, float& rz, float& sx,
+                                              float& sy, float& sz)
 {
-    const double3 oc = origin(M, cur);
-    if (M.use_nbr) {
-        int4 nb = __ldg(M.nbr + cur);
-        int cand[4] = {nb.x, nb.y, nb.z, nb.w};
+    int t = cur;
+    float qx = rx, qy = ry, qz = rz, ox = 0.f, oy = 0.f, oz = 0.f;
+    float l[4], j[9];
+    load_j(M, t, j);
+    baryj(j, qx, qy, qz, l);
+    for (int k = 0; k < kWalkSteps; ++k) {
+        int f = 0;
 #pragma unroll
-        for (int f = 0; f < 4; ++f) {
-            int t = cand[f];
-            if (t < 0) continue;
-            double3 on = origin(M, t);
-            float dx = (float)(oc.x - on.x), dy = (float)(oc.y - on.y), dz = (float)(oc.z - on.z);
-            float qx = rx + dx, qy = ry + dy, qz = rz + dz;
-            float l[4];
-            baryf(load_geomf(M, t), qx, qy, qz, l);
-            if (inside_f(l)) {
-                rx = qx; ry = qy; rz = qz;
-                sx += dx; sy += dy; sz += dz;
-                return t;
-            }
+        for (int i = 1; i < 4; ++i)
+            if (l[i] < l[f]) f = i;
+        const float* rec = M.trec + 64 * (int64_t)t;
+        int nt = __float_as_int(__ldg(rec + 25 + f));
+        if (nt < 0) break;
+        float dx = __ldg(rec + 32 + 3 * f), dy = __ldg(rec + 33 + 3 * f), dz = __ldg(rec + 34 + 3 * f);
+        qx += dx; qy += dy; qz += dz;
+        ox += dx; oy += dy; oz += dz;
+        t = nt;
+        load_j(M, t, j);
+        baryj(j, qx, qy, qz, l);
+        if (inside_f(l)) {
+            rx = qx; ry = qy; rz = qz;
+            sx += ox; sy += oy; sz += oz;
+            return t;
         }
+        if (!(l[0] == l[0])) break;
     }
+    const double3 oc = origin(M, cur);
     double px = oc.x + (double)rx, py = oc.y + (double)ry, pz = oc.z + (double)rz;
-    int t = locate_far(M, px, py, pz, cur);
-    if (t < 0) return -1;
-    double3 on = origin(M, t);
+    int tt = locate_far(M, px, py, pz, cur);
+    if (tt < 0) return -1;
+    double3 on = origin(M, tt);
     float dx = (float)(oc.x - on.x), dy = (float)(oc.y - on.y), dz = (float)(oc.z - on.z);
     rx = (float)(px - on.x); ry = (float)(py - on.y); rz = (float)(pz - on.z);
     sx += dx; sy += dy; sz += dz;
-    return t;
+    return tt;
 }
 
+// Deposit along start -> end (both FP32 offsets from the origin of t) into t: the sample
+// points that lie in t (the sub-step changed tet), summed in FP32 per node, then converted
+// once to fixed point.
+static __device__ __noinline__ void deposit_traj_f(const MeshView& M, const SpeciesDev& S, const PushParams& pp,
+                                                   int t, float sx, float sy, float sz, float rx, float ry, float rz,
+                                                   unsigned long long* rlo, unsigned long long* rhi)
+{
+    float j[9];
+    load_j(M, t, j);
+    float sum[4] = {0.f, 0.f, 0.f, 0.f};
+    double cw = S.cw_seg;
+    bool any = false;
+    const int nseg = pp.nseg;
+    float tx = rx - sx, ty = ry - sy, tz = rz - sz;
+    if (sqrtf(tx * tx + ty * ty + tz * tz) < 1e-15f || pp.dep_kernel == 0) {
+        float q0[4];
+        if (pp.dep_kernel == 0 && !(sqrtf(tx * tx + ty * ty + tz * tz) < 1e-15f)) baryj(j, rx, ry, rz, q0);
+        else baryj(j, sx, sy, sz, q0);
+        if (inside_f(q0)) {
+            for (int q = 0; q < 4; ++q) sum[q] = q0[q];
+            any = true;
+        }
+        cw = S.q * S.w;
+    } else {
+        float ls[4], dl[4];
+        baryj(j, sx, sy, sz, ls);
+        dl[1] = j[0] * tx + j[1] * ty + j[2] * tz;
+        dl[2] = j[3] * tx + j[4] * ty + j[5] * tz;
+        dl[3] = j[6] * tx + j[7] * ty + j[8] * tz;
+        dl[0] = -dl[1] - dl[2] - dl[3];
+        if (pp.dep_kernel == 2) {
+            const float gn[3] = {-0.7745966692414834f, 0.0f, 0.7745966692414834f};
+            const float gw[3] = {5.0f / 18.0f, 8.0f / 18.0f, 5.0f / 18.0f};
+            for (int sg = 0; sg < nseg; ++sg) {
+                float tc = ((float)sg + 0.5f) / (float)nseg, th = 0.5f / (float)nseg;
+                for (int q = 0; q < 3; ++q) {
+                    float tau = tc + th * gn[q];
+                    float lq[4] = {ls[0] + tau * dl[0], ls[1] + tau * dl[1], ls[2] + tau * dl[2], ls[3] + tau * dl[3]};
+                    if (inside_f(lq)) {
+                        for (int k = 0; k < 4; ++k) sum[k] = fmaf(gw[q], lq[k], sum[k]);
+                        any = true;
+                    }
+                }
+            }
+        } else {
+            for (int sg = 0; sg < nseg; ++sg) {
+                float tau = ((float)sg + 0.5f) / (float)nseg;
+                float lq[4] = {ls[0] + tau * dl[0], ls[1] + tau * dl[1], ls[2] + tau * dl[2], ls[3] + tau * dl[3]};
+                if (inside_f(lq)) {
+                    for (int k = 0; k < 4; ++k) sum[k] += lq[k];
+                    any = true;
+                }
+            }
+        }
+    }
+    if (!any) return;
+    const int* nd = reinterpret_cast<const int*>(M.trec + 64 * (int64_t)t + 21);
+    for (int k = 0; k < 4; ++k) {
+        int node = __ldg(nd + k);
+        fx_atomic_add(rlo + node, rhi + node, fx_from_double((cw * (double)sum[k]) * pp.inv_uq));
+    }
+}
+
+struct FlightF {
+    float rx, ry, rz, vx, vy, vz;
+    float rem, vstart;
+    int cur, it;
+};
+
+// Run sub-steps until the step's time is used up, the particle is lost, or `cap` sub-steps
+// ran in this call.
+__device__ __forceinline__ int advance_f(const MeshView& M, const SpeciesDev& S, const PushParams& pp, FlightF& f,
+                                         int cap, unsigned long long* rlo, unsigned long long* rhi,
+                                         unsigned long long& nsub)
+{
+    const float qm = (float)S.qm;
+    const float floor_ratio = (float)pp.floor_ratio;
+    const double qw = S.q * S.w;
+    TetRec R = load_rec(M, f.cur);
+    float l[4];
+    baryj(R.j, f.rx, f.ry, f.rz, l);
+    bool in = inside_f(l);
+    int k = 0;
+    while (f.rem > 1e-20f && f.it < kMaxSubsteps) {
+        if (k == cap) return kCapped;
+        ++k;
+        ++f.it;
+        float Ex = 0.f, Ey = 0.f, Ez = 0.f;
+        if (in) {  // E = E0 + sum_i lambda_i (E_i - E0), i = 1..3
+            Ex = fmaf(l[1], R.d[0], fmaf(l[2], R.d[3], fmaf(l[3], R.d[6], R.e0[0])));
+            Ey = fmaf(l[1], R.d[1], fmaf(l[2], R.d[4], fmaf(l[3], R.d[7], R.e0[1])));
+            Ez = fmaf(l[1], R.d[2], fmaf(l[2], R.d[5], fmaf(l[3], R.d[8], R.e0[2])));
+        }
+        float adt = f.rem;
+        float Em = sqrtf(Ex * Ex + Ey * Ey + Ez * Ez);
+        if (Em > 1e-10f) {
+            float acc = Em * fabsf(qm);
+            if (acc > 1e-10f && f.vstart > 1.0f) adt = fminf(adt, 0.1f * f.vstart / acc);
+        }
+        adt = fmaxf(adt, f.rem * floor_ratio);
+        adt = fminf(adt, f.rem);
+        float sx = f.rx, sy = f.ry, sz = f.rz;
+        if (fabsf(qm) > 1e-20f) {
+            float h = 2.0f * (qm * (0.5f * adt));
+            f.vx = fmaf(h, Ex, f.vx);
+            f.vy = fmaf(h, Ey, f.vy);
+            f.vz = fmaf(h, Ez, f.vz);
+        }
+        f.rx = fmaf(f.vx, adt, f.rx);
+        f.ry = fmaf(f.vy, adt, f.ry);
+        f.rz = fmaf(f.vz, adt, f.rz);
+        float le[4];
+        baryj(R.j, f.rx, f.ry, f.rz, le);
+        if (inside_f(le)) {
+            if (pp.deposit) {
+                if (in) {
+                    float tx = f.rx - sx, ty = f.ry - sy, tz = f.rz - sz;
+                    bool tiny = sqrtf(tx * tx + ty * ty + tz * tz) < 1e-15f;
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        float lk = tiny ? l[q] : (pp.dep_kernel == 0 ? le[q] : 0.5f * (l[q] + le[q]));
+                        fx_atomic_add(rlo + R.nd[q], rhi + R.nd[q], fx_from_double((qw * (double)lk) * pp.inv_uq));
+                    }
+                } else {
+                    deposit_traj_f(M, S, pp, f.cur, sx, sy, sz, f.rx, f.ry, f.rz, rlo, rhi);
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q) l[q] = le[q];
+            in = true;
+        } else {
+            int nt = relocate_f(M, f.cur, f.rx, f.ry, f.rz, sx, sy, sz);
+            if (nt < 0) return kLost;
+            f.cur = nt;
+            R = load_rec(M, nt);
+            if (pp.deposit) deposit_traj_f(M, S, pp, nt, sx, sy, sz, f.rx, f.ry, f.rz, rlo, rhi);
+            baryj(R.j, f.rx, f.ry, f.rz, l);
+            in = inside_f(l);
+        }
+        f.rem -= adt;
+        ++nsub;
+    }
+    return f.it >= kMaxSubsteps ? kLost : kDone;
+}
+
+// End of a particle's step: boundary events for a lost particle, the statistics, the fused
+// MCC, and the store.
+__device__ __forceinline__ void finish_f(const MeshView& M, const ParticleStore& P, const SpeciesDev& S,
+                                         const PushParams& pp, LedgerDev* L, int64_t i, FlightF& f, int st,
+                                         PushStats& c)
+{
+    double dvx = f.vx, dvy = f.vy, dvz = f.vz;
+    const double ke = 0.5 * S.m * (dvx * dvx + dvy * dvy + dvz * dvz);
+    int tet_out = f.cur;
+    if (st == kLost) {
+        ++c.nlost;
+        double px, py, pz;
+        int hint = f.cur;
+        if (f.cur >= 0) {
+            double3 o = origin(M, f.cur);
+            px = o.x + (double)f.rx; py = o.y + (double)f.ry; pz = o.z + (double)f.rz;
+        } else {
+            px = f.rx; py = f.ry; pz = f.rz;
+            hint = 0;
+        }
+        tet_out = resolve_lost(M, S, pp, L, px, py, pz, ke, hint);
+        if (tet_out >= 0) {
+            double3 o = origin(M, tet_out);
+            f.rx = (float)(px - o.x); f.ry = (float)(py - o.y); f.rz = (float)(pz - o.z);
+        } else {
+            // inactive particles keep an absolute FP32 position for read-back
+            f.rx = (float)px; f.ry = (float)py; f.rz = (float)pz;
+        }
+    }
+    c.ke_sum += ke;
+    if (tet_out >= 0) {
+        ++c.nact;
+        if (pp.do_mcc && S.mcc_enabled && mcc_elastic(S, pp, P.id[i], dvx, dvy, dvz)) {
+            ++c.nhit;
+            f.vx = (float)dvx; f.vy = (float)dvy; f.vz = (float)dvz;
+        }
+    }
+    P.xf[i] = f.rx; P.yf[i] = f.ry; P.zf[i] = f.rz;
+    P.vxf[i] = f.vx; P.vyf[i] = f.vy; P.vzf[i] = f.vz;
+    P.tet[i] = tet_out;
+}
+
+__device__ __forceinline__ void defer_store_f(const ParticleStore& P, const DeferList& D, unsigned slot, int64_t i,
+                                              const FlightF& f)
+{
+    D.idx[slot] = (uint32_t)i;
+    D.it[slot] = f.it;
+    D.rem[slot] = f.rem;
+    D.vstart[slot] = f.vstart;
+    P.xf[i] = f.rx; P.yf[i] = f.ry; P.zf[i] = f.rz;
+    P.vxf[i] = f.vx; P.vyf[i] = f.vy; P.vzf[i] = f.vz;
+    P.tet[i] = f.cur;
+}
+
+// Pass 1: every stored particle, at most kCap1 sub-steps.
 __global__ void __launch_bounds__(256) k_push_mixed(MeshView M, ParticleStore P, SpeciesDev S, PushParams pp,
-                                                    const float* __restrict__ Ef, unsigned long long* rlo,
-                                                    unsigned long long* rhi, LedgerDev* L, double* ke_part)
+                                                    DeferList D, unsigned long long* rlo, unsigned long long* rhi,
+                                                    LedgerDev* L, double* ke_part)
 {
     const int64_t n = *P.count;
-    double ke_sum = 0.0;
-    unsigned long long nsub = 0, nlost = 0, nhit = 0, nact = 0;
-    const float qm = (float)S.qm;
-    const float dtf = (float)pp.dt;
-    const float floor_ratio = (float)pp.floor_ratio;
-    const int nseg = pp.nseg;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        int cur = P.tet[i];
-        if (cur <= kTetAbsorbed) continue;
-        float rx = P.xf[i], ry = P.yf[i], rz = P.zf[i];
-        float vx = P.vxf[i], vy = P.vyf[i], vz = P.vzf[i];
-        const float vstart = sqrtf(vx * vx + vy * vy + vz * vz);
-        bool lost = false;
-        if (cur < 0) {
-            // no hint: the offset is absolute (set when the particle was placed outside the mesh)
-            double px = rx, py = ry, pz = rz;
-            int t = locate_far(M, px, py, pz, -1);
-            if (t < 0) {
-                lost = true;
+    PushStats c{0.0, 0ull, 0ull, 0ull, 0ull};
+    const int lane = threadIdx.x & 31;
+    const int64_t gwarp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t base = gwarp * 32; base < n; base += nwarps * 32) {
+        const int64_t i = base + lane;
+        int st = -1;
+        FlightF f;
+        if (i < n) {
+            f.cur = P.tet[i];
+            f.vx = P.vxf[i]; f.vy = P.vyf[i]; f.vz = P.vzf[i];
+            if (f.cur <= kTetAbsorbed) {
+                // updateStatistics sums every particle the container still holds (PICCycle.cpp:941-966)
+                double ux = f.vx, uy = f.vy, uz = f.vz;
+                c.ke_sum += 0.5 * S.m * (ux * ux + uy * uy + uz * uz);
             } else {
-                double3 o = origin(M, t);
-                rx = (float)(px - o.x); ry = (float)(py - o.y); rz = (float)(pz - o.z);
-                cur = t;
-            }
-        }
-        if (!lost) {
-            float remaining = dtf;
-            int it = 0;
-            while (remaining > 1e-20f && it < kMaxSubsteps) {
-                ++it;
-                GeomF G = load_geomf(M, cur);
-                int4 tn = __ldg(M.tet + cur);
-                float l[4];
-                baryf(G, rx, ry, rz, l);
-                float Ex = 0.f, Ey = 0.f, Ez = 0.f;
-                if (inside_f(l)) {
-                    int nd[4] = {tn.x, tn.y, tn.z, tn.w};
-#pragma unroll
-                    for (int k = 0; k < 4; ++k) {
-                        const float* e = Ef + 3 * (int64_t)nd[k];
-                        Ex = fmaf(__ldg(e), l[k], Ex);
-                        Ey = fmaf(__ldg(e + 1), l[k], Ey);
-                        Ez = fmaf(__ldg(e + 2), l[k], Ez);
-                    }
-                }
-                float adt = remaining;
-                float Em = sqrtf(Ex * Ex + Ey * Ey + Ez * Ez);
-                if (Em > 1e-10f) {
-                    float acc = Em * fabsf(qm);
-                    if (acc > 1e-10f && vstart > 1.0f) adt = fminf(adt, 0.1f * vstart / acc);
-                }
-                adt = fmaxf(adt, remaining * floor_ratio);
-                adt = fminf(adt, remaining);
-                float sx = rx, sy = ry, sz = rz;
-                if (fabsf(qm) > 1e-20f) {
-                    float f = qm * (0.5f * adt);
-                    vx = fmaf(2.0f * f, Ex, vx);
-                    vy = fmaf(2.0f * f, Ey, vy);
-                    vz = fmaf(2.0f * f, Ez, vz);
-                }
-                rx = fmaf(vx, adt, rx);
-                ry = fmaf(vy, adt, ry);
-                rz = fmaf(vz, adt, rz);
-                baryf(G, rx, ry, rz, l);
-                if (!inside_f(l)) {
-                    int nt = relocate_f(M, cur, rx, ry, rz, sx, sy, sz);
-                    if (nt < 0) {
-                        lost = true;
-                        break;
-                    }
-                    cur = nt;
-                    G = load_geomf(M, cur);
-                    tn = __ldg(M.tet + cur);
-                }
-                // deposit along start -> end in the post-move tet
-                Fx128 acc[4] = {{0ull, 0ll}, {0ull, 0ll}, {0ull, 0ll}, {0ull, 0ll}};
-                bool any = false;
-                float tx = rx - sx, ty = ry - sy, tz = rz - sz;
-                if (sqrtf(tx * tx + ty * ty + tz * tz) < 1e-15f) {
-                    float q0[4];
-                    baryf(G, sx, sy, sz, q0);
-                    if (inside_f(q0)) dep_point_f(acc, any, q0, S.q * S.w, pp.inv_uq);
-                } else if (pp.dep_kernel == 0) {
-                    float q0[4];
-                    baryf(G, rx, ry, rz, q0);
-                    if (inside_f(q0)) dep_point_f(acc, any, q0, S.q * S.w, pp.inv_uq);
-                } else {
-                    float ls[4], dl[4];
-                    baryf(G, sx, sy, sz, ls);
-                    dl[1] = G.j[0] * tx + G.j[1] * ty + G.j[2] * tz;
-                    dl[2] = G.j[3] * tx + G.j[4] * ty + G.j[5] * tz;
-                    dl[3] = G.j[6] * tx + G.j[7] * ty + G.j[8] * tz;
-                    dl[0] = -dl[1] - dl[2] - dl[3];
-                    if (pp.dep_kernel == 2) {
-                        const float gn[3] = {-0.7745966692414834f, 0.0f, 0.7745966692414834f};
-                        const double gw[3] = {5.0 / 18.0, 8.0 / 18.0, 5.0 / 18.0};
-                        for (int sg = 0; sg < nseg; ++sg) {
-                            float tc = ((float)sg + 0.5f) / (float)nseg, th = 0.5f / (float)nseg;
-#pragma unroll
-                            for (int q = 0; q < 3; ++q) {
-                                float tau = tc + th * gn[q];
-                                float lq[4] = {ls[0] + tau * dl[0], ls[1] + tau * dl[1], ls[2] + tau * dl[2],
-                                               ls[3] + tau * dl[3]};
-                                if (inside_f(lq)) dep_point_f(acc, any, lq, (S.q * gw[q] / (double)nseg) * S.w, pp.inv_uq);
-                            }
-                        }
+                f.rx = P.xf[i]; f.ry = P.yf[i]; f.rz = P.zf[i];
+                f.vstart = sqrtf(f.vx * f.vx + f.vy * f.vy + f.vz * f.vz);
+                f.rem = (float)pp.dt;
+                f.it = 0;
+                st = kDone;
+                if (f.cur < 0) {
+                    // no hint: the stored offset is an absolute position
+                    double px = f.rx, py = f.ry, pz = f.rz;
+                    int t = locate_far(M, px, py, pz, -1);
+                    if (t < 0) {
+                        st = kLost;
                     } else {
-                        for (int sg = 0; sg < nseg; ++sg) {
-                            float tau = ((float)sg + 0.5f) / (float)nseg;
-                            float lq[4] = {ls[0] + tau * dl[0], ls[1] + tau * dl[1], ls[2] + tau * dl[2],
-                                           ls[3] + tau * dl[3]};
-                            if (inside_f(lq)) dep_point_f(acc, any, lq, S.cw_seg, pp.inv_uq);
-                        }
+                        double3 o = origin(M, t);
+                        f.rx = (float)(px - o.x); f.ry = (float)(py - o.y); f.rz = (float)(pz - o.z);
+                        f.cur = t;
                     }
                 }
-                if (any && pp.deposit) {
-                    fx_atomic_add(rlo + tn.x, rhi + tn.x, acc[0]);
-                    fx_atomic_add(rlo + tn.y, rhi + tn.y, acc[1]);
-                    fx_atomic_add(rlo + tn.z, rhi + tn.z, acc[2]);
-                    fx_atomic_add(rlo + tn.w, rhi + tn.w, acc[3]);
-                }
-                remaining -= adt;
-                ++nsub;
-            }
-            if (it >= kMaxSubsteps) lost = true;
-        }
-        double dvx = vx, dvy = vy, dvz = vz;
-        const double ke = 0.5 * S.m * (dvx * dvx + dvy * dvy + dvz * dvz);
-        int tet_out = cur;
-        if (lost) {
-            ++nlost;
-            // absolute position in FP64 for the boundary events
-            double px, py, pz;
-            if (cur >= 0) {
-                double3 o = origin(M, cur);
-                px = o.x + (double)rx; py = o.y + (double)ry; pz = o.z + (double)rz;
-            } else {
-                px = rx; py = ry; pz = rz;
-                cur = 0;
-            }
-            tet_out = resolve_lost(M, S, pp, L, px, py, pz, ke, cur);
-            if (tet_out >= 0) {
-                double3 o = origin(M, tet_out);
-                rx = (float)(px - o.x); ry = (float)(py - o.y); rz = (float)(pz - o.z);
-            } else {
-                // inactive particles keep an absolute FP32 position for read-back
-                rx = (float)px; ry = (float)py; rz = (float)pz;
+                if (st != kLost) st = advance_f(M, S, pp, f, kCap1, rlo, rhi, c.nsub);
             }
         }
-        ke_sum += ke;
-        if (tet_out >= 0) {
-            ++nact;
-            if (pp.do_mcc && S.mcc_enabled && mcc_elastic(S, pp, P.id[i], dvx, dvy, dvz)) {
-                ++nhit;
-                vx = (float)dvx; vy = (float)dvy; vz = (float)dvz;
-            }
+        unsigned slot = warp_append(st == kCapped, D.count);
+        if (st == kCapped && slot < D.cap) {
+            defer_store_f(P, D, slot, i, f);
+        } else if (st >= 0) {
+            if (st == kCapped) st = advance_f(M, S, pp, f, 0x7fffffff, rlo, rhi, c.nsub);
+            finish_f(M, P, S, pp, L, i, f, st, c);
         }
-        P.xf[i] = rx; P.yf[i] = ry; P.zf[i] = rz;
-        P.vxf[i] = vx; P.vyf[i] = vy; P.vzf[i] = vz;
-        P.tet[i] = tet_out;
     }
-    __shared__ double sk[256];
-    __shared__ unsigned long long sc[4][8];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int o = 16; o > 0; o >>= 1) {
-        nsub += __shfl_down_sync(0xffffffffu, nsub, o);
-        nlost += __shfl_down_sync(0xffffffffu, nlost, o);
-        nhit += __shfl_down_sync(0xffffffffu, nhit, o);
-        nact += __shfl_down_sync(0xffffffffu, nact, o);
-    }
-    if (lane == 0) {
-        sc[0][warp] = nsub; sc[1][warp] = nlost; sc[2][warp] = nhit; sc[3][warp] = nact;
-    }
-    sk[threadIdx.x] = ke_sum;
-    __syncthreads();
-    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-        if (threadIdx.x < s) sk[threadIdx.x] += sk[threadIdx.x + s];
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) {
-        ke_part[blockIdx.x] += sk[0];
-        unsigned long long a = 0, b = 0, c = 0, d = 0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
-            a += sc[0][w]; b += sc[1][w]; c += sc[2][w]; d += sc[3][w];
+    block_stats(c, L, ke_part);
+}
+
+// Passes 2 and 3: continue the particles of list `Din` (up to `cap` sub-steps, then append
+// to Dout; with Dout.count == nullptr the particles run to the end).
+__global__ void __launch_bounds__(256) k_push_mixed_more(MeshView M, ParticleStore P, SpeciesDev S, PushParams pp,
+                                                         DeferList Din, DeferList Dout, int cap,
+                                                         unsigned long long* rlo, unsigned long long* rhi,
+                                                         LedgerDev* L, double* ke_part)
+{
+    const int64_t n = (int64_t)min(*Din.count, Din.cap);
+    PushStats c{0.0, 0ull, 0ull, 0ull, 0ull};
+    const int lane = threadIdx.x & 31;
+    const int64_t gwarp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const bool chain = Dout.count != nullptr;
+    for (int64_t base = gwarp * 32; base < n; base += nwarps * 32) {
+        const int64_t e = base + lane;
+        int st = -1;
+        FlightF f;
+        int64_t i = 0;
+        if (e < n) {
+            i = Din.idx[e];
+            f.cur = P.tet[i];
+            f.rx = P.xf[i]; f.ry = P.yf[i]; f.rz = P.zf[i];
+            f.vx = P.vxf[i]; f.vy = P.vyf[i]; f.vz = P.vzf[i];
+            f.it = Din.it[e];
+            f.rem = (float)Din.rem[e];
+            f.vstart = (float)Din.vstart[e];
+            st = advance_f(M, S, pp, f, chain ? cap : 0x7fffffff, rlo, rhi, c.nsub);
         }
-        if (a) atomicAdd(&L->substeps, a);
-        if (b) atomicAdd(&L->lost_events, b);
-        if (c) atomicAdd(&L->mcc_hits, c);
-        if (d) atomicAdd(&L->active, d);
+        unsigned slot = chain ? warp_append(st == kCapped, Dout.count) : 0xffffffffu;
+        if (st == kCapped && chain && slot < Dout.cap) {
+            defer_store_f(P, Dout, slot, i, f);
+        } else if (st >= 0) {
+            if (st == kCapped) st = advance_f(M, S, pp, f, 0x7fffffff, rlo, rhi, c.nsub);
+            finish_f(M, P, S, pp, L, i, f, st, c);
+        }
     }
+    block_stats(c, L, ke_part);
 }
 
 __global__ void k_mcc_mixed(ParticleStore P, SpeciesDev S, PushParams pp, LedgerDev* L)
@@ -340,11 +468,36 @@ __global__ void k_from_mixed(MeshView M, int64_t n, ParticleStore P, double* x, 
     }
 }
 
-void launch_push_mixed(const MeshView& M, const ParticleStore& P, const SpeciesDev& S, const PushParams& pp,
-                       const float* Ef, unsigned long long* rlo, unsigned long long* rhi, LedgerDev* L,
-                       double* ke_part, int grid, cudaStream_t st)
+// Refresh the nodal-E words of every tet record from the FP64 nodal field.
+__global__ void k_refresh_trec(int64_t T, const int4* __restrict__ tet, const double* __restrict__ E, float* trec)
 {
-    k_push_mixed<<<grid, 256, 0, st>>>(M, P, S, pp, Ef, rlo, rhi, L, ke_part);
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < T; t += (int64_t)gridDim.x * blockDim.x) {
+        int4 tn = tet[t];
+        const double* e0 = E + 3 * (int64_t)tn.x;
+        const double* e1 = E + 3 * (int64_t)tn.y;
+        const double* e2 = E + 3 * (int64_t)tn.z;
+        const double* e3 = E + 3 * (int64_t)tn.w;
+        float* r = trec + 64 * t;
+        float4* r4 = reinterpret_cast<float4*>(r);
+        float j8 = r[8];
+        float nd0 = r[21], nd1 = r[22], nd2 = r[23];
+        r4[2] = make_float4(j8, (float)e0[0], (float)e0[1], (float)e0[2]);
+        r4[3] = make_float4((float)(e1[0] - e0[0]), (float)(e1[1] - e0[1]), (float)(e1[2] - e0[2]),
+                            (float)(e2[0] - e0[0]));
+        r4[4] = make_float4((float)(e2[1] - e0[1]), (float)(e2[2] - e0[2]), (float)(e3[0] - e0[0]),
+                            (float)(e3[1] - e0[1]));
+        r4[5] = make_float4((float)(e3[2] - e0[2]), nd0, nd1, nd2);
+    }
+}
+
+void launch_push_mixed(const MeshView& M, const ParticleStore& P, const SpeciesDev& S, const PushParams& pp,
+                       const DeferList& D1, const DeferList& D2, unsigned long long* rlo, unsigned long long* rhi,
+                       LedgerDev* L, double* ke_part, int grid, cudaStream_t st)
+{
+    k_push_mixed<<<grid, 256, 0, st>>>(M, P, S, pp, D1, rlo, rhi, L, ke_part);
+    k_push_mixed_more<<<grid, 256, 0, st>>>(M, P, S, pp, D1, D2, kCap2, rlo, rhi, L, ke_part);
+    DeferList none{};
+    k_push_mixed_more<<<grid, 256, 0, st>>>(M, P, S, pp, D2, none, 0, rlo, rhi, L, ke_part);
 }
 
 void launch_mcc_mixed(const ParticleStore& P, const SpeciesDev& S, const PushParams& pp, LedgerDev* L, int grid,
@@ -363,6 +516,11 @@ void launch_from_mixed(const MeshView& M, int64_t n, const ParticleStore& P, dou
                        double* vx, double* vy, double* vz, cudaStream_t st)
 {
     k_from_mixed<<<148 * 4, 256, 0, st>>>(M, n, P, x, y, z, vx, vy, vz);
+}
+
+void launch_refresh_trec(int64_t T, const int4* tet, const double* E, float* trec, cudaStream_t st)
+{
+    k_refresh_trec<<<148 * 8, 256, 0, st>>>(T, tet, E, trec);
 }
 
 }  // namespace scdat

@@ -231,6 +231,6 @@ def test_mixed_precision_error_bounded(lib):
     assert rel_err(p1, p0) < 1e-6
     assert rel_err(e1, e0) < 1e-4
     both = (s0["status"] == O.ACTIVE) & (s1["status"] == O.ACTIVE)
-    assert both.mean() > 0.95
-    assert np.abs(s1["x"][both] - s0["x"][both]).max() < 1e-4
-    assert (s0["status"] != s1["status"]).mean() < 0.02
+    assert (s0["status"] != s1["status"]).mean() < 0.005
+    assert both.sum() > 0.9 * (s0["status"] == O.ACTIVE).sum()
+    assert np.abs(s1["x"][both] - s0["x"][both]).max() < 1e-6
