@@ -24,13 +24,13 @@
 
 namespace scdat {
 void launch_push_f64(const MeshView& M, const ParticleStore& P, const SpeciesDev& S, const PushParams& pp,
-                     const DeferList& D1, const DeferList& D2, unsigned long long* rlo, unsigned long long* rhi,
-                     LedgerDev* L, double* ke_part, int grid, cudaStream_t st);
+                     const DeferList& D1, const DeferList& D2, ChargeAcc A, LedgerDev* L, double* ke_part, int grid,
+                     cudaStream_t st);
 void launch_mcc_f64(const ParticleStore& P, const SpeciesDev& S, const PushParams& pp, LedgerDev* L, int grid,
                     cudaStream_t st);
 void launch_push_mixed(const MeshView& M, const ParticleStore& P, const SpeciesDev& S, const PushParams& pp,
-                       const DeferList& D1, const DeferList& D2, unsigned long long* rlo, unsigned long long* rhi,
-                       LedgerDev* L, double* ke_part, int grid, cudaStream_t st);
+                       const DeferList& D1, const DeferList& D2, ChargeAcc A, LedgerDev* L, double* ke_part, int grid,
+                       cudaStream_t st);
 void launch_mcc_mixed(const ParticleStore& P, const SpeciesDev& S, const PushParams& pp, LedgerDev* L, int grid,
                       cudaStream_t st);
 void launch_refresh_erec(int64_t T, const int4* tet, const double* E, double* erec, cudaStream_t st);
@@ -128,7 +128,7 @@ struct scdat_ctx {
     // fields
     DBuf<double> rho, phi, E, tmp_rho;
     DBuf<float> Ef;
-    DBuf<unsigned long long> acc_lo, acc_hi, totq;
+    DBuf<unsigned long long> acc_l0, acc_l1, acc_h, totq;
     // particles
     std::vector<SpeciesState> species;
     DBuf<int64_t> counts;
@@ -279,8 +279,9 @@ int do_push(scdat_ctx* ctx, bool do_mcc)
         return SCDAT_ERR_STATE;
     }
     const int64_t N = ctx->hm.N;
-    CK(cudaMemsetAsync(ctx->acc_lo.p, 0, sizeof(unsigned long long) * S * N, ctx->st));
-    CK(cudaMemsetAsync(ctx->acc_hi.p, 0, sizeof(unsigned long long) * S * N, ctx->st));
+    CK(cudaMemsetAsync(ctx->acc_l0.p, 0, sizeof(unsigned long long) * S * N, ctx->st));
+    CK(cudaMemsetAsync(ctx->acc_l1.p, 0, sizeof(unsigned long long) * S * N, ctx->st));
+    CK(cudaMemsetAsync(ctx->acc_h.p, 0, sizeof(unsigned long long) * S * N, ctx->st));
     CK(cudaMemsetAsync(ctx->ke_part.p, 0, sizeof(double) * ctx->grid_push, ctx->st));
     CK(cudaMemsetAsync(&ctx->led.p->active, 0, sizeof(unsigned long long), ctx->st));
     PushParams pp = push_params(ctx, do_mcc);
@@ -299,12 +300,11 @@ int do_push(scdat_ctx* ctx, bool do_mcc)
         DeferList d1{ctx->dcount.p, ctx->dcap, ctx->d1idx.p, ctx->d1it.p, ctx->d1rem.p, ctx->d1vs.p};
         DeferList d2{ctx->dcount.p + 1, ctx->dcap, ctx->d2idx.p, ctx->d2it.p, ctx->d2rem.p, ctx->d2vs.p};
         ctx->launches += 3;
+        ChargeAcc acc{ctx->acc_l0.p + s * N, ctx->acc_l1.p + s * N, ctx->acc_h.p + s * N};
         if (ctx->mixed)
-            launch_push_mixed(ctx->mv, P, sd, pp, d1, d2, ctx->acc_lo.p + s * N, ctx->acc_hi.p + s * N, ctx->led.p,
-                              ctx->ke_part.p, ctx->grid_push, ctx->st);
+            launch_push_mixed(ctx->mv, P, sd, pp, d1, d2, acc, ctx->led.p, ctx->ke_part.p, ctx->grid_push, ctx->st);
         else
-            launch_push_f64(ctx->mv, P, sd, pp, d1, d2, ctx->acc_lo.p + s * N, ctx->acc_hi.p + s * N, ctx->led.p,
-                            ctx->ke_part.p, ctx->grid_push, ctx->st);
+            launch_push_f64(ctx->mv, P, sd, pp, d1, d2, acc, ctx->led.p, ctx->ke_part.p, ctx->grid_push, ctx->st);
     }
     CK(cudaGetLastError());
     if (ctx->timing) {
@@ -314,8 +314,8 @@ int do_push(scdat_ctx* ctx, bool do_mcc)
     }
     CK(cudaMemsetAsync(ctx->totq.p, 0, sizeof(unsigned long long) * 2, ctx->st));
     ++ctx->launches;
-    launch_finalize_rho(N, S, ctx->acc_lo.p, ctx->acc_hi.p, ctx->uq, ctx->rho.p, ctx->totq.p, ctx->totq.p + 1,
-                        ctx->grid_nodes, ctx->st);
+    launch_finalize_rho(N, S, ctx->acc_l0.p, ctx->acc_l1.p, ctx->acc_h.p, ctx->uq, ctx->rho.p, ctx->totq.p,
+                        ctx->totq.p + 1, ctx->grid_nodes, ctx->st);
     CK(cudaGetLastError());
     return SCDAT_OK;
 }
@@ -752,12 +752,14 @@ SCDAT_API int scdat_set_species(scdat_ctx* ctx, int32_t n_species, const scdat_s
     ctx->uq = pow2_ceil(mq);
     ctx->ue = pow2_ceil(me);
     const int64_t N = ctx->hm.N;
-    CK(ctx->acc_lo.alloc((size_t)(n_species * N)));
-    CK(ctx->acc_hi.alloc((size_t)(n_species * N)));
+    CK(ctx->acc_l0.alloc((size_t)(n_species * N)));
+    CK(ctx->acc_l1.alloc((size_t)(n_species * N)));
+    CK(ctx->acc_h.alloc((size_t)(n_species * N)));
     CK(ctx->counts.alloc((size_t)n_species));
     CK(cudaMemsetAsync(ctx->counts.p, 0, sizeof(int64_t) * n_species, ctx->st));
-    CK(cudaMemsetAsync(ctx->acc_lo.p, 0, sizeof(unsigned long long) * n_species * N, ctx->st));
-    CK(cudaMemsetAsync(ctx->acc_hi.p, 0, sizeof(unsigned long long) * n_species * N, ctx->st));
+    CK(cudaMemsetAsync(ctx->acc_l0.p, 0, sizeof(unsigned long long) * n_species * N, ctx->st));
+    CK(cudaMemsetAsync(ctx->acc_l1.p, 0, sizeof(unsigned long long) * n_species * N, ctx->st));
+    CK(cudaMemsetAsync(ctx->acc_h.p, 0, sizeof(unsigned long long) * n_species * N, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
     return SCDAT_OK;
 }
@@ -1089,8 +1091,8 @@ SCDAT_API int scdat_get_species_charge(scdat_ctx* ctx, int32_t species, double* 
     if (!ctx) return SCDAT_ERR_ARG;
     ARG(species >= 0 && species < (int)ctx->species.size() && rho_s, "bad species index");
     const int64_t N = ctx->hm.N;
-    launch_species_rho(N, ctx->acc_lo.p + species * N, ctx->acc_hi.p + species * N, ctx->uq, ctx->tmp_rho.p,
-                       ctx->grid_nodes, ctx->st);
+    launch_species_rho(N, ctx->acc_l0.p + species * N, ctx->acc_l1.p + species * N, ctx->acc_h.p + species * N,
+                       ctx->uq, ctx->tmp_rho.p, ctx->grid_nodes, ctx->st);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(rho_s, ctx->tmp_rho.p, sizeof(double) * N, cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));

@@ -56,6 +56,32 @@ __device__ inline void fx_atomic_add(unsigned long long* lo_acc, unsigned long l
     if (h) atomicAdd(hi_acc, h);
 }
 
+// Node charge accumulators: each 128-bit contribution is split into 32-bit limbs that go
+// into three 64-bit words with return-free atomic adds (no thread waits on an atomic), and
+// the limbs are recombined exactly when the charge is read.  2^32 contributions per node
+// and step fit before a limb could wrap.
+struct ChargeAcc {
+    unsigned long long* l0;  // bits 0..31 of each contribution
+    unsigned long long* l1;  // bits 32..63
+    unsigned long long* h;   // the signed high word
+};
+
+__device__ __forceinline__ void fx_red(const ChargeAcc& A, int node, const Fx128& v)
+{
+    unsigned long long a = v.lo & 0xffffffffull, b = v.lo >> 32;
+    if (a) atomicAdd(A.l0 + node, a);
+    if (b) atomicAdd(A.l1 + node, b);
+    if (v.hi) atomicAdd(A.h + node, (unsigned long long)v.hi);
+}
+
+__host__ __device__ inline Fx128 fx_from_limbs(unsigned long long l0, unsigned long long l1, unsigned long long h)
+{
+    Fx128 r{l0, (long long)h};
+    Fx128 m{l1 << 32, (long long)(l1 >> 32)};
+    fx_add(r, m);
+    return r;
+}
+
 // ------------------------------------------------------------------------------------
 // Philox4x32-10
 // ------------------------------------------------------------------------------------

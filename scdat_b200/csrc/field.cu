@@ -64,17 +64,15 @@ __device__ inline bool last_block(double (&v)[NV], double* part, unsigned int* t
 // ---------------------------------------------------------------------------------------
 // Charge finalisation
 // ---------------------------------------------------------------------------------------
-__global__ void k_finalize_rho(int64_t N, int S, const unsigned long long* __restrict__ lo,
-                               const unsigned long long* __restrict__ hi, double unit, double* __restrict__ rho,
-                               unsigned long long* total_lo, unsigned long long* total_hi)
+__global__ void k_finalize_rho(int64_t N, int S, const unsigned long long* __restrict__ l0,
+                               const unsigned long long* __restrict__ l1, const unsigned long long* __restrict__ h,
+                               double unit, double* __restrict__ rho, unsigned long long* total_lo,
+                               unsigned long long* total_hi)
 {
     Fx128 tot{0ull, 0ll};
     for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < N; n += (int64_t)gridDim.x * blockDim.x) {
         Fx128 a{0ull, 0ll};
-        for (int s = 0; s < S; ++s) {
-            Fx128 b{lo[s * N + n], (long long)hi[s * N + n]};
-            fx_add(a, b);
-        }
+        for (int s = 0; s < S; ++s) fx_add(a, fx_from_limbs(l0[s * N + n], l1[s * N + n], h[s * N + n]));
         rho[n] = fx_to_double(a.lo, a.hi, unit);
         fx_add(tot, a);
     }
@@ -88,11 +86,14 @@ __global__ void k_finalize_rho(int64_t N, int S, const unsigned long long* __res
     if ((threadIdx.x & 31) == 0) fx_atomic_add(total_lo, total_hi, tot);
 }
 
-__global__ void k_species_rho(int64_t N, const unsigned long long* __restrict__ lo,
-                              const unsigned long long* __restrict__ hi, double unit, double* __restrict__ out)
+__global__ void k_species_rho(int64_t N, const unsigned long long* __restrict__ l0,
+                              const unsigned long long* __restrict__ l1, const unsigned long long* __restrict__ h,
+                              double unit, double* __restrict__ out)
 {
-    for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < N; n += (int64_t)gridDim.x * blockDim.x)
-        out[n] = fx_to_double(lo[n], (long long)hi[n], unit);
+    for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < N; n += (int64_t)gridDim.x * blockDim.x) {
+        Fx128 a = fx_from_limbs(l0[n], l1[n], h[n]);
+        out[n] = fx_to_double(a.lo, a.hi, unit);
+    }
 }
 
 // ---------------------------------------------------------------------------------------
@@ -327,16 +328,17 @@ __global__ void k_zero_if_flag(int64_t n3, double* E, float* Ef, const unsigned 
 // ---------------------------------------------------------------------------------------
 // Host launchers
 // ---------------------------------------------------------------------------------------
-void launch_finalize_rho(int64_t N, int S, const unsigned long long* lo, const unsigned long long* hi, double unit,
-                         double* rho, unsigned long long* tlo, unsigned long long* thi, int grid, cudaStream_t st)
+void launch_finalize_rho(int64_t N, int S, const unsigned long long* l0, const unsigned long long* l1,
+                         const unsigned long long* h, double unit, double* rho, unsigned long long* tlo,
+                         unsigned long long* thi, int grid, cudaStream_t st)
 {
-    k_finalize_rho<<<grid, 256, 0, st>>>(N, S, lo, hi, unit, rho, tlo, thi);
+    k_finalize_rho<<<grid, 256, 0, st>>>(N, S, l0, l1, h, unit, rho, tlo, thi);
 }
 
-void launch_species_rho(int64_t N, const unsigned long long* lo, const unsigned long long* hi, double unit,
-                        double* out, int grid, cudaStream_t st)
+void launch_species_rho(int64_t N, const unsigned long long* l0, const unsigned long long* l1,
+                        const unsigned long long* h, double unit, double* out, int grid, cudaStream_t st)
 {
-    k_species_rho<<<grid, 256, 0, st>>>(N, lo, hi, unit, out);
+    k_species_rho<<<grid, 256, 0, st>>>(N, l0, l1, h, unit, out);
 }
 
 void launch_rhs(const PoissonView& A, const double* rho, const double* phi, double sign, double* b, int grid,

@@ -29,10 +29,11 @@ struct PcgScalars {
     unsigned int pad2[3];
 };
 
-void launch_finalize_rho(int64_t N, int S, const unsigned long long* lo, const unsigned long long* hi, double unit,
-                         double* rho, unsigned long long* tlo, unsigned long long* thi, int grid, cudaStream_t st);
-void launch_species_rho(int64_t N, const unsigned long long* lo, const unsigned long long* hi, double unit,
-                        double* out, int grid, cudaStream_t st);
+void launch_finalize_rho(int64_t N, int S, const unsigned long long* l0, const unsigned long long* l1,
+                         const unsigned long long* h, double unit, double* rho, unsigned long long* tlo,
+                         unsigned long long* thi, int grid, cudaStream_t st);
+void launch_species_rho(int64_t N, const unsigned long long* l0, const unsigned long long* l1,
+                        const unsigned long long* h, double unit, double* out, int grid, cudaStream_t st);
 void launch_rhs(const PoissonView& A, const double* rho, const double* phi, double sign, double* b, int grid,
                 cudaStream_t st);
 void launch_gather_rows(const PoissonView& A, const double* phi, double* x, int grid, cudaStream_t st);

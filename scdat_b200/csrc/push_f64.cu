@@ -32,7 +32,7 @@ __device__ __forceinline__ void dep_point(DepositAcc& acc, const double lam[4], 
 // (PICParticleAlgorithms.cpp:371-433); each sample point counts only when it lies in t.
 static __device__ __noinline__ void deposit_traj(const MeshView& M, const SpeciesDev& S, const PushParams& pp, int t,
                                                  double sx, double sy, double sz, double ex, double ey, double ez,
-                                                 unsigned long long* rlo, unsigned long long* rhi)
+                                                 ChargeAcc A)
 {
     DepositAcc acc;
 #pragma unroll
@@ -77,10 +77,10 @@ static __device__ __noinline__ void deposit_traj(const MeshView& M, const Specie
     }
     if (!acc.any) return;
     int4 tn = rec_nodes(M, t);
-    fx_atomic_add(rlo + tn.x, rhi + tn.x, acc.n[0]);
-    fx_atomic_add(rlo + tn.y, rhi + tn.y, acc.n[1]);
-    fx_atomic_add(rlo + tn.z, rhi + tn.z, acc.n[2]);
-    fx_atomic_add(rlo + tn.w, rhi + tn.w, acc.n[3]);
+    fx_red(A, tn.x, acc.n[0]);
+    fx_red(A, tn.y, acc.n[1]);
+    fx_red(A, tn.z, acc.n[2]);
+    fx_red(A, tn.w, acc.n[3]);
 }
 
 struct FlightD {
@@ -92,7 +92,7 @@ struct FlightD {
 // Run sub-steps until the step's time is used up, the particle is lost, or `cap` sub-steps
 // ran in this call.
 __device__ __forceinline__ int advance_d(const MeshView& M, const SpeciesDev& S, const PushParams& pp, FlightD& f,
-                                         int cap, unsigned long long* rlo, unsigned long long* rhi,
+                                         int cap, ChargeAcc A,
                                          unsigned long long& nsub)
 {
     const double qm = S.qm;
@@ -145,10 +145,10 @@ __device__ __forceinline__ int advance_d(const MeshView& M, const SpeciesDev& S,
 #pragma unroll
                     for (int q = 0; q < 4; ++q) {
                         double lk = tiny ? lam[q] : (pp.dep_kernel == 0 ? le[q] : 0.5 * (lam[q] + le[q]));
-                        fx_atomic_add(rlo + nd[q], rhi + nd[q], fx_from_double((qw * lk) * pp.inv_uq));
+                        fx_red(A, nd[q], fx_from_double((qw * lk) * pp.inv_uq));
                     }
                 } else {
-                    deposit_traj(M, S, pp, f.cur, sx, sy, sz, f.px, f.py, f.pz, rlo, rhi);
+                    deposit_traj(M, S, pp, f.cur, sx, sy, sz, f.px, f.py, f.pz, A);
                 }
             }
 #pragma unroll
@@ -158,7 +158,7 @@ __device__ __forceinline__ int advance_d(const MeshView& M, const SpeciesDev& S,
             int nt = locate(M, f.px, f.py, f.pz, f.cur);
             if (nt < 0) return kLost;
             f.cur = nt;
-            if (pp.deposit) deposit_traj(M, S, pp, nt, sx, sy, sz, f.px, f.py, f.pz, rlo, rhi);
+            if (pp.deposit) deposit_traj(M, S, pp, nt, sx, sy, sz, f.px, f.py, f.pz, A);
             in = bary64(M, nt, f.px, f.py, f.pz, lam);
         }
         f.rem -= adt;
@@ -201,7 +201,7 @@ __device__ __forceinline__ void defer_store_d(const ParticleStore& P, const Defe
 
 // Pass 1: every stored particle, at most kCap1 sub-steps.
 __global__ void __launch_bounds__(256) k_push_f64(MeshView M, ParticleStore P, SpeciesDev S, PushParams pp,
-                                                  DeferList D, unsigned long long* rlo, unsigned long long* rhi,
+                                                  DeferList D, ChargeAcc A,
                                                   LedgerDev* L, double* ke_part)
 {
     const int64_t n = *P.count;
@@ -229,7 +229,7 @@ __global__ void __launch_bounds__(256) k_push_f64(MeshView M, ParticleStore P, S
                     f.cur = 0;  // result.final_element stays 0 (PICParticleAlgorithms.cpp:543,577)
                     st = kLost;
                 } else {
-                    st = advance_d(M, S, pp, f, kCap1, rlo, rhi, c.nsub);
+                    st = advance_d(M, S, pp, f, kCap1, A, c.nsub);
                 }
             }
         }
@@ -237,7 +237,7 @@ __global__ void __launch_bounds__(256) k_push_f64(MeshView M, ParticleStore P, S
         if (st == kCapped && slot < D.cap) {
             defer_store_d(P, D, slot, i, f);
         } else if (st >= 0) {
-            if (st == kCapped) st = advance_d(M, S, pp, f, 0x7fffffff, rlo, rhi, c.nsub);
+            if (st == kCapped) st = advance_d(M, S, pp, f, 0x7fffffff, A, c.nsub);
             finish_d(M, P, S, pp, L, i, f, st, c);
         }
     }
@@ -246,8 +246,7 @@ __global__ void __launch_bounds__(256) k_push_f64(MeshView M, ParticleStore P, S
 
 // Passes 2 and 3 over a deferred list (see k_push_mixed_more).
 __global__ void __launch_bounds__(256) k_push_f64_more(MeshView M, ParticleStore P, SpeciesDev S, PushParams pp,
-                                                       DeferList Din, DeferList Dout, int cap, unsigned long long* rlo,
-                                                       unsigned long long* rhi, LedgerDev* L, double* ke_part)
+                                                       DeferList Din, DeferList Dout, int cap, ChargeAcc A, LedgerDev* L, double* ke_part)
 {
     const int64_t n = (int64_t)min(*Din.count, Din.cap);
     PushStats c{0.0, 0ull, 0ull, 0ull, 0ull};
@@ -268,13 +267,13 @@ __global__ void __launch_bounds__(256) k_push_f64_more(MeshView M, ParticleStore
             f.it = Din.it[e];
             f.rem = Din.rem[e];
             f.vstart = Din.vstart[e];
-            st = advance_d(M, S, pp, f, chain ? cap : 0x7fffffff, rlo, rhi, c.nsub);
+            st = advance_d(M, S, pp, f, chain ? cap : 0x7fffffff, A, c.nsub);
         }
         unsigned slot = chain ? warp_append(st == kCapped, Dout.count) : 0xffffffffu;
         if (st == kCapped && chain && slot < Dout.cap) {
             defer_store_d(P, Dout, slot, i, f);
         } else if (st >= 0) {
-            if (st == kCapped) st = advance_d(M, S, pp, f, 0x7fffffff, rlo, rhi, c.nsub);
+            if (st == kCapped) st = advance_d(M, S, pp, f, 0x7fffffff, A, c.nsub);
             finish_d(M, P, S, pp, L, i, f, st, c);
         }
     }
@@ -314,13 +313,13 @@ __global__ void k_refresh_erec(int64_t T, const int4* __restrict__ tet, const do
 }
 
 void launch_push_f64(const MeshView& M, const ParticleStore& P, const SpeciesDev& S, const PushParams& pp,
-                     const DeferList& D1, const DeferList& D2, unsigned long long* rlo, unsigned long long* rhi,
+                     const DeferList& D1, const DeferList& D2, ChargeAcc A,
                      LedgerDev* L, double* ke_part, int grid, cudaStream_t st)
 {
-    k_push_f64<<<grid, 256, 0, st>>>(M, P, S, pp, D1, rlo, rhi, L, ke_part);
-    k_push_f64_more<<<grid, 256, 0, st>>>(M, P, S, pp, D1, D2, kCap2, rlo, rhi, L, ke_part);
+    k_push_f64<<<grid, 256, 0, st>>>(M, P, S, pp, D1, A, L, ke_part);
+    k_push_f64_more<<<grid, 256, 0, st>>>(M, P, S, pp, D1, D2, kCap2, A, L, ke_part);
     DeferList none{};
-    k_push_f64_more<<<grid, 256, 0, st>>>(M, P, S, pp, D2, none, 0, rlo, rhi, L, ke_part);
+    k_push_f64_more<<<grid, 256, 0, st>>>(M, P, S, pp, D2, none, 0, A, L, ke_part);
 }
 
 void launch_mcc_f64(const ParticleStore& P, const SpeciesDev& S, const PushParams& pp, LedgerDev* L, int grid,

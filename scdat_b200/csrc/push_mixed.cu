@@ -135,7 +135,7 @@ static __device__ __noinline__ int relocate_f(const MeshView& M, int cur, float&
 // once to fixed point.
 static __device__ __noinline__ void deposit_traj_f(const MeshView& M, const SpeciesDev& S, const PushParams& pp,
                                                    int t, float sx, float sy, float sz, float rx, float ry, float rz,
-                                                   unsigned long long* rlo, unsigned long long* rhi)
+                                                   ChargeAcc A)
 {
     float j[9];
     load_j(M, t, j);
@@ -189,7 +189,7 @@ static __device__ __noinline__ void deposit_traj_f(const MeshView& M, const Spec
     const int* nd = reinterpret_cast<const int*>(M.trec + 64 * (int64_t)t + 21);
     for (int k = 0; k < 4; ++k) {
         int node = __ldg(nd + k);
-        fx_atomic_add(rlo + node, rhi + node, fx_from_double((cw * (double)sum[k]) * pp.inv_uq));
+        fx_red(A, node, fx_from_double((cw * (double)sum[k]) * pp.inv_uq));
     }
 }
 
@@ -202,7 +202,7 @@ struct FlightF {
 // Run sub-steps until the step's time is used up, the particle is lost, or `cap` sub-steps
 // ran in this call.
 __device__ __forceinline__ int advance_f(const MeshView& M, const SpeciesDev& S, const PushParams& pp, FlightF& f,
-                                         int cap, unsigned long long* rlo, unsigned long long* rhi,
+                                         int cap, ChargeAcc A,
                                          unsigned long long& nsub)
 {
     const float qm = (float)S.qm;
@@ -251,10 +251,10 @@ __device__ __forceinline__ int advance_f(const MeshView& M, const SpeciesDev& S,
 #pragma unroll
                     for (int q = 0; q < 4; ++q) {
                         float lk = tiny ? l[q] : (pp.dep_kernel == 0 ? le[q] : 0.5f * (l[q] + le[q]));
-                        fx_atomic_add(rlo + R.nd[q], rhi + R.nd[q], fx_from_double((qw * (double)lk) * pp.inv_uq));
+                        fx_red(A, R.nd[q], fx_from_double((qw * (double)lk) * pp.inv_uq));
                     }
                 } else {
-                    deposit_traj_f(M, S, pp, f.cur, sx, sy, sz, f.rx, f.ry, f.rz, rlo, rhi);
+                    deposit_traj_f(M, S, pp, f.cur, sx, sy, sz, f.rx, f.ry, f.rz, A);
                 }
             }
 #pragma unroll
@@ -265,7 +265,7 @@ __device__ __forceinline__ int advance_f(const MeshView& M, const SpeciesDev& S,
             if (nt < 0) return kLost;
             f.cur = nt;
             R = load_rec(M, nt);
-            if (pp.deposit) deposit_traj_f(M, S, pp, nt, sx, sy, sz, f.rx, f.ry, f.rz, rlo, rhi);
+            if (pp.deposit) deposit_traj_f(M, S, pp, nt, sx, sy, sz, f.rx, f.ry, f.rz, A);
             baryj(R.j, f.rx, f.ry, f.rz, l);
             in = inside_f(l);
         }
@@ -330,8 +330,8 @@ __device__ __forceinline__ void defer_store_f(const ParticleStore& P, const Defe
 }
 
 // Pass 1: every stored particle, at most kCap1 sub-steps.
-__global__ void __launch_bounds__(256) k_push_mixed(MeshView M, ParticleStore P, SpeciesDev S, PushParams pp,
-                                                    DeferList D, unsigned long long* rlo, unsigned long long* rhi,
+__global__ void __launch_bounds__(256, 4) k_push_mixed(MeshView M, ParticleStore P, SpeciesDev S, PushParams pp,
+                                                    DeferList D, ChargeAcc A,
                                                     LedgerDev* L, double* ke_part)
 {
     const int64_t n = *P.count;
@@ -368,14 +368,14 @@ __global__ void __launch_bounds__(256) k_push_mixed(MeshView M, ParticleStore P,
                         f.cur = t;
                     }
                 }
-                if (st != kLost) st = advance_f(M, S, pp, f, kCap1, rlo, rhi, c.nsub);
+                if (st != kLost) st = advance_f(M, S, pp, f, kCap1, A, c.nsub);
             }
         }
         unsigned slot = warp_append(st == kCapped, D.count);
         if (st == kCapped && slot < D.cap) {
             defer_store_f(P, D, slot, i, f);
         } else if (st >= 0) {
-            if (st == kCapped) st = advance_f(M, S, pp, f, 0x7fffffff, rlo, rhi, c.nsub);
+            if (st == kCapped) st = advance_f(M, S, pp, f, 0x7fffffff, A, c.nsub);
             finish_f(M, P, S, pp, L, i, f, st, c);
         }
     }
@@ -384,9 +384,9 @@ __global__ void __launch_bounds__(256) k_push_mixed(MeshView M, ParticleStore P,
 
 // Passes 2 and 3: continue the particles of list `Din` (up to `cap` sub-steps, then append
 // to Dout; with Dout.count == nullptr the particles run to the end).
-__global__ void __launch_bounds__(256) k_push_mixed_more(MeshView M, ParticleStore P, SpeciesDev S, PushParams pp,
+__global__ void __launch_bounds__(256, 4) k_push_mixed_more(MeshView M, ParticleStore P, SpeciesDev S, PushParams pp,
                                                          DeferList Din, DeferList Dout, int cap,
-                                                         unsigned long long* rlo, unsigned long long* rhi,
+                                                         ChargeAcc A,
                                                          LedgerDev* L, double* ke_part)
 {
     const int64_t n = (int64_t)min(*Din.count, Din.cap);
@@ -408,13 +408,13 @@ __global__ void __launch_bounds__(256) k_push_mixed_more(MeshView M, ParticleSto
             f.it = Din.it[e];
             f.rem = (float)Din.rem[e];
             f.vstart = (float)Din.vstart[e];
-            st = advance_f(M, S, pp, f, chain ? cap : 0x7fffffff, rlo, rhi, c.nsub);
+            st = advance_f(M, S, pp, f, chain ? cap : 0x7fffffff, A, c.nsub);
         }
         unsigned slot = chain ? warp_append(st == kCapped, Dout.count) : 0xffffffffu;
         if (st == kCapped && chain && slot < Dout.cap) {
             defer_store_f(P, Dout, slot, i, f);
         } else if (st >= 0) {
-            if (st == kCapped) st = advance_f(M, S, pp, f, 0x7fffffff, rlo, rhi, c.nsub);
+            if (st == kCapped) st = advance_f(M, S, pp, f, 0x7fffffff, A, c.nsub);
             finish_f(M, P, S, pp, L, i, f, st, c);
         }
     }
@@ -491,13 +491,13 @@ __global__ void k_refresh_trec(int64_t T, const int4* __restrict__ tet, const do
 }
 
 void launch_push_mixed(const MeshView& M, const ParticleStore& P, const SpeciesDev& S, const PushParams& pp,
-                       const DeferList& D1, const DeferList& D2, unsigned long long* rlo, unsigned long long* rhi,
+                       const DeferList& D1, const DeferList& D2, ChargeAcc A,
                        LedgerDev* L, double* ke_part, int grid, cudaStream_t st)
 {
-    k_push_mixed<<<grid, 256, 0, st>>>(M, P, S, pp, D1, rlo, rhi, L, ke_part);
-    k_push_mixed_more<<<grid, 256, 0, st>>>(M, P, S, pp, D1, D2, kCap2, rlo, rhi, L, ke_part);
+    k_push_mixed<<<grid, 256, 0, st>>>(M, P, S, pp, D1, A, L, ke_part);
+    k_push_mixed_more<<<grid, 256, 0, st>>>(M, P, S, pp, D1, D2, kCap2, A, L, ke_part);
     DeferList none{};
-    k_push_mixed_more<<<grid, 256, 0, st>>>(M, P, S, pp, D2, none, 0, rlo, rhi, L, ke_part);
+    k_push_mixed_more<<<grid, 256, 0, st>>>(M, P, S, pp, D2, none, 0, A, L, ke_part);
 }
 
 void launch_mcc_mixed(const ParticleStore& P, const SpeciesDev& S, const PushParams& pp, LedgerDev* L, int grid,
