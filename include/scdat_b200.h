@@ -224,6 +224,17 @@ SCDAT_API int scdat_set_timing(scdat_ctx* ctx, int32_t enable);
 SCDAT_API int scdat_get_timing(scdat_ctx* ctx, double* push_ms, int64_t* push_launches, int64_t* push_particles,
                                double* field_ms, int64_t* field_solves, int64_t* kernel_launches);
 
+/* LinearSystem::solve(ITERATIVE) (Tools/Solver/src/LinearSystem.cpp:84-87,258-327) without a
+ * context: Jacobi-preconditioned CG on a caller-assembled SPD system whose arrays all live in
+ * device memory.  Row r holds its off-diagonal entries in col/val[row_ptr[r]..row_ptr[r+1]) and
+ * its diagonal in diag[r]; x is the start vector on entry and the solution on return; the
+ * solve stops when ||r|| <= rtol*||b|| or after max_iter iterations (SCDAT_ERR_NOT_CONVERGED,
+ * x kept).  stream is a cudaStream_t (NULL: the default stream); the call blocks until the
+ * solve ends.  Scratch device memory (6 vectors of R doubles) is allocated and freed inside. */
+SCDAT_API int scdat_pcg_csr(int32_t R, const int32_t* row_ptr, const int32_t* col, const double* val,
+                            const double* diag, const double* b, double* x, double rtol, int32_t max_iter,
+                            void* stream, int32_t* iterations, double* relres);
+
 /* Library version string. */
 SCDAT_API const char* scdat_version(void);
 

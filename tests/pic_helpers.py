@@ -69,3 +69,41 @@ def gpu_state(dom, nspecies, nparts):
         tet[ids] = g["tet"]
         status[ids] = g["status"]
     return dict(x=x, v=v, tet=tet, status=status)
+
+
+def reduced_system(mesh, A, rho, phi_bc, charge_sign=-1.0):
+    """The Dirichlet-eliminated system of the interior rows (LinearSystem.cpp:37-58) in CSR:
+    (row_ptr, col, val, diag, b, interior node ids)."""
+    inner = np.nonzero(mesh.dirichlet == 0)[0]
+    row_of = -np.ones(mesh.N, np.int64)
+    row_of[inner] = np.arange(len(inner))
+    rp, cols, vals, b = [0], [], [], np.zeros(len(inner))
+    for r, n in enumerate(inner):
+        bi = charge_sign * rho[n] * A["cv"][n]
+        for e in range(A["rowptr"][n], A["rowptr"][n + 1]):
+            j = A["col"][e]
+            if mesh.dirichlet[j]:
+                bi -= A["offw"][e] * phi_bc[j]
+            else:
+                cols.append(row_of[j])
+                vals.append(A["offw"][e])
+        b[r] = bi
+        rp.append(len(cols))
+    return (np.array(rp, np.int32), np.array(cols, np.int32), np.array(vals, np.float64),
+            A["diag"][inner].copy(), b, inner)
+
+
+def pcg_csr_on_device(entry, rp, col, val, diag, b, x0, rtol, max_iter):
+    """Call a scdat_pcg_csr-shaped entry point on device copies (torch owns the memory)."""
+    import ctypes as C
+
+    import torch
+
+    dev = torch.device("cuda:0")
+    t = [torch.from_numpy(np.ascontiguousarray(a)).to(dev) for a in (rp, col, val, diag, b, x0)]
+    it, rel = C.c_int32(), C.c_double()
+    torch.cuda.synchronize()
+    rc = entry(len(b), *(C.c_void_p(a.data_ptr()) for a in t[:5]), C.c_void_p(t[5].data_ptr()), rtol, max_iter, None,
+               C.byref(it), C.byref(rel))
+    torch.cuda.synchronize()
+    return rc, t[5].cpu().numpy(), it.value, rel.value
