@@ -235,6 +235,20 @@ SCDAT_API int scdat_pcg_csr(int32_t R, const int32_t* row_ptr, const int32_t* co
                             const double* diag, const double* b, double* x, double rtol, int32_t max_iter,
                             void* stream, int32_t* iterations, double* relres);
 
+/* scdat_pcg_csr for callers that cannot allocate device memory (no counterpart in the
+ * reference).  Some callers may not call cudaMalloc at all -- a host application that owns a
+ * fixed device-memory arena and hands the library only pointers into it, or code running
+ * where the allocator is unavailable -- so this call allocates nothing: its scratch lives in
+ * one static device array of 12.6 MB that every GPU loading the library keeps until exit.
+ * Limit: R <= 262144 rows; larger systems return SCDAT_ERR_CAPACITY before any GPU work.
+ * The first call on each device looks up the array's device address (cudaGetSymbolAddress,
+ * with that device current); make that first call before any stream capture.  All calls
+ * share the one array, so calls that overlap on the GPU (other streams, other threads) race:
+ * serialise them.  Arguments, results and blocking behaviour are those of scdat_pcg_csr. */
+SCDAT_API int scdat_pcg_csr_noalloc(int32_t R, const int32_t* row_ptr, const int32_t* col, const double* val,
+                                    const double* diag, const double* b, double* x, double rtol, int32_t max_iter,
+                                    void* stream, int32_t* iterations, double* relres);
+
 /* Library version string. */
 SCDAT_API const char* scdat_version(void);
 

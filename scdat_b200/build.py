@@ -19,7 +19,7 @@ BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libscdat_b200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
-SOURCES = ["capi.cu", "push_f64.cu", "push_mixed.cu", "field.cu", "utils.cu", "pcg_csr.cu", "mesh_setup.cpp"]
+SOURCES = ["capi.cu", "push_f64.cu", "push_mixed.cu", "field.cu", "utils.cu", "pcg_csr.cu", "pcg_noalloc.cu", "mesh_setup.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
          "--expt-relaxed-constexpr", f"-I{os.path.join(ROOT, 'include')}"]

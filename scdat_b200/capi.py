@@ -58,7 +58,7 @@ EXPORTS = ["scdat_default_params", "scdat_create", "scdat_destroy", "scdat_last_
            "scdat_set_elastic_mcc", "scdat_step", "scdat_push", "scdat_solve_field", "scdat_collide", "scdat_compact",
            "scdat_get_fields", "scdat_get_species_charge", "scdat_get_ledger", "scdat_reset_ledger",
            "scdat_get_statistics", "scdat_version", "scdat_stream", "scdat_set_timing", "scdat_get_timing",
-           "scdat_pcg_csr"]
+           "scdat_pcg_csr", "scdat_pcg_csr_noalloc"]
 
 _LIB = None
 
@@ -105,6 +105,7 @@ def load():
                                    C.POINTER(C.c_double), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
     L.scdat_pcg_csr.argtypes = [C.c_int32, vp, vp, vp, vp, vp, vp, C.c_double, C.c_int32, vp,
                                 C.POINTER(C.c_int32), C.POINTER(C.c_double)]
+    L.scdat_pcg_csr_noalloc.argtypes = L.scdat_pcg_csr.argtypes
     L.scdat_version.argtypes = []
     L.scdat_version.restype = C.c_char_p
     _LIB = L
