@@ -123,11 +123,12 @@ def build_domain(cfg, precision, capi):
 
 def alg_bytes_push(dom, precision, particles):
     """Algorithmic bytes of one push launch (all species of a step): particle state read and
-    written once (+ the 4-byte id the fused MCC reads), the mesh read once, node E read once
-    and the fixed-point accumulators read-modify-written once."""
+    written once (+ the 4-byte id the fused MCC reads), every tet record read once (FP64: the
+    128-byte geometry record and the 96-byte nodal-E record; mixed: the first 128 bytes of its
+    record), and each node's three 8-byte charge limbs read and written once per species."""
     b_p = 60 if precision == 1 else 108
-    t_b = 16 + (36 if precision == 1 else 96)
-    n_b = (12 if precision == 1 else 24) + 2 * 16 * dom.nspecies
+    t_b = 128 if precision == 1 else 128 + 96
+    n_b = 48 * dom.nspecies
     return particles * b_p + dom.T * t_b + dom.N * n_b
 
 
