@@ -37,11 +37,14 @@ __device__ inline void block_sum(double (&v)[NV], double* sh /* [NV*32] */)
 }
 
 // Writes this block's partials, and returns true in thread 0 of the last block to finish,
-// after which part[k*grid + b] for all blocks b are visible.
+// with v[k] the sum over all blocks.  The last block sums the partials with all its threads
+// (thread t takes blocks t, t+256, ...) and a fixed-shape tree, so the order is the same on
+// every run.  Blocks have 256 threads.
 template <int NV>
 __device__ inline bool last_block(double (&v)[NV], double* part, unsigned int* ticket)
 {
     __shared__ bool am_last;
+    __shared__ double red[NV][256];
     if (threadIdx.x == 0) {
 #pragma unroll
         for (int k = 0; k < NV; ++k) part[k * gridDim.x + blockIdx.x] = v[k];
@@ -50,14 +53,24 @@ __device__ inline bool last_block(double (&v)[NV], double* part, unsigned int* t
         am_last = (t == gridDim.x - 1);
     }
     __syncthreads();
-    if (!am_last || threadIdx.x != 0) return false;
+    if (!am_last) return false;
     __threadfence();
 #pragma unroll
     for (int k = 0; k < NV; ++k) {
         double s = 0.0;
-        for (unsigned int b = 0; b < gridDim.x; ++b) s += ((volatile double*)part)[k * gridDim.x + b];
-        v[k] = s;
+        for (unsigned int b = threadIdx.x; b < gridDim.x; b += blockDim.x) s += __ldcg(part + k * gridDim.x + b);
+        red[k][threadIdx.x] = s;
     }
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w)
+#pragma unroll
+            for (int k = 0; k < NV; ++k) red[k][threadIdx.x] += red[k][threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x != 0) return false;
+#pragma unroll
+    for (int k = 0; k < NV; ++k) v[k] = red[k][0];
     return true;
 }
 
@@ -124,11 +137,19 @@ __global__ void k_scatter_rows(PoissonView A, const double* __restrict__ x, doub
 // ---------------------------------------------------------------------------------------
 // PCG (FP64 values, or FP32 values for the inner solve of the mixed form)
 // ---------------------------------------------------------------------------------------
+// diagonal and its reciprocal in the precision of the solve
+template <typename V> __device__ __forceinline__ double diag_at(const PoissonView& A, int i);
+template <> __device__ __forceinline__ double diag_at<double>(const PoissonView& A, int i) { return A.diag[i]; }
+template <> __device__ __forceinline__ double diag_at<float>(const PoissonView& A, int i) { return (double)A.diagf[i]; }
+template <typename V> __device__ __forceinline__ double dinv_at(const PoissonView& A, int i);
+template <> __device__ __forceinline__ double dinv_at<double>(const PoissonView& A, int i) { return A.dinv[i]; }
+template <> __device__ __forceinline__ double dinv_at<float>(const PoissonView& A, int i) { return (double)A.dinvf[i]; }
+
 template <typename V>
 __device__ __forceinline__ double spmv_row(const PoissonView& A, const V* __restrict__ val, int r,
                                            const V* __restrict__ xv)
 {
-    double s = (double)A.diag[r] * (double)xv[r];
+    double s = diag_at<V>(A, r) * (double)xv[r];
     for (int e = A.row_ptr[r]; e < A.row_ptr[r + 1]; ++e) s += (double)val[e] * (double)xv[A.col[e]];
     return s;
 }
@@ -141,7 +162,7 @@ __global__ void k_pcg_init(PoissonView A, const V* __restrict__ val, const V* __
     double acc[3] = {0.0, 0.0, 0.0};
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.R; i += gridDim.x * blockDim.x) {
         double ri = (double)b[i] - spmv_row(A, val, i, x);
-        double zi = ri * A.dinv[i];
+        double zi = ri * dinv_at<V>(A, i);
         r[i] = (V)ri;
         z[i] = (V)zi;
         acc[0] += ri * zi;
@@ -174,7 +195,7 @@ __global__ void k_pcg_spmv(PoissonView A, const V* __restrict__ val, const V* __
     double acc[1] = {0.0};
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.R; i += gridDim.x * blockDim.x) {
         double pi = first ? (double)z[i] : (double)z[i] + beta * (double)p[i];
-        double s = (double)A.diag[i] * pi;
+        double s = diag_at<V>(A, i) * pi;
         for (int e = A.row_ptr[i]; e < A.row_ptr[i + 1]; ++e) {
             int c = A.col[e];
             double pc = first ? (double)z[c] : (double)z[c] + beta * (double)p[c];
@@ -201,7 +222,7 @@ __global__ void k_pcg_update(PoissonView A, V* __restrict__ x, const V* __restri
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.R; i += gridDim.x * blockDim.x) {
         double xi = (double)x[i] + alpha * (double)pn[i];
         double ri = (double)r[i] - alpha * (double)q[i];
-        double zi = ri * A.dinv[i];
+        double zi = ri * dinv_at<V>(A, i);
         x[i] = (V)xi;
         r[i] = (V)ri;
         z[i] = (V)zi;

@@ -20,6 +20,8 @@ struct PoissonView {
     const float* valf;        // K_rr' (FP32, mixed form)
     const double* diag;       // K_rr
     const double* dinv;       // 1 / K_rr
+    const float* diagf;       // K_rr (FP32, mixed form)
+    const float* dinvf;       // 1 / K_rr (FP32, mixed form)
 };
 
 struct PcgScalars {

@@ -277,6 +277,8 @@ std::string assemble_poisson(const HostMesh& m, const HostGraph& gr, HostPoisson
     ps.cv.resize(ps.R);
     ps.diag.resize(ps.R);
     ps.dinv.resize(ps.R);
+    ps.diagf.resize(ps.R);
+    ps.dinvf.resize(ps.R);
     ps.row_ptr.assign((size_t)ps.R + 1, 0);
     ps.lift_ptr.assign((size_t)ps.R + 1, 0);
     ps.col.clear();
@@ -290,6 +292,8 @@ std::string assemble_poisson(const HostMesh& m, const HostGraph& gr, HostPoisson
         ps.diag[r] = diag[n];
         if (!(diag[n] > 0.0)) return "interior node with no positive diagonal (isolated node not marked Dirichlet)";
         ps.dinv[r] = 1.0 / diag[n];
+        ps.diagf[r] = (float)ps.diag[r];
+        ps.dinvf[r] = (float)ps.dinv[r];
         for (int32_t e = gr.ptr[n]; e < gr.ptr[n + 1]; ++e) {
             int32_t j = gr.col[e];
             if (m.dirichlet[j]) {

@@ -41,6 +41,7 @@ struct HostPoisson {
     std::vector<int32_t> row_of_node;  // -1 for Dirichlet nodes
     std::vector<int32_t> row_node;
     std::vector<double> cv, diag, dinv;
+    std::vector<float> diagf, dinvf;
     std::vector<int32_t> row_ptr, col;
     std::vector<double> val;
     std::vector<float> valf;
