@@ -176,6 +176,16 @@ SCDAT_API int scdat_set_node_potentials(scdat_ctx* ctx, int64_t n, const int64_t
 /* FieldInterpolator::setElectricField (PICParticleAlgorithms.h:92): freeze a nodal E. */
 SCDAT_API int scdat_set_electric_field(scdat_ctx* ctx, const double* E);
 
+/* PoissonSolver::setChargeDensity (Tools/FieldSolver/include/PoissonSolver.h:41-43): nodal
+ * charge [C] for the next scdat_solve_field.  The next scdat_push or scdat_step replaces it
+ * with the deposited charge. */
+SCDAT_API int scdat_set_charge_density(scdat_ctx* ctx, const double* rho);
+/* PICCycle::setTimeStep (PICCycle.h:92-98). */
+SCDAT_API int scdat_set_dt(scdat_ctx* ctx, double dt);
+/* MonteCarloCollisionHandler(seed) (CollisionAlgorithm.h:176): the Philox key of the MCC
+ * streams from the next step on. */
+SCDAT_API int scdat_set_seed(scdat_ctx* ctx, uint64_t seed);
+
 /* MonteCarloCollisionHandler::addCollisionProcess (CollisionAlgorithm.h:176-226) for one
  * species; executed once per step after the push, like executeBackgroundMccStep
  * (CollisionPicAdapter.cpp:338-434). */

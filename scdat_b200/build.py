@@ -3,7 +3,8 @@
     python -m scdat_b200.build          # incremental
     python -m scdat_b200.build --force  # rebuild everything
 
-Objects go to scdat_b200/_build/, the library to scdat_b200/libscdat_b200.so.
+Objects go to scdat_b200/_build/, the library to scdat_b200/libscdat_b200.so, and the C++20
+host layer over it (scdat_b200/host/) to scdat_b200/libscdat_host.so.
 """
 from __future__ import annotations
 
@@ -18,6 +19,9 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libscdat_b200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+CXX = os.environ.get("CXX", "g++")
+HOST_DIR = os.path.join(HERE, "host")
+HOST_LIB = os.path.join(HERE, "libscdat_host.so")
 
 SOURCES = ["capi.cu", "push_f64.cu", "push_mixed.cu", "field.cu", "utils.cu", "pcg_csr.cu", "pcg_noalloc.cu", "mesh_setup.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -59,7 +63,23 @@ def build(force: bool = False, verbose_ptxas: bool = False) -> str:
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    build_host(force)
     return LIB
+
+
+def build_host(force: bool = False) -> str:
+    """The C++20 host layer: g++ over scdat_b200/host/*.cpp, linked to the C-ABI library."""
+    srcs = [os.path.join(HOST_DIR, f) for f in sorted(os.listdir(HOST_DIR)) if f.endswith(".cpp")]
+    deps = srcs + [os.path.join(HOST_DIR, f) for f in os.listdir(HOST_DIR) if f.endswith(".hpp")]
+    deps += [LIB, os.path.join(ROOT, "include", "scdat_b200.h")]
+    if not force and os.path.exists(HOST_LIB) and os.path.getmtime(HOST_LIB) >= max(os.path.getmtime(d) for d in deps):
+        return HOST_LIB
+    cmd = [CXX, "-std=c++20", "-O2", "-fPIC", "-shared", "-Wall", "-Wextra", *srcs, f"-I{os.path.join(ROOT, 'include')}",
+           f"-I{HOST_DIR}", f"-L{HERE}", "-lscdat_b200", "-Wl,-rpath,$ORIGIN", "-o", HOST_LIB]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"host layer build failed:\n{r.stdout}\n{r.stderr}")
+    return HOST_LIB
 
 
 if __name__ == "__main__":

@@ -58,7 +58,7 @@ EXPORTS = ["scdat_default_params", "scdat_create", "scdat_destroy", "scdat_last_
            "scdat_set_elastic_mcc", "scdat_step", "scdat_push", "scdat_solve_field", "scdat_collide", "scdat_compact",
            "scdat_get_fields", "scdat_get_species_charge", "scdat_get_ledger", "scdat_reset_ledger",
            "scdat_get_statistics", "scdat_version", "scdat_stream", "scdat_set_timing", "scdat_get_timing",
-           "scdat_pcg_csr", "scdat_pcg_csr_noalloc"]
+           "scdat_pcg_csr", "scdat_pcg_csr_noalloc", "scdat_set_charge_density", "scdat_set_dt", "scdat_set_seed"]
 
 _LIB = None
 
@@ -79,6 +79,9 @@ def load():
     L.scdat_last_error.argtypes = [vp]
     L.scdat_last_error.restype = C.c_char_p
     L.scdat_set_species.argtypes = [vp, C.c_int32, C.POINTER(SpeciesC)]
+    L.scdat_set_charge_density.argtypes = [vp, vp]
+    L.scdat_set_dt.argtypes = [vp, C.c_double]
+    L.scdat_set_seed.argtypes = [vp, C.c_uint64]
     L.scdat_set_particles.argtypes = [vp, C.c_int32, C.c_int64, vp, vp, vp, vp]
     L.scdat_seed_box_particles.argtypes = [vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_double, vp, vp,
                                            C.c_int32, C.c_double, C.c_uint64]
@@ -250,6 +253,16 @@ class Domain:
     def set_electric_field(self, E):
         E = np.ascontiguousarray(E, np.float64)
         self._ck(self.L.scdat_set_electric_field(self.h, _p(E)))
+
+    def set_charge_density(self, rho):
+        rho = np.ascontiguousarray(rho, np.float64)
+        self._ck(self.L.scdat_set_charge_density(self.h, _p(rho)))
+
+    def set_dt(self, dt):
+        self._ck(self.L.scdat_set_dt(self.h, float(dt)))
+
+    def set_seed(self, seed):
+        self._ck(self.L.scdat_set_seed(self.h, int(seed)))
 
     def set_elastic(self, s, n_target, sigma, mode=0, alpha=0.0, e_ref=1.0, e_th=0.0, enabled=True):
         proc = ElasticC(n_target, sigma, e_ref, alpha, e_th, 1 if enabled else 0, mode)

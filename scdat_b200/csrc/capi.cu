@@ -120,7 +120,7 @@ struct scdat_ctx {
     // poisson
     DBuf<int32_t> row_node, lift_ptr, lift_node, row_ptr, col;
     DBuf<double> cv, lift_val, val, diag, dinv;
-    DBuf<float> valf;
+    DBuf<float> valf, diagf, dinvf;
     DBuf<double> b, x, r, z, p, pn, q;
     DBuf<float> xf, rf, zf, pf, pnf, qf;
     DBuf<PcgScalars> sc;
@@ -156,7 +156,7 @@ struct scdat_ctx {
     double last_pcg_rel = 0.0;
     cudaStream_t st = nullptr;
     int nsm = 148;
-    int grid_push = 148 * 8, grid_nodes = 148 * 4, grid_red = 148 * 2;
+    int grid_push = 148 * 8, grid_nodes = 148 * 4, grid_red = 148 * 8;
     // optional per-kernel timing (CUDA events around the launches on the context stream)
     bool timing = false;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_push, ev_field;
@@ -617,7 +617,7 @@ SCDAT_API int scdat_create(const scdat_mesh_desc* mesh, const scdat_params* para
     CK(cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, dev));
     ctx->grid_push = ctx->nsm * 8;
     ctx->grid_nodes = ctx->nsm * 8;
-    ctx->grid_red = ctx->nsm * 4;
+    ctx->grid_red = ctx->nsm * 8;
     cudaStream_t st = ctx->st;
     // mesh
     CK(ctx->xyz.upload(m.xyz.data(), m.xyz.size(), st));
@@ -684,6 +684,8 @@ SCDAT_API int scdat_create(const scdat_mesh_desc* mesh, const scdat_params* para
     CK(ctx->valf.upload(ps.valf.data(), ps.valf.size(), st));
     CK(ctx->diag.upload(ps.diag.data(), ps.diag.size(), st));
     CK(ctx->dinv.upload(ps.dinv.data(), ps.dinv.size(), st));
+    CK(ctx->diagf.upload(ps.diagf.data(), ps.diagf.size(), st));
+    CK(ctx->dinvf.upload(ps.dinvf.data(), ps.dinvf.size(), st));
     PoissonView& pv = ctx->pv;
     pv.R = ps.R;
     pv.row_node = ctx->row_node.p;
@@ -697,6 +699,8 @@ SCDAT_API int scdat_create(const scdat_mesh_desc* mesh, const scdat_params* para
     pv.valf = ctx->valf.p;
     pv.diag = ctx->diag.p;
     pv.dinv = ctx->dinv.p;
+    pv.diagf = ctx->diagf.p;
+    pv.dinvf = ctx->dinvf.p;
     size_t R = (size_t)std::max(ps.R, 1);
     for (DBuf<double>* v : {&ctx->b, &ctx->x, &ctx->r, &ctx->z, &ctx->p, &ctx->pn, &ctx->q}) CK(v->alloc(R));
     for (DBuf<float>* v : {&ctx->xf, &ctx->rf, &ctx->zf, &ctx->pf, &ctx->pnf, &ctx->qf}) CK(v->alloc(R));
@@ -995,6 +999,30 @@ SCDAT_API int scdat_set_electric_field(scdat_ctx* ctx, const double* E)
     int rc = refresh_tet_field(ctx);
     if (rc) return rc;
     CK(cudaStreamSynchronize(ctx->st));
+    return SCDAT_OK;
+}
+
+SCDAT_API int scdat_set_charge_density(scdat_ctx* ctx, const double* rho)
+{
+    if (!ctx) return SCDAT_ERR_ARG;
+    ARG(rho, "null charge density");
+    CK(cudaMemcpyAsync(ctx->rho.p, rho, sizeof(double) * ctx->hm.N, cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return SCDAT_OK;
+}
+
+SCDAT_API int scdat_set_dt(scdat_ctx* ctx, double dt)
+{
+    if (!ctx) return SCDAT_ERR_ARG;
+    ARG(dt > 0.0 && std::isfinite(dt), "time step must be positive");
+    ctx->prm.dt = dt;
+    return SCDAT_OK;
+}
+
+SCDAT_API int scdat_set_seed(scdat_ctx* ctx, uint64_t seed)
+{
+    if (!ctx) return SCDAT_ERR_ARG;
+    ctx->prm.seed = seed;
     return SCDAT_OK;
 }
 
