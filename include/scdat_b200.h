@@ -220,6 +220,35 @@ SCDAT_API int scdat_reset_ledger(scdat_ctx* ctx);
 /* PICCycle::getStatistics (PICCycle.h:165-168). */
 SCDAT_API int scdat_get_statistics(scdat_ctx* ctx, scdat_stats* st);
 
+/* ---- Batched scenarios (no reference counterpart: the reference runs one PICCycle at a
+ * time) ----
+ * A batch advances many independent contexts (each with its own mesh, species, particles and
+ * potentials, all created with SCDAT_PREC_MIXED) together: every push pass is one launch over
+ * all (scenario, species) pairs, the field solve one launch per kernel over all scenarios with
+ * per-scenario convergence, and the whole step is captured once as a CUDA graph whose solver
+ * loops are conditional nodes.  The contexts stay valid for every query (scdat_get_*); step
+ * them only through the batch while it exists. */
+typedef struct scdat_batch scdat_batch;
+typedef struct {
+    int32_t push_blocks_per_sm;   /* grid of the push launches, in blocks of 256 per SM (default 4) */
+    int32_t field_blocks_per_sm;  /* blocks per SM shared among the scenarios in the field launches (8) */
+    int32_t use_graph;            /* 1: one CUDA-graph launch per step; 0: host-driven loops */
+    int32_t pad;
+} scdat_batch_tuning;
+
+SCDAT_API void scdat_batch_default_tuning(scdat_batch_tuning* t);
+/* On failure *out still holds the batch so that scdat_batch_last_error can be read; destroy it. */
+SCDAT_API int scdat_batch_create(int32_t n, scdat_ctx* const* ctxs, scdat_batch** out);
+SCDAT_API int scdat_batch_destroy(scdat_batch* b);
+SCDAT_API const char* scdat_batch_last_error(const scdat_batch* b);
+SCDAT_API int scdat_batch_step(scdat_batch* b, int32_t n_steps);
+SCDAT_API int scdat_batch_set_tuning(scdat_batch* b, const scdat_batch_tuning* t);
+SCDAT_API int scdat_batch_get_tuning(const scdat_batch* b, scdat_batch_tuning* t);
+/* Times each candidate launch shape on steps_each real steps and keeps the fastest. */
+SCDAT_API int scdat_batch_autotune(scdat_batch* b, int32_t steps_each, scdat_batch_tuning* chosen);
+/* Device time per step of the last run of steps (CUDA events on the batch stream). */
+SCDAT_API int scdat_batch_last_step_ms(const scdat_batch* b, double* ms);
+
 /* The CUDA stream every call of this context runs on (a cudaStream_t), for callers that
  * order their own work or events against the library.  No reference counterpart. */
 SCDAT_API void* scdat_stream(scdat_ctx* ctx);

@@ -43,6 +43,11 @@ class ElasticC(C.Structure):
                 ("alpha", C.c_double), ("e_threshold_ev", C.c_double), ("enabled", C.c_int32), ("mode", C.c_int32)]
 
 
+class BatchTuning(C.Structure):
+    _fields_ = [("push_blocks_per_sm", C.c_int32), ("field_blocks_per_sm", C.c_int32), ("use_graph", C.c_int32),
+                ("pad", C.c_int32)]
+
+
 class StatsC(C.Structure):
     _fields_ = [("completed_steps", C.c_int64), ("simulation_time", C.c_double), ("total_charge", C.c_double),
                 ("total_energy", C.c_double), ("active_particles", C.c_int64), ("stored_particles", C.c_int64),
@@ -58,7 +63,10 @@ EXPORTS = ["scdat_default_params", "scdat_create", "scdat_destroy", "scdat_last_
            "scdat_set_elastic_mcc", "scdat_step", "scdat_push", "scdat_solve_field", "scdat_collide", "scdat_compact",
            "scdat_get_fields", "scdat_get_species_charge", "scdat_get_ledger", "scdat_reset_ledger",
            "scdat_get_statistics", "scdat_version", "scdat_stream", "scdat_set_timing", "scdat_get_timing",
-           "scdat_pcg_csr", "scdat_pcg_csr_noalloc", "scdat_set_charge_density", "scdat_set_dt", "scdat_set_seed"]
+           "scdat_pcg_csr", "scdat_pcg_csr_noalloc", "scdat_set_charge_density", "scdat_set_dt", "scdat_set_seed",
+           "scdat_batch_default_tuning", "scdat_batch_create", "scdat_batch_destroy", "scdat_batch_last_error",
+           "scdat_batch_step", "scdat_batch_set_tuning", "scdat_batch_get_tuning", "scdat_batch_autotune",
+           "scdat_batch_last_step_ms"]
 
 _LIB = None
 
@@ -82,6 +90,17 @@ def load():
     L.scdat_set_charge_density.argtypes = [vp, vp]
     L.scdat_set_dt.argtypes = [vp, C.c_double]
     L.scdat_set_seed.argtypes = [vp, C.c_uint64]
+    L.scdat_batch_default_tuning.argtypes = [C.POINTER(BatchTuning)]
+    L.scdat_batch_default_tuning.restype = None
+    L.scdat_batch_create.argtypes = [C.c_int32, C.POINTER(vp), C.POINTER(vp)]
+    L.scdat_batch_destroy.argtypes = [vp]
+    L.scdat_batch_last_error.argtypes = [vp]
+    L.scdat_batch_last_error.restype = C.c_char_p
+    L.scdat_batch_step.argtypes = [vp, C.c_int32]
+    L.scdat_batch_set_tuning.argtypes = [vp, C.POINTER(BatchTuning)]
+    L.scdat_batch_get_tuning.argtypes = [vp, C.POINTER(BatchTuning)]
+    L.scdat_batch_autotune.argtypes = [vp, C.c_int32, C.POINTER(BatchTuning)]
+    L.scdat_batch_last_step_ms.argtypes = [vp, C.POINTER(C.c_double)]
     L.scdat_set_particles.argtypes = [vp, C.c_int32, C.c_int64, vp, vp, vp, vp]
     L.scdat_seed_box_particles.argtypes = [vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_double, vp, vp,
                                            C.c_int32, C.c_double, C.c_uint64]
@@ -324,3 +343,67 @@ class Domain:
         st = StatsC()
         self._ck(self.L.scdat_get_statistics(self.h, C.byref(st)))
         return {k: getattr(st, k) for k, _ in StatsC._fields_ if k != "pad"}
+
+
+class Batch:
+    """scdat_batch: independent mixed-precision Domains stepped together (one CUDA-graph launch
+    per step).  The Domains stay usable for queries; step them only through the batch."""
+
+    def __init__(self, domains, use_graph=True, push_blocks_per_sm=None, field_blocks_per_sm=None):
+        self.L = load()
+        self.domains = list(domains)
+        arr = (C.c_void_p * len(self.domains))(*[d.h for d in self.domains])
+        h = C.c_void_p()
+        rc = self.L.scdat_batch_create(len(self.domains), arr, C.byref(h))
+        self.h = h
+        if rc != 0:
+            msg = self.L.scdat_batch_last_error(h).decode() if h.value else "batch create failed"
+            if h.value:
+                self.L.scdat_batch_destroy(h)
+            self.h = None
+            raise ScdatError(rc, msg)
+        t = self.tuning()
+        t.use_graph = 1 if use_graph else 0
+        if push_blocks_per_sm:
+            t.push_blocks_per_sm = push_blocks_per_sm
+        if field_blocks_per_sm:
+            t.field_blocks_per_sm = field_blocks_per_sm
+        self.set_tuning(t)
+
+    def _ck(self, rc):
+        if rc != 0:
+            raise ScdatError(rc, self.L.scdat_batch_last_error(self.h).decode())
+        return rc
+
+    def tuning(self):
+        t = BatchTuning()
+        self._ck(self.L.scdat_batch_get_tuning(self.h, C.byref(t)))
+        return t
+
+    def set_tuning(self, t):
+        self._ck(self.L.scdat_batch_set_tuning(self.h, C.byref(t)))
+
+    def step(self, n=1):
+        self._ck(self.L.scdat_batch_step(self.h, int(n)))
+
+    def autotune(self, steps_each=1):
+        t = BatchTuning()
+        self._ck(self.L.scdat_batch_autotune(self.h, int(steps_each), C.byref(t)))
+        return dict(push_blocks_per_sm=t.push_blocks_per_sm, field_blocks_per_sm=t.field_blocks_per_sm,
+                    use_graph=t.use_graph)
+
+    def last_step_ms(self):
+        v = C.c_double()
+        self._ck(self.L.scdat_batch_last_step_ms(self.h, C.byref(v)))
+        return v.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.scdat_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

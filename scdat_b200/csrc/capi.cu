@@ -6,11 +6,7 @@
 //   -> RHS -> PCG -> potentials -> nodal LSQ field
 // which is the order of PICCycle::executeTimeStep (PICCycle.cpp:311-416) followed by the
 // background MCC step of the reference driver (Main/main_PICcore.cpp:487-515).
-#include "../../include/scdat_b200.h"
-#include "common.cuh"
-#include "field.cuh"
-#include "mesh_setup.h"
-#include "push.cuh"
+#include "ctx.cuh"
 
 #include <cub/device/device_radix_sort.cuh>
 
@@ -51,120 +47,6 @@ void launch_scatter_values(int64_t n, const int64_t* idx, const double* v, doubl
 
 using namespace scdat;
 
-namespace {
-
-template <typename T>
-struct DBuf {
-    T* p = nullptr;
-    size_t n = 0;
-    DBuf() = default;
-    DBuf(const DBuf&) = delete;
-    DBuf& operator=(const DBuf&) = delete;
-    ~DBuf() { release(); }
-    void release()
-    {
-        if (p) cudaFree(p);
-        p = nullptr;
-        n = 0;
-    }
-    cudaError_t alloc(size_t count)
-    {
-        release();
-        if (count == 0) return cudaSuccess;
-        cudaError_t e = cudaMalloc((void**)&p, count * sizeof(T));
-        if (e == cudaSuccess) n = count;
-        return e;
-    }
-    cudaError_t upload(const T* h, size_t count, cudaStream_t st)
-    {
-        cudaError_t e = alloc(count);
-        if (e != cudaSuccess || count == 0) return e;
-        return cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, st);
-    }
-    void swap(DBuf& o)
-    {
-        std::swap(p, o.p);
-        std::swap(n, o.n);
-    }
-};
-
-struct SpeciesState {
-    scdat_species sp{};
-    scdat_elastic mcc{};
-    int64_t cap = 0;
-    int64_t n = 0;  // host view of the stored count (updated on set/compact)
-    DBuf<double> x, y, z, vx, vy, vz;
-    DBuf<float> xf, yf, zf, vxf, vyf, vzf;
-    DBuf<int32_t> tet;
-    DBuf<uint32_t> id;
-};
-
-}  // namespace
-
-struct scdat_ctx {
-    std::string err;
-    scdat_params prm{};
-    bool mixed = false;
-    HostMesh hm;
-    HostGeometry hg;
-    HostGrid hgrid;
-    HostGraph hgr;
-    HostPoisson hps;
-    MeshView mv{};
-    PoissonView pv{};
-    // mesh
-    DBuf<double> xyz, geom, erec;
-    DBuf<float> geomf, trec;
-    DBuf<int4> tet, nbr;
-    DBuf<int32_t> bin_start, bin_tets, gptr, gcol;
-    // poisson
-    DBuf<int32_t> row_node, lift_ptr, lift_node, row_ptr, col;
-    DBuf<double> cv, lift_val, val, diag, dinv;
-    DBuf<float> valf, diagf, dinvf;
-    DBuf<double> b, x, r, z, p, pn, q;
-    DBuf<float> xf, rf, zf, pf, pnf, qf;
-    DBuf<PcgScalars> sc;
-    DBuf<double> part;
-    // fields
-    DBuf<double> rho, phi, E, tmp_rho;
-    DBuf<float> Ef;
-    DBuf<unsigned long long> acc_l0, acc_l1, acc_h, totq;
-    // particles
-    std::vector<SpeciesState> species;
-    DBuf<int64_t> counts;
-    DBuf<LedgerDev> led;
-    DBuf<double> ke_part;
-    // sort scratch
-    DBuf<uint32_t> kin, kout, vin, vout;
-    DBuf<unsigned char> cub_tmp;
-    DBuf<double> scratch64;
-    DBuf<float> scratch32;
-    DBuf<int32_t> scratchi;
-    DBuf<uint32_t> scratchu;
-    DBuf<int64_t> nact;
-    DBuf<int64_t> idx64;
-    // deferred-particle lists of the multi-pass push
-    DBuf<unsigned> dcount;
-    DBuf<uint32_t> d1idx, d2idx;
-    DBuf<int> d1it, d2it;
-    DBuf<double> d1rem, d2rem, d1vs, d2vs;
-    unsigned dcap = 0;
-    double uq = 1.0, ue = 1.0;
-    int64_t steps = 0;
-    double sim_time = 0.0;
-    int last_pcg_iter = 0;
-    double last_pcg_rel = 0.0;
-    cudaStream_t st = nullptr;
-    int nsm = 148;
-    int grid_push = 148 * 8, grid_nodes = 148 * 4, grid_red = 148 * 8;
-    // optional per-kernel timing (CUDA events around the launches on the context stream)
-    bool timing = false;
-    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_push, ev_field;
-    double push_ms = 0.0, field_ms = 0.0;
-    int64_t push_launches = 0, field_solves = 0;
-    int64_t push_particles = 0;
-    int64_t launches = 0;  // kernels of this library launched since scdat_set_timing
-};
 
 #define CK(call)                                                                                    \
     do {                                                                                            \
@@ -192,6 +74,10 @@ double pow2_ceil(double v)
     std::frexp(v, &e);  // v = f * 2^e, f in [0.5, 1)
     return std::ldexp(1.0, e);
 }
+
+}  // namespace
+
+namespace scdat {
 
 ParticleStore store_of(scdat_ctx* ctx, int s)
 {
@@ -334,10 +220,10 @@ int refresh_tet_field(scdat_ctx* ctx)
 
 int do_lsq(scdat_ctx* ctx, double reg)
 {
-    CK(cudaMemsetAsync(&ctx->led.p->flags, 0, sizeof(unsigned long long), ctx->st));
+    CK(cudaMemsetAsync(&ctx->led.p->lsq_bad, 0, sizeof(unsigned long long), ctx->st));
     ctx->launches += 2;
     launch_lsq(ctx->hm.N, ctx->xyz.p, ctx->gptr.p, ctx->gcol.p, ctx->phi.p, reg, ctx->E.p, ctx->Ef.p,
-               &ctx->led.p->flags, ctx->grid_nodes, ctx->st);
+               &ctx->led.p->lsq_bad, ctx->grid_nodes, ctx->st);
     CK(cudaGetLastError());
     return refresh_tet_field(ctx);
 }
@@ -547,7 +433,7 @@ int do_sort(scdat_ctx* ctx, int s)
     return SCDAT_OK;
 }
 
-}  // namespace
+}  // namespace scdat
 
 // ======================================================================================
 // C ABI

@@ -157,7 +157,8 @@ struct LedgerDev {
     unsigned long long surf_lo, surf_hi;     // surface_deposited_charge
     unsigned long long substeps, lost_events, mcc_hits, active;
     unsigned long long flags;                // device error flag word
-    unsigned long long pad[5];
+    unsigned long long lsq_bad;              // bit 8: the nodal field had a non-finite value
+    unsigned long long pad[4];
 };
 
 enum DeviceFlag : unsigned long long {

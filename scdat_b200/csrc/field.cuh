@@ -26,7 +26,7 @@ struct PoissonView {
 
 struct PcgScalars {
     double rz, rz_prev, pq, rr, bb, thr2, rtol, abs_thr2;
-    int iter, done, max_iter, pad;
+    int iter, done, max_iter, outer;  // outer: refinement passes (batched mixed solve)
     unsigned int ticket;
     unsigned int pad2[3];
 };

@@ -14,6 +14,7 @@
 // kCap1 sub-steps and appends the unfinished ones to a list; pass 2 gives those up to kCap2
 // more; pass 3 finishes the rest.  The step structure is the reference's
 // CrossTetrahedron::integrateTrajectory (PICParticleAlgorithms.cpp:536-740).
+#include "batch.cuh"
 #include "push.cuh"
 
 namespace scdat {
@@ -52,6 +53,28 @@ __device__ __forceinline__ TetRec load_rec(const MeshView& M, int t)
     R.nd[0] = __float_as_int(f.y); R.nd[1] = __float_as_int(f.z); R.nd[2] = __float_as_int(f.w);
     R.nd[3] = __float_as_int(h.x);
     return R;
+}
+
+// Rewrite words 9..20 of record t (E0 and the three differences) from the nodal field,
+// keeping J^-1 and the node ids that share those 16-byte lines.
+__device__ __forceinline__ void refresh_trec_one(int64_t t, const int4* __restrict__ tet, const double* __restrict__ E,
+                                                 float* trec)
+{
+    int4 tn = tet[t];
+    const double* e0 = E + 3 * (int64_t)tn.x;
+    const double* e1 = E + 3 * (int64_t)tn.y;
+    const double* e2 = E + 3 * (int64_t)tn.z;
+    const double* e3 = E + 3 * (int64_t)tn.w;
+    float* r = trec + 64 * t;
+    float4* r4 = reinterpret_cast<float4*>(r);
+    float j8 = r[8];
+    float nd0 = r[21], nd1 = r[22], nd2 = r[23];
+    r4[2] = make_float4(j8, (float)e0[0], (float)e0[1], (float)e0[2]);
+    r4[3] = make_float4((float)(e1[0] - e0[0]), (float)(e1[1] - e0[1]), (float)(e1[2] - e0[2]),
+                        (float)(e2[0] - e0[0]));
+    r4[4] = make_float4((float)(e2[1] - e0[1]), (float)(e2[2] - e0[2]), (float)(e3[0] - e0[0]),
+                        (float)(e3[1] - e0[1]));
+    r4[5] = make_float4((float)(e3[2] - e0[2]), nd0, nd1, nd2);
 }
 
 __device__ __forceinline__ void baryj(const float* j, float rx, float ry, float rz, float l[4])
@@ -329,61 +352,97 @@ __device__ __forceinline__ void defer_store_f(const ParticleStore& P, const Defe
     P.tet[i] = f.cur;
 }
 
-// Pass 1: every stored particle, at most kCap1 sub-steps.
+// Pass 1 for the 32 particles [base, base + 32) of one warp: at most kCap1 sub-steps, the
+// unfinished ones appended to D.
+__device__ __forceinline__ void push1_warp(const MeshView& M, const ParticleStore& P, const SpeciesDev& S,
+                                           const PushParams& pp, const DeferList& D, ChargeAcc A, LedgerDev* L,
+                                           int64_t base, int64_t n, PushStats& c)
+{
+    const int64_t i = base + (threadIdx.x & 31);
+    int st = -1;
+    FlightF f;
+    if (i < n) {
+        f.cur = P.tet[i];
+        f.vx = P.vxf[i]; f.vy = P.vyf[i]; f.vz = P.vzf[i];
+        if (f.cur <= kTetAbsorbed) {
+            // updateStatistics sums every particle the container still holds (PICCycle.cpp:941-966)
+            double ux = f.vx, uy = f.vy, uz = f.vz;
+            c.ke_sum += 0.5 * S.m * (ux * ux + uy * uy + uz * uz);
+        } else {
+            f.rx = P.xf[i]; f.ry = P.yf[i]; f.rz = P.zf[i];
+            f.vstart = sqrtf(f.vx * f.vx + f.vy * f.vy + f.vz * f.vz);
+            f.rem = (float)pp.dt;
+            f.it = 0;
+            st = kDone;
+            if (f.cur < 0) {
+                // no hint: the stored offset is an absolute position
+                double px = f.rx, py = f.ry, pz = f.rz;
+                int t = locate_far(M, px, py, pz, -1);
+                if (t < 0) {
+                    st = kLost;
+                } else {
+                    double3 o = origin(M, t);
+                    f.rx = (float)(px - o.x); f.ry = (float)(py - o.y); f.rz = (float)(pz - o.z);
+                    f.cur = t;
+                }
+            }
+            if (st != kLost) st = advance_f(M, S, pp, f, kCap1, A, c.nsub);
+        }
+    }
+    unsigned slot = warp_append(st == kCapped, D.count);
+    if (st == kCapped && slot < D.cap) {
+        defer_store_f(P, D, slot, i, f);
+    } else if (st >= 0) {
+        if (st == kCapped) st = advance_f(M, S, pp, f, 0x7fffffff, A, c.nsub);
+        finish_f(M, P, S, pp, L, i, f, st, c);
+    }
+}
+
+// Passes 2 and 3 for entries [base, base + 32) of list Din (up to `cap` sub-steps, then
+// append to Dout; with Dout.count == nullptr the particles run to the end).
+__device__ __forceinline__ void push_more_warp(const MeshView& M, const ParticleStore& P, const SpeciesDev& S,
+                                               const PushParams& pp, const DeferList& Din, const DeferList& Dout,
+                                               int cap, ChargeAcc A, LedgerDev* L, int64_t base, int64_t n,
+                                               PushStats& c)
+{
+    const bool chain = Dout.count != nullptr;
+    const int64_t e = base + (threadIdx.x & 31);
+    int st = -1;
+    FlightF f;
+    int64_t i = 0;
+    if (e < n) {
+        i = Din.idx[e];
+        f.cur = P.tet[i];
+        f.rx = P.xf[i]; f.ry = P.yf[i]; f.rz = P.zf[i];
+        f.vx = P.vxf[i]; f.vy = P.vyf[i]; f.vz = P.vzf[i];
+        f.it = Din.it[e];
+        f.rem = (float)Din.rem[e];
+        f.vstart = (float)Din.vstart[e];
+        st = advance_f(M, S, pp, f, chain ? cap : 0x7fffffff, A, c.nsub);
+    }
+    unsigned slot = chain ? warp_append(st == kCapped, Dout.count) : 0xffffffffu;
+    if (st == kCapped && chain && slot < Dout.cap) {
+        defer_store_f(P, Dout, slot, i, f);
+    } else if (st >= 0) {
+        if (st == kCapped) st = advance_f(M, S, pp, f, 0x7fffffff, A, c.nsub);
+        finish_f(M, P, S, pp, L, i, f, st, c);
+    }
+}
+
+// Pass 1: every stored particle.
 __global__ void __launch_bounds__(256, 4) k_push_mixed(MeshView M, ParticleStore P, SpeciesDev S, PushParams pp,
                                                     DeferList D, ChargeAcc A,
                                                     LedgerDev* L, double* ke_part)
 {
     const int64_t n = *P.count;
     PushStats c{0.0, 0ull, 0ull, 0ull, 0ull};
-    const int lane = threadIdx.x & 31;
     const int64_t gwarp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t base = gwarp * 32; base < n; base += nwarps * 32) {
-        const int64_t i = base + lane;
-        int st = -1;
-        FlightF f;
-        if (i < n) {
-            f.cur = P.tet[i];
-            f.vx = P.vxf[i]; f.vy = P.vyf[i]; f.vz = P.vzf[i];
-            if (f.cur <= kTetAbsorbed) {
-                // updateStatistics sums every particle the container still holds (PICCycle.cpp:941-966)
-                double ux = f.vx, uy = f.vy, uz = f.vz;
-                c.ke_sum += 0.5 * S.m * (ux * ux + uy * uy + uz * uz);
-            } else {
-                f.rx = P.xf[i]; f.ry = P.yf[i]; f.rz = P.zf[i];
-                f.vstart = sqrtf(f.vx * f.vx + f.vy * f.vy + f.vz * f.vz);
-                f.rem = (float)pp.dt;
-                f.it = 0;
-                st = kDone;
-                if (f.cur < 0) {
-                    // no hint: the stored offset is an absolute position
-                    double px = f.rx, py = f.ry, pz = f.rz;
-                    int t = locate_far(M, px, py, pz, -1);
-                    if (t < 0) {
-                        st = kLost;
-                    } else {
-                        double3 o = origin(M, t);
-                        f.rx = (float)(px - o.x); f.ry = (float)(py - o.y); f.rz = (float)(pz - o.z);
-                        f.cur = t;
-                    }
-                }
-                if (st != kLost) st = advance_f(M, S, pp, f, kCap1, A, c.nsub);
-            }
-        }
-        unsigned slot = warp_append(st == kCapped, D.count);
-        if (st == kCapped && slot < D.cap) {
-            defer_store_f(P, D, slot, i, f);
-        } else if (st >= 0) {
-            if (st == kCapped) st = advance_f(M, S, pp, f, 0x7fffffff, A, c.nsub);
-            finish_f(M, P, S, pp, L, i, f, st, c);
-        }
-    }
+    for (int64_t base = gwarp * 32; base < n; base += nwarps * 32) push1_warp(M, P, S, pp, D, A, L, base, n, c);
     block_stats(c, L, ke_part);
 }
 
-// Passes 2 and 3: continue the particles of list `Din` (up to `cap` sub-steps, then append
-// to Dout; with Dout.count == nullptr the particles run to the end).
+// Passes 2 and 3.
 __global__ void __launch_bounds__(256, 4) k_push_mixed_more(MeshView M, ParticleStore P, SpeciesDev S, PushParams pp,
                                                          DeferList Din, DeferList Dout, int cap,
                                                          ChargeAcc A,
@@ -391,34 +450,92 @@ __global__ void __launch_bounds__(256, 4) k_push_mixed_more(MeshView M, Particle
 {
     const int64_t n = (int64_t)min(*Din.count, Din.cap);
     PushStats c{0.0, 0ull, 0ull, 0ull, 0ull};
-    const int lane = threadIdx.x & 31;
     const int64_t gwarp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    const bool chain = Dout.count != nullptr;
-    for (int64_t base = gwarp * 32; base < n; base += nwarps * 32) {
-        const int64_t e = base + lane;
-        int st = -1;
-        FlightF f;
-        int64_t i = 0;
-        if (e < n) {
-            i = Din.idx[e];
-            f.cur = P.tet[i];
-            f.rx = P.xf[i]; f.ry = P.yf[i]; f.rz = P.zf[i];
-            f.vx = P.vxf[i]; f.vy = P.vyf[i]; f.vz = P.vzf[i];
-            f.it = Din.it[e];
-            f.rem = (float)Din.rem[e];
-            f.vstart = (float)Din.vstart[e];
-            st = advance_f(M, S, pp, f, chain ? cap : 0x7fffffff, A, c.nsub);
+    for (int64_t base = gwarp * 32; base < n; base += nwarps * 32)
+        push_more_warp(M, P, S, pp, Din, Dout, cap, A, L, base, n, c);
+    block_stats(c, L, ke_part);
+}
+
+// ---- batched step: all (scenario, species) jobs in one launch per pass -----------------
+__global__ void k_batch_prefix(const PushJob* __restrict__ jobs, int njobs, int pass, int64_t* __restrict__ pre)
+{
+    __shared__ int64_t cnt[kMaxBatchJobs];
+    for (int j = threadIdx.x; j < njobs; j += blockDim.x) {
+        const PushJob& J = jobs[j];
+        int64_t n;
+        if (pass == 1)
+            n = *J.P.count;
+        else if (pass == 2)
+            n = min((int64_t)*J.D1.count, (int64_t)J.D1.cap);
+        else
+            n = min((int64_t)*J.D2.count, (int64_t)J.D2.cap);
+        cnt[j] = (n + 255) / 256;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int64_t a = 0;
+        for (int j = 0; j < njobs; ++j) {
+            pre[j] = a;
+            a += cnt[j];
         }
-        unsigned slot = chain ? warp_append(st == kCapped, Dout.count) : 0xffffffffu;
-        if (st == kCapped && chain && slot < Dout.cap) {
-            defer_store_f(P, Dout, slot, i, f);
-        } else if (st >= 0) {
-            if (st == kCapped) st = advance_f(M, S, pp, f, 0x7fffffff, A, c.nsub);
-            finish_f(M, P, S, pp, L, i, f, st, c);
+        pre[njobs] = a;
+    }
+}
+
+// Pass `pass` (1, 2 or 3) of every job.  Chunk g of the global index belongs to the job j
+// with pre[j] <= g < pre[j + 1]; a block flushes its statistics into a job's ledger when it
+// moves on to the next job.
+template <int PASS>
+__global__ void __launch_bounds__(256, 4) k_push_mixed_batch(const PushJob* __restrict__ jobs, int njobs,
+                                                          const int64_t* __restrict__ pre)
+{
+    __shared__ int64_t spre[kMaxBatchJobs + 1];
+    for (int j = threadIdx.x; j <= njobs; j += blockDim.x) spre[j] = pre[j];
+    __syncthreads();
+    const int64_t total = spre[njobs];
+    PushStats c{0.0, 0ull, 0ull, 0ull, 0ull};
+    int cur = -1;
+    const int warp = threadIdx.x >> 5;
+    for (int64_t g = blockIdx.x; g < total; g += gridDim.x) {
+        int lo = 0, hi = njobs;  // spre[lo] <= g < spre[hi]
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (spre[mid] <= g)
+                lo = mid;
+            else
+                hi = mid;
+        }
+        if (lo != cur) {
+            if (cur >= 0) {
+                block_stats(c, jobs[cur].L, jobs[cur].ke_part);
+                c = PushStats{0.0, 0ull, 0ull, 0ull, 0ull};
+            }
+            cur = lo;
+        }
+        const PushJob& J = jobs[cur];
+        const int64_t base = (g - spre[cur]) * 256 + warp * 32;
+        if (PASS == 1) {
+            push1_warp(J.M, J.P, J.S, J.pp, J.D1, J.A, J.L, base, *J.P.count, c);
+        } else if (PASS == 2) {
+            const int64_t n = min((int64_t)*J.D1.count, (int64_t)J.D1.cap);
+            push_more_warp(J.M, J.P, J.S, J.pp, J.D1, J.D2, kCap2, J.A, J.L, base, n, c);
+        } else {
+            const int64_t n = min((int64_t)*J.D2.count, (int64_t)J.D2.cap);
+            push_more_warp(J.M, J.P, J.S, J.pp, J.D2, DeferList{}, 0, J.A, J.L, base, n, c);
         }
     }
-    block_stats(c, L, ke_part);
+    if (cur >= 0) block_stats(c, jobs[cur].L, jobs[cur].ke_part);
+}
+
+// nodal E -> tet records of every scenario (tets block map)
+__global__ void k_batch_refresh_trec(const FieldJob* __restrict__ jobs, BlockMap m)
+{
+    const int k = m.ctx_of[blockIdx.x];
+    const unsigned lb = blockIdx.x - m.first[k], nb = m.first[k + 1] - m.first[k];
+    const FieldJob& J = jobs[k];
+    for (int64_t t = lb * (int64_t)blockDim.x + threadIdx.x; t < J.T; t += (int64_t)nb * blockDim.x)
+        refresh_trec_one(t, J.tet, J.E, J.trec);
 }
 
 __global__ void k_mcc_mixed(ParticleStore P, SpeciesDev S, PushParams pp, LedgerDev* L)
@@ -471,23 +588,8 @@ __global__ void k_from_mixed(MeshView M, int64_t n, ParticleStore P, double* x, 
 // Refresh the nodal-E words of every tet record from the FP64 nodal field.
 __global__ void k_refresh_trec(int64_t T, const int4* __restrict__ tet, const double* __restrict__ E, float* trec)
 {
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < T; t += (int64_t)gridDim.x * blockDim.x) {
-        int4 tn = tet[t];
-        const double* e0 = E + 3 * (int64_t)tn.x;
-        const double* e1 = E + 3 * (int64_t)tn.y;
-        const double* e2 = E + 3 * (int64_t)tn.z;
-        const double* e3 = E + 3 * (int64_t)tn.w;
-        float* r = trec + 64 * t;
-        float4* r4 = reinterpret_cast<float4*>(r);
-        float j8 = r[8];
-        float nd0 = r[21], nd1 = r[22], nd2 = r[23];
-        r4[2] = make_float4(j8, (float)e0[0], (float)e0[1], (float)e0[2]);
-        r4[3] = make_float4((float)(e1[0] - e0[0]), (float)(e1[1] - e0[1]), (float)(e1[2] - e0[2]),
-                            (float)(e2[0] - e0[0]));
-        r4[4] = make_float4((float)(e2[1] - e0[1]), (float)(e2[2] - e0[2]), (float)(e3[0] - e0[0]),
-                            (float)(e3[1] - e0[1]));
-        r4[5] = make_float4((float)(e3[2] - e0[2]), nd0, nd1, nd2);
-    }
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < T; t += (int64_t)gridDim.x * blockDim.x)
+        refresh_trec_one(t, tet, E, trec);
 }
 
 void launch_push_mixed(const MeshView& M, const ParticleStore& P, const SpeciesDev& S, const PushParams& pp,
@@ -516,6 +618,27 @@ void launch_from_mixed(const MeshView& M, int64_t n, const ParticleStore& P, dou
                        double* vx, double* vy, double* vz, cudaStream_t st)
 {
     k_from_mixed<<<148 * 4, 256, 0, st>>>(M, n, P, x, y, z, vx, vy, vz);
+}
+
+void launch_batch_prefix(const PushJob* jobs, int njobs, int pass, int64_t* chunk_prefix, cudaStream_t st)
+{
+    k_batch_prefix<<<1, 1024, 0, st>>>(jobs, njobs, pass, chunk_prefix);
+}
+
+void launch_push_mixed_batch(const PushJob* jobs, int njobs, const int64_t* chunk_prefix, int pass, int grid,
+                             cudaStream_t st)
+{
+    if (pass == 1)
+        k_push_mixed_batch<1><<<grid, 256, 0, st>>>(jobs, njobs, chunk_prefix);
+    else if (pass == 2)
+        k_push_mixed_batch<2><<<grid, 256, 0, st>>>(jobs, njobs, chunk_prefix);
+    else
+        k_push_mixed_batch<3><<<grid, 256, 0, st>>>(jobs, njobs, chunk_prefix);
+}
+
+void launch_batch_refresh_trec(const FieldJob* jobs, const BlockMap& tets, cudaStream_t st)
+{
+    k_batch_refresh_trec<<<tets.blocks, 256, 0, st>>>(jobs, tets);
 }
 
 void launch_refresh_trec(int64_t T, const int4* tet, const double* E, float* trec, cudaStream_t st)
