@@ -10,6 +10,13 @@ Workloads (all synthetic, seeded; the reference publishes no dataset):
                 FP32 cell-relative push, fixed-point deposit, FP32-SpMV PCG under FP64
                 refinement to 1e-10, elastic MCC (sigma 1e-19 m^2, n_n 1e14 m^-3)   [default]
   plain32       32^3 cells, h = 0.05 m, 8^3-cell body, 20 ppc, FP64, Jacobi-PCG to 1e-8
+  batched64     64 independent scenarios stepped together (one launch per kernel over all of
+                them, one CUDA-graph launch per step, launch shapes autotuned): box edge
+                uniform in 16..64 cells of one Debye length, central body of a quarter of the
+                edge at a bias uniform in -1000..-1 V, n log-uniform in 1e8..1e12 m^-3, Te and
+                Ti log-uniform in 0.1..10 eV, 8..64 ppc per species, dt = 0.1 / omega_pe;
+                mixed form, timed against the plain FP64 form of the same scenarios run one at
+                a time
 Every rank runs an independent replica ("replicas only": the path has no exchange step).
 """
 from __future__ import annotations
@@ -35,7 +42,28 @@ CONFIGS = {
                          density=1e10, te=1.0, ti=1.0, sort_interval=4),
     "plain32": dict(n=32, L=1.6, body=(12, 20), bias=-10.0, ppc=20, dt=2e-8, precision=0, rtol=1e-8, density=1e10,
                     te=1.0, ti=1.0, sort_interval=8),
+    "batched64": dict(scenarios=64, seed=2026, precision=1, rtol=1e-10, sort_interval=4),
 }
+EPS0 = 8.8541878128e-12
+
+
+def batched_scenarios(count, seed):
+    """The seeded scenario list of the batched workload (sizes, plasma, bias, ppc, dt)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        n = int(rng.integers(16, 65))
+        dens = 10 ** rng.uniform(8, 12)
+        te, ti = 10 ** rng.uniform(-1, 1), 10 ** rng.uniform(-1, 1)
+        bias = rng.uniform(-1000, -1)
+        ppc = int(rng.integers(8, 65))
+        h = float(np.sqrt(EPS0 * te / (dens * QE)))  # one electron Debye length
+        wpe = float(np.sqrt(dens * QE * QE / (EPS0 * ME)))
+        q = max(1, n // 4)
+        lo = (n - q) // 2
+        out.append(dict(n=n, L=n * h, body=(lo, lo + q), bias=bias, ppc=ppc, dt=0.1 / wpe, density=dens, te=te,
+                        ti=ti, rtol=1e-10, sort_interval=4))
+    return out
 
 
 def load_peaks():
@@ -98,7 +126,7 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def build_domain(cfg, precision, capi):
+def build_domain(cfg, precision, capi, solve=True):
     n = cfg["n"]
     h = cfg["L"] / n
     body = ((cfg["body"][0], cfg["body"][1]),) * 3 if cfg["body"] else None
@@ -117,7 +145,8 @@ def build_domain(cfg, precision, capi):
     for s in range(2):
         dom.set_elastic(s, 1e14, 1e-19, mode=1)
     dom.set_potential(m["phi"])
-    dom.solve_field(allow_not_converged=True)
+    if solve:
+        dom.solve_field(allow_not_converged=True)
     return dom, m
 
 
@@ -256,6 +285,137 @@ def run_ours(args, cfg):
         print(json.dumps(out))
 
 
+def run_batched(args, cfg):
+    """The batched workload: the plain FP64 form one scenario at a time (the 1x), then the
+    mixed form of the same scenarios as one batch (autotuned, CUDA graph), both for the same
+    number of steps from the same seeded state; potentials compared at the end."""
+    import torch
+
+    from scdat_b200 import build, capi
+
+    build.build()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=900))
+    scen = batched_scenarios(args.scenarios or cfg["scenarios"], cfg["seed"])
+    tune_steps = 6  # scdat_batch_autotune: 6 candidate shapes x 1 step
+    total = tune_steps + args.warmup + args.steps
+    # plain FP64 form, one scenario at a time
+    fp64_ms, fp64_ps, phi64 = 0.0, 0, []
+    for c in scen:
+        dom, _ = build_domain(c, 0, capi)
+        stream = torch.cuda.ExternalStream(dom.stream())
+        for _ in range(total - args.steps):
+            dom.step(1)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            dom.step(1)
+            fp64_ps += dom.stats()["active_particles"]
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        fp64_ms += ev0.elapsed_time(ev1)
+        phi64.append(dom.fields()[1])
+        dom.close()
+    # mixed form, all scenarios in one batch
+    built = [build_domain(c, 1, capi) for c in scen]
+    doms = [dm for dm, _ in built]
+    batch = capi.Batch(doms)
+    chosen = batch.autotune(1)
+    for _ in range(args.warmup):
+        batch.step(1)
+    stream = torch.cuda.ExternalStream(batch.stream())
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    launches0 = batch.kernel_launches()
+    clocks = ClockSampler(local)
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    ps = 0
+    for _ in range(args.steps):
+        batch.step(1)
+        ps += sum(d.stats()["active_particles"] for d in doms)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    clk = clocks.stop()
+    launches = batch.kernel_launches() - launches0
+    errs = []
+    for d, p64 in zip(doms, phi64):
+        errs.append(float(np.abs(d.fields()[1] - p64).max() / max(np.abs(p64).max(), 1e-300)))
+    parts = int(sum(d.count(s) for d in doms for s in range(d.nspecies)))
+    # end to end through the C ABI with host buffers: per step, each scenario's Dirichlet
+    # potentials in from pinned memory, the potentials and statistics back
+    dirs = [np.nonzero(m["dirichlet"])[0].astype(np.int64) for _, m in built]
+    h_nodes = [torch.from_numpy(dn).pin_memory() for dn in dirs]
+    h_vals = [torch.from_numpy(m["phi"][dn].copy()).pin_memory() for (_, m), dn in zip(built, dirs)]
+    h_phi = [torch.empty(d.N, dtype=torch.float64).pin_memory() for d in doms]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e2e_ps = 0
+    e2e_steps = max(1, min(args.steps, 3))
+    for _ in range(e2e_steps):
+        for d, hn, hv in zip(doms, h_nodes, h_vals):
+            d.L.scdat_set_node_potentials(d.h, hn.shape[0], hn.data_ptr(), hv.data_ptr())
+        batch.step(1)
+        for d, hp in zip(doms, h_phi):
+            d.L.scdat_get_fields(d.h, None, hp.data_ptr(), None)
+            e2e_ps += d.stats()["active_particles"]
+    e2e_val = e2e_ps / (time.perf_counter() - t0)
+    h2d = int(sum(16 * len(dn) for dn in dirs))
+    d2h = int(sum(8 * d.N + 120 for d in doms))
+    batch.close()
+    for d in doms:
+        d.close()
+    t_local = ms / 1e3
+    if dist:
+        t = torch.tensor([t_local, float(ps)], device="cuda", dtype=torch.float64)
+        tmax = t.clone()
+        dist.all_reduce(tmax[:1], op=dist.ReduceOp.MAX)
+        dist.all_reduce(t[1:], op=dist.ReduceOp.SUM)
+        t_max, total_ps = float(tmax[0]), float(t[1])
+    else:
+        t_max, total_ps = t_local, float(ps)
+    out = {
+        "metric": "PIC particle-steps/s on 1 B200 (mixed/batched vs plain FP64 at equal error)",
+        "value": total_ps / t_max,
+        "unit": "particle-steps/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": t_max * 1e3 / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded scenarios, no dataset)",
+        "config": {"workload": "batched64", "scenarios": len(scen), "particles": parts,
+                   "cells": int(sum(c["n"] ** 3 for c in scen)), "edge_cells": [c["n"] for c in scen],
+                   "precision": "mixed, batched, CUDA graph", "tuning": chosen, "pcg_rtol": 1e-10,
+                   "l2": "inputs larger than L2 (particle state > 126 MB)", "parallelism": f"replicas x{world}"},
+        "fp64_form": {"value": fp64_ps / (fp64_ms / 1e3), "unit": "particle-steps/s", "steps": args.steps,
+                      "ms_per_step": fp64_ms / args.steps, "note": "plain FP64 form, scenarios one at a time"},
+        "phi_rel_err_vs_fp64": {"max": max(errs), "median": float(np.median(errs)), "after_steps": total},
+        "gpu_launches": int(launches),
+        "clocks": clk,
+        "e2e": {"value": e2e_val, "unit": "particle-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+    }
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out))
+
+
 def fp64_compare(cfg, args):
     """The plain FP64 form on the same workload (the 1x of the mixed-form speed-up)."""
     import torch
@@ -369,8 +529,15 @@ def main():
     ap.add_argument("--ppc", type=int, default=0, help="override particles per cell per species")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64-compare", dest="fp64_compare", action="store_false")
+    ap.add_argument("--scenarios", type=int, default=0, help="batched64: number of scenarios (default 64)")
     args = ap.parse_args()
     cfg = dict(CONFIGS[args.config])
+    if args.config == "batched64":
+        if args.impl == "reference":
+            run_reference(args, dict(CONFIGS["precision128"]))
+        else:
+            run_batched(args, cfg)
+        return
     if args.n:
         f = args.n / cfg["n"]
         cfg["body"] = (int(cfg["body"][0] * f), int(cfg["body"][1] * f))

@@ -186,6 +186,29 @@ SCDAT_API int scdat_set_dt(scdat_ctx* ctx, double dt);
  * streams from the next step on. */
 SCDAT_API int scdat_set_seed(scdat_ctx* ctx, uint64_t seed);
 
+/* Surface circuit of the body (the surface-charging caller's dielectric faces, no PICCycle
+ * counterpart): each face XMin..ZMax of the body box [body_lo, body_hi] is a circuit node with
+ * capacitance eps0*eps_r*A/d (Toolkit/Surface Charging/src/DensePlasmaSurfaceCharging.cpp:6544-6552;
+ * A = the face's area when area[f] is 0), a shunt conductance to ground and a linearised plasma
+ * current.  Each scdat_step collects the charge of the particles lost into the body per face,
+ * advances the face potentials with the implicit node update of
+ * SurfaceCircuitCoupling::advanceImplicit (Tools/Coupling/src/SurfaceCircuitCoupling.cpp:953-966)
+ * in FP64, and gives the body's surface nodes the mean potential of their faces before the field
+ * solve.  Turns on body_tally. */
+typedef struct {
+    double body_lo[3], body_hi[3];
+    double eps_r[6];       /* relative permittivity of each face's dielectric */
+    double thickness[6];   /* m */
+    double area[6];        /* m^2; 0 = from the box */
+    double v0[6];          /* initial potential, V */
+    double shunt_s[6];     /* conductance to ground, S (0 = floating) */
+    double didv[6];        /* plasma current linearisation dI/dV, A/V (0 = plain charge integration) */
+} scdat_surface_circuit;
+SCDAT_API int scdat_set_surface_circuit(scdat_ctx* ctx, const scdat_surface_circuit* sc);
+/* Face potentials [6], collected charge [6], last-step current [6] and the number of particles
+ * collected so far [6]; any pointer may be NULL. */
+SCDAT_API int scdat_get_surface_state(scdat_ctx* ctx, double* V, double* Q, double* I, int64_t* counts);
+
 /* MonteCarloCollisionHandler::addCollisionProcess (CollisionAlgorithm.h:176-226) for one
  * species; executed once per step after the push, like executeBackgroundMccStep
  * (CollisionPicAdapter.cpp:338-434). */
@@ -248,6 +271,10 @@ SCDAT_API int scdat_batch_get_tuning(const scdat_batch* b, scdat_batch_tuning* t
 SCDAT_API int scdat_batch_autotune(scdat_batch* b, int32_t steps_each, scdat_batch_tuning* chosen);
 /* Device time per step of the last run of steps (CUDA events on the batch stream). */
 SCDAT_API int scdat_batch_last_step_ms(const scdat_batch* b, double* ms);
+/* The CUDA stream the batch steps on (a cudaStream_t). */
+SCDAT_API int scdat_batch_stream(const scdat_batch* b, void** stream);
+/* Kernels of this library the batch's steps have launched so far. */
+SCDAT_API int scdat_batch_kernel_launches(scdat_batch* b, int64_t* launches);
 
 /* The CUDA stream every call of this context runs on (a cudaStream_t), for callers that
  * order their own work or events against the library.  No reference counterpart. */

@@ -506,3 +506,68 @@ class Reference:
         hits = int(self.L.ref_mcc_count(v.shape[0], np.ascontiguousarray(v, np.float64).reshape(-1), kind, w, sigma,
                                         n_target, dt, seed, repeats, C.byref(sc)))
         return hits, sc.value
+
+
+# ----------------------------------------------------------------------------------------
+# Surface circuit of the body faces (restated for the parity tests; no reference test covers
+# an interior body, so these follow the device rule and the reference's node update)
+# ----------------------------------------------------------------------------------------
+EPS0 = 8.8541878128e-12
+
+
+def body_face_of(x, blo, bhi):
+    """Face XMin..ZMax of the body box nearest to each position (ties: the lowest face)."""
+    d = np.stack([np.abs(x[:, 0] - blo[0]), np.abs(bhi[0] - x[:, 0]), np.abs(x[:, 1] - blo[1]),
+                  np.abs(bhi[1] - x[:, 1]), np.abs(x[:, 2] - blo[2]), np.abs(bhi[2] - x[:, 2])], axis=1)
+    return np.argmin(d, axis=1)
+
+
+class SurfaceCircuit:
+    """Faces of the body box as circuit nodes, C = eps0 eps_r A / d
+    (DensePlasmaSurfaceCharging.cpp:6544-6552), advanced per step by the implicit node update
+    of SurfaceCircuitCoupling::advanceImplicit (SurfaceCircuitCoupling.cpp:953-966):
+    (C/dt + G - dI/dV) V' = C/dt V + I - dI/dV V with I = dq/dt."""
+
+    def __init__(self, mesh, blo, bhi, eps_r=3.0, thickness=1e-3, v0=0.0, shunt=0.0, didv=0.0):
+        self.blo, self.bhi = np.asarray(blo, float), np.asarray(bhi, float)
+        ext = self.bhi - self.blo
+        area = np.array([ext[(f // 2 + 1) % 3] * ext[(f // 2 + 2) % 3] for f in range(6)])
+        b = lambda v: np.broadcast_to(np.asarray(v, float), (6,)).copy()
+        self.C = EPS0 * b(eps_r) * area / b(thickness)
+        self.G, self.didv, self.V = b(shunt), b(didv), b(v0)
+        self.Q = np.zeros(6)
+        tol = 1e-9 * ext.max()
+        p = mesh.xyz
+        inside = np.all((p >= self.blo - tol) & (p <= self.bhi + tol), axis=1) & (mesh.dirichlet == 1)
+        masks = np.zeros(mesh.N, np.int64)
+        for f in range(6):
+            a = f // 2
+            plane = self.bhi[a] if f & 1 else self.blo[a]
+            masks |= (inside & (np.abs(p[:, a] - plane) <= tol)).astype(np.int64) << f
+        self.nodes = np.nonzero(masks)[0]
+        self.masks = masks[self.nodes]
+
+    def collect(self, x_lost, q_lost):
+        """Charge of this step's particles lost into the body, per face."""
+        dq = np.zeros(6)
+        if len(q_lost):
+            np.add.at(dq, body_face_of(x_lost, self.blo, self.bhi), q_lost)
+        return dq
+
+    def advance(self, dq, dt):
+        self.Q += dq
+        I = dq / dt
+        cdt = self.C / dt
+        den = cdt + self.G - self.didv
+        ok = den > 0
+        self.V[ok] = ((cdt * self.V + I - self.didv * self.V) / np.where(ok, den, 1.0))[ok]
+
+    def apply(self, phi):
+        for i, m in zip(self.nodes, self.masks):
+            faces = [f for f in range(6) if (m >> f) & 1]
+            s = 0.0
+            for f in faces:
+                s += self.V[f]
+            phi[i] = s / len(faces)
+        return phi
+

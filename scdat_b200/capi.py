@@ -48,6 +48,12 @@ class BatchTuning(C.Structure):
                 ("pad", C.c_int32)]
 
 
+class SurfaceCircuitC(C.Structure):
+    _fields_ = [("body_lo", C.c_double * 3), ("body_hi", C.c_double * 3), ("eps_r", C.c_double * 6),
+                ("thickness", C.c_double * 6), ("area", C.c_double * 6), ("v0", C.c_double * 6),
+                ("shunt_s", C.c_double * 6), ("didv", C.c_double * 6)]
+
+
 class StatsC(C.Structure):
     _fields_ = [("completed_steps", C.c_int64), ("simulation_time", C.c_double), ("total_charge", C.c_double),
                 ("total_energy", C.c_double), ("active_particles", C.c_int64), ("stored_particles", C.c_int64),
@@ -66,7 +72,8 @@ EXPORTS = ["scdat_default_params", "scdat_create", "scdat_destroy", "scdat_last_
            "scdat_pcg_csr", "scdat_pcg_csr_noalloc", "scdat_set_charge_density", "scdat_set_dt", "scdat_set_seed",
            "scdat_batch_default_tuning", "scdat_batch_create", "scdat_batch_destroy", "scdat_batch_last_error",
            "scdat_batch_step", "scdat_batch_set_tuning", "scdat_batch_get_tuning", "scdat_batch_autotune",
-           "scdat_batch_last_step_ms"]
+           "scdat_batch_last_step_ms", "scdat_batch_stream", "scdat_batch_kernel_launches",
+           "scdat_set_surface_circuit", "scdat_get_surface_state"]
 
 _LIB = None
 
@@ -101,6 +108,10 @@ def load():
     L.scdat_batch_get_tuning.argtypes = [vp, C.POINTER(BatchTuning)]
     L.scdat_batch_autotune.argtypes = [vp, C.c_int32, C.POINTER(BatchTuning)]
     L.scdat_batch_last_step_ms.argtypes = [vp, C.POINTER(C.c_double)]
+    L.scdat_batch_stream.argtypes = [vp, C.POINTER(vp)]
+    L.scdat_set_surface_circuit.argtypes = [vp, C.POINTER(SurfaceCircuitC)]
+    L.scdat_get_surface_state.argtypes = [vp, vp, vp, vp, vp]
+    L.scdat_batch_kernel_launches.argtypes = [vp, C.POINTER(C.c_int64)]
     L.scdat_set_particles.argtypes = [vp, C.c_int32, C.c_int64, vp, vp, vp, vp]
     L.scdat_seed_box_particles.argtypes = [vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_double, vp, vp,
                                            C.c_int32, C.c_double, C.c_uint64]
@@ -283,6 +294,26 @@ class Domain:
     def set_seed(self, seed):
         self._ck(self.L.scdat_set_seed(self.h, int(seed)))
 
+    def set_surface_circuit(self, body_lo, body_hi, eps_r=3.0, thickness=1e-3, v0=0.0, shunt=0.0, didv=0.0,
+                            area=0.0):
+        """Faces XMin..ZMax of the body box as floating dielectric patches (scalars apply to all)."""
+        sc = SurfaceCircuitC()
+        for a in range(3):
+            sc.body_lo[a] = body_lo[a]
+            sc.body_hi[a] = body_hi[a]
+        for name, val in (("eps_r", eps_r), ("thickness", thickness), ("v0", v0), ("shunt_s", shunt),
+                          ("didv", didv), ("area", area)):
+            arr = np.broadcast_to(np.asarray(val, np.float64), (6,))
+            for f in range(6):
+                getattr(sc, name)[f] = float(arr[f])
+        self._ck(self.L.scdat_set_surface_circuit(self.h, C.byref(sc)))
+
+    def surface_state(self):
+        V, Q, I = np.zeros(6), np.zeros(6), np.zeros(6)
+        n = np.zeros(6, np.int64)
+        self._ck(self.L.scdat_get_surface_state(self.h, _p(V), _p(Q), _p(I), _p(n)))
+        return dict(V=V, Q=Q, I=I, counts=n)
+
     def set_elastic(self, s, n_target, sigma, mode=0, alpha=0.0, e_ref=1.0, e_th=0.0, enabled=True):
         proc = ElasticC(n_target, sigma, e_ref, alpha, e_th, 1 if enabled else 0, mode)
         self._ck(self.L.scdat_set_elastic_mcc(self.h, s, C.byref(proc)))
@@ -391,6 +422,16 @@ class Batch:
         self._ck(self.L.scdat_batch_autotune(self.h, int(steps_each), C.byref(t)))
         return dict(push_blocks_per_sm=t.push_blocks_per_sm, field_blocks_per_sm=t.field_blocks_per_sm,
                     use_graph=t.use_graph)
+
+    def stream(self):
+        v = C.c_void_p()
+        self._ck(self.L.scdat_batch_stream(self.h, C.byref(v)))
+        return v.value
+
+    def kernel_launches(self):
+        v = C.c_int64()
+        self._ck(self.L.scdat_batch_kernel_launches(self.h, C.byref(v)))
+        return v.value
 
     def last_step_ms(self):
         v = C.c_double()

@@ -11,6 +11,7 @@
 
 #include "field.cuh"
 #include "push.cuh"
+#include "surface.cuh"
 
 namespace scdat {
 
@@ -60,6 +61,13 @@ struct FieldJob {
     float* Ef;
     const int4* tet;
     float* trec;
+    // surface circuit (surf == nullptr: none)
+    SurfaceDev* surf;
+    LedgerDev* led;
+    double dt;
+    const int32_t* surf_node;
+    const uint8_t* surf_mask;
+    int64_t surf_n;
 };
 
 // Block b of a field launch works on scenario ctx_of[b], as block b - first[ctx] of
@@ -80,14 +88,16 @@ void launch_batch_refresh_trec(const FieldJob* jobs, const BlockMap& tets, cudaS
 // field (batch_field.cu).  cond_* are CUDA-graph conditional handles (0 outside a graph);
 // any_out (nullable) receives the same "some scenario still iterating" flag for a host loop.
 void launch_batch_zero(const FieldJob* jobs, const PushJob* pjobs, int njobs, int npjobs, int grid, cudaStream_t st);
+void launch_batch_surface(const FieldJob* jobs, int njobs, cudaStream_t st);
 void launch_batch_finalize_rhs(const FieldJob* jobs, const BlockMap& nodes, const BlockMap& rows, cudaStream_t st);
 void launch_batch_pcg_mixed_prologue(const FieldJob* jobs, const BlockMap& rows, int njobs, cudaStream_t st);
 void launch_batch_outer_begin(const FieldJob* jobs, const BlockMap& rows, int njobs, unsigned long long cond_inner,
                               int* any_out, cudaStream_t st);
+// passes[0] counts refinement passes, passes[1] inner double-iterations (launch accounting)
 void launch_batch_inner_iter2(const FieldJob* jobs, const BlockMap& rows, int njobs, unsigned long long cond_inner,
-                              int* any_out, cudaStream_t st);
+                              int* any_out, unsigned long long* passes, cudaStream_t st);
 void launch_batch_outer_end(const FieldJob* jobs, const BlockMap& rows, int njobs, unsigned long long cond_outer,
-                            int* any_out, cudaStream_t st);
+                            int* any_out, unsigned long long* passes, cudaStream_t st);
 void launch_batch_epilogue(const FieldJob* jobs, const BlockMap& nodes, const BlockMap& rows, const BlockMap& tets,
                            PushJob* pjobs, int npjobs, cudaStream_t st);
 

@@ -51,6 +51,17 @@ __global__ void k_batch_zero(const FieldJob* __restrict__ jobs, const PushJob* _
     }
 }
 
+// one block per scenario: its surface circuit's step (face charges -> potentials -> nodes)
+__global__ void k_batch_surface(const FieldJob* __restrict__ jobs)
+{
+    const FieldJob& J = jobs[blockIdx.x];
+    if (!J.surf) return;
+    if (threadIdx.x < J.surf->n) surface_advance_face(J.surf, J.led, threadIdx.x, J.uq, J.dt);
+    __syncthreads();
+    for (int64_t i = threadIdx.x; i < J.surf_n; i += blockDim.x)
+        if (J.surf_mask[i]) J.phi[J.surf_node[i]] = surface_node_potential(J.surf, J.surf_mask[i]);
+}
+
 __global__ void k_batch_finalize(const FieldJob* __restrict__ jobs, BlockMap m)
 {
     Grid g;
@@ -157,7 +168,7 @@ __global__ void k_batch_update32(const FieldJob* __restrict__ jobs, BlockMap m)
 }
 
 __global__ void k_batch_inner_check(const FieldJob* __restrict__ jobs, int njobs, unsigned long long cond,
-                                    int* any_out)
+                                    int* any_out, unsigned long long* passes)
 {
     int active = 0;
     for (int k = threadIdx.x; k < njobs; k += blockDim.x)
@@ -166,6 +177,7 @@ __global__ void k_batch_inner_check(const FieldJob* __restrict__ jobs, int njobs
     if (threadIdx.x == 0) {
         set_cond(cond, active ? 1u : 0u);
         if (any_out) *any_out = active;
+        passes[1] += 1ull;
     }
 }
 
@@ -177,7 +189,8 @@ __global__ void k_batch_add_correction(const FieldJob* __restrict__ jobs, BlockM
     k_add_correction_body(J.A.R, J.x, J.xf, g);
 }
 
-__global__ void k_batch_outer_end(const FieldJob* __restrict__ jobs, int njobs, unsigned long long cond, int* any_out)
+__global__ void k_batch_outer_end(const FieldJob* __restrict__ jobs, int njobs, unsigned long long cond, int* any_out,
+                                  unsigned long long* passes)
 {
     int active = 0;
     for (int k = threadIdx.x; k < njobs; k += blockDim.x) {
@@ -191,6 +204,7 @@ __global__ void k_batch_outer_end(const FieldJob* __restrict__ jobs, int njobs, 
     if (threadIdx.x == 0) {
         set_cond(cond, active ? 1u : 0u);
         if (any_out) *any_out = active;
+        passes[0] += 1ull;
     }
 }
 
@@ -227,6 +241,11 @@ void launch_batch_zero(const FieldJob* jobs, const PushJob* pjobs, int njobs, in
     k_batch_zero<<<dim3(grid, njobs), 256, 0, st>>>(jobs, pjobs, npjobs);
 }
 
+void launch_batch_surface(const FieldJob* jobs, int njobs, cudaStream_t st)
+{
+    k_batch_surface<<<njobs, 256, 0, st>>>(jobs);
+}
+
 void launch_batch_finalize_rhs(const FieldJob* jobs, const BlockMap& nodes, const BlockMap& rows, cudaStream_t st)
 {
     k_batch_finalize<<<nodes.blocks, 256, 0, st>>>(jobs, nodes);
@@ -248,20 +267,20 @@ void launch_batch_outer_begin(const FieldJob* jobs, const BlockMap& rows, int nj
 }
 
 void launch_batch_inner_iter2(const FieldJob* jobs, const BlockMap& rows, int njobs, unsigned long long cond_inner,
-                              int* any_out, cudaStream_t st)
+                              int* any_out, unsigned long long* passes, cudaStream_t st)
 {
     k_batch_spmv32<0><<<rows.blocks, 256, 0, st>>>(jobs, rows);
     k_batch_update32<0><<<rows.blocks, 256, 0, st>>>(jobs, rows);
     k_batch_spmv32<1><<<rows.blocks, 256, 0, st>>>(jobs, rows);
     k_batch_update32<1><<<rows.blocks, 256, 0, st>>>(jobs, rows);
-    k_batch_inner_check<<<1, 1024, 0, st>>>(jobs, njobs, cond_inner, any_out);
+    k_batch_inner_check<<<1, 1024, 0, st>>>(jobs, njobs, cond_inner, any_out, passes);
 }
 
 void launch_batch_outer_end(const FieldJob* jobs, const BlockMap& rows, int njobs, unsigned long long cond_outer,
-                            int* any_out, cudaStream_t st)
+                            int* any_out, unsigned long long* passes, cudaStream_t st)
 {
     k_batch_add_correction<<<rows.blocks, 256, 0, st>>>(jobs, rows);
-    k_batch_outer_end<<<1, 1024, 0, st>>>(jobs, njobs, cond_outer, any_out);
+    k_batch_outer_end<<<1, 1024, 0, st>>>(jobs, njobs, cond_outer, any_out, passes);
 }
 
 void launch_batch_epilogue(const FieldJob* jobs, const BlockMap& nodes, const BlockMap& rows, const BlockMap& tets,

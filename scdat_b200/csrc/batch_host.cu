@@ -61,6 +61,7 @@ struct scdat_batch {
     DBuf<int64_t> prefix;
     DBuf<PcgScalars> sco;
     DBuf<int> any;
+    DBuf<unsigned long long> passes;  // [outer passes, inner double-iterations]
     int* any_host = nullptr;
     MapBufs nodes, rows, tets;
     scdat_batch_tuning tune{};
@@ -165,6 +166,12 @@ int upload_jobs(scdat_batch* b)
         F.Ef = c->Ef.p;
         F.tet = c->tet.p;
         F.trec = c->trec.p;
+        F.surf = c->surface ? c->surf.p : nullptr;
+        F.led = c->led.p;
+        F.dt = c->prm.dt;
+        F.surf_node = c->surf_node.p;
+        F.surf_mask = c->surf_mask.p;
+        F.surf_n = (int64_t)c->surf_node.n;
         fj.push_back(F);
     }
     BCK(cudaMemcpyAsync(b->pjobs.p, pj.data(), sizeof(PushJob) * pj.size(), cudaMemcpyHostToDevice, b->st));
@@ -198,6 +205,7 @@ void enqueue_front(scdat_batch* b, cudaStream_t s)
         launch_batch_prefix(b->pjobs.p, nj, pass, b->prefix.p, s);
         launch_push_mixed_batch(b->pjobs.p, nj, b->prefix.p, pass, grid, s);
     }
+    launch_batch_surface(b->fjobs.p, nc, s);
     launch_batch_finalize_rhs(b->fjobs.p, b->nodes.view, b->rows.view, s);
     launch_batch_pcg_mixed_prologue(b->fjobs.p, b->rows.view, nc, s);
 }
@@ -224,11 +232,11 @@ int step_eager(scdat_batch* b)
         int a = read_any(b);
         if (a < 0) return SCDAT_ERR_CUDA;
         while (a) {
-            for (int k = 0; k < 8; ++k) launch_batch_inner_iter2(b->fjobs.p, b->rows.view, nc, 0ull, b->any.p, b->st);
+            for (int k = 0; k < 8; ++k) launch_batch_inner_iter2(b->fjobs.p, b->rows.view, nc, 0ull, b->any.p, b->passes.p, b->st);
             a = read_any(b);
             if (a < 0) return SCDAT_ERR_CUDA;
         }
-        launch_batch_outer_end(b->fjobs.p, b->rows.view, nc, 0ull, b->any.p, b->st);
+        launch_batch_outer_end(b->fjobs.p, b->rows.view, nc, 0ull, b->any.p, b->passes.p, b->st);
         a = read_any(b);
         if (a < 0) return SCDAT_ERR_CUDA;
         if (!a) break;
@@ -281,9 +289,9 @@ int capture_graph(scdat_batch* b)
         rc = add_while(b, b->st2, h_in, &ibody);
         if (rc) return rc;
         BCK(cudaStreamBeginCaptureToGraph(b->st3, ibody, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-        launch_batch_inner_iter2(b->fjobs.p, b->rows.view, nc, (unsigned long long)h_in, nullptr, b->st3);
+        launch_batch_inner_iter2(b->fjobs.p, b->rows.view, nc, (unsigned long long)h_in, nullptr, b->passes.p, b->st3);
         BCK(cudaStreamEndCapture(b->st3, &ibody));
-        launch_batch_outer_end(b->fjobs.p, b->rows.view, nc, (unsigned long long)h_out, nullptr, b->st2);
+        launch_batch_outer_end(b->fjobs.p, b->rows.view, nc, (unsigned long long)h_out, nullptr, b->passes.p, b->st2);
         BCK(cudaStreamEndCapture(b->st2, &obody));
     }
     enqueue_back(b, b->st);
@@ -395,6 +403,8 @@ SCDAT_API int scdat_batch_create(int32_t n, scdat_ctx* const* ctxs, scdat_batch*
     BCK(b->sco.alloc((size_t)n));
     BCK(cudaMemsetAsync(b->sco.p, 0, sizeof(PcgScalars) * n, b->st));
     BCK(b->any.alloc(1));
+    BCK(b->passes.alloc(2));
+    BCK(cudaMemsetAsync(b->passes.p, 0, 2 * sizeof(unsigned long long), b->st));
     int rc = sync_contexts(b);
     if (rc) return rc;
     // the inner-solve scalars start with their reduction tickets at zero
@@ -499,6 +509,24 @@ SCDAT_API int scdat_batch_step(scdat_batch* b, int32_t n_steps)
         done += run;
         b->steps += run;
     }
+    return SCDAT_OK;
+}
+
+SCDAT_API int scdat_batch_stream(const scdat_batch* b, void** stream)
+{
+    if (!b || !stream) return SCDAT_ERR_ARG;
+    *stream = (void*)b->st;
+    return SCDAT_OK;
+}
+
+// Kernels of this library launched by the steps so far: 16 per step plus 6 per refinement
+// pass and 5 per inner double-iteration (the loop passes are counted on the device).
+SCDAT_API int scdat_batch_kernel_launches(scdat_batch* b, int64_t* launches)
+{
+    if (!b || !launches) return SCDAT_ERR_ARG;
+    unsigned long long p[2] = {0, 0};
+    BCK(cudaMemcpy(p, b->passes.p, sizeof(p), cudaMemcpyDeviceToHost));
+    *launches = 16 * b->steps + 6 * (int64_t)p[0] + 5 * (int64_t)p[1];
     return SCDAT_OK;
 }
 

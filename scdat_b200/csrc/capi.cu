@@ -141,6 +141,11 @@ PushParams push_params(const scdat_ctx* ctx, bool do_mcc)
     pp.seed = ctx->prm.seed;
     pp.step = (uint32_t)ctx->steps;
     pp.deposit = 1;
+    pp.patches = ctx->surface ? 1 : 0;
+    for (int a = 0; a < 3; ++a) {
+        pp.blo[a] = ctx->body_lo[a];
+        pp.bhi[a] = ctx->body_hi[a];
+    }
     return pp;
 }
 
@@ -382,6 +387,19 @@ int harvest_timing(scdat_ctx* ctx)
         cudaEventDestroy(pr.second);
     }
     ctx->ev_field.clear();
+    return SCDAT_OK;
+}
+
+// the surface circuit's step: face charges -> face potentials -> Dirichlet values of the
+// body's surface nodes for the following field solve
+int do_surface(scdat_ctx* ctx)
+{
+    if (!ctx->surface) return SCDAT_OK;
+    ctx->launches += 2;
+    launch_surface_advance(ctx->surf.p, ctx->led.p, ctx->uq, ctx->prm.dt, ctx->st);
+    launch_surface_apply(ctx->surf.p, (int64_t)ctx->surf_node.n, ctx->surf_node.p, ctx->surf_mask.p, ctx->phi.p,
+                         ctx->st);
+    CK(cudaGetLastError());
     return SCDAT_OK;
 }
 
@@ -912,6 +930,85 @@ SCDAT_API int scdat_set_seed(scdat_ctx* ctx, uint64_t seed)
     return SCDAT_OK;
 }
 
+SCDAT_API int scdat_set_surface_circuit(scdat_ctx* ctx, const scdat_surface_circuit* sc)
+{
+    if (!ctx) return SCDAT_ERR_ARG;
+    ARG(sc, "null surface circuit");
+    ARG(!ctx->species.empty(), "set the species first");
+    for (int a = 0; a < 3; ++a) ARG(sc->body_hi[a] > sc->body_lo[a], "empty body box");
+    const double ext[3] = {sc->body_hi[0] - sc->body_lo[0], sc->body_hi[1] - sc->body_lo[1],
+                           sc->body_hi[2] - sc->body_lo[2]};
+    SurfaceDev h{};
+    h.n = 6;
+    for (int f = 0; f < 6; ++f) {
+        const int a = f / 2;
+        const double area = sc->area[f] > 0.0 ? sc->area[f] : ext[(a + 1) % 3] * ext[(a + 2) % 3];
+        ARG(sc->eps_r[f] >= 1.0 && sc->thickness[f] > 0.0, "each face needs eps_r >= 1 and a positive thickness");
+        ARG(sc->shunt_s[f] >= 0.0 && std::isfinite(sc->didv[f]) && std::isfinite(sc->v0[f]), "bad face parameters");
+        h.C[f] = 8.8541878128e-12 * sc->eps_r[f] * area / sc->thickness[f];
+        h.G[f] = sc->shunt_s[f];
+        h.didv[f] = sc->didv[f];
+        h.V[f] = sc->v0[f];
+    }
+    // Dirichlet nodes on the body box's surface, with the faces each lies on
+    const double tol = 1e-9 * std::max(ext[0], std::max(ext[1], ext[2]));
+    std::vector<int32_t> nodes;
+    std::vector<uint8_t> masks;
+    for (int64_t i = 0; i < ctx->hm.N; ++i) {
+        if (!ctx->hm.dirichlet[i]) continue;
+        const double* p = &ctx->hm.xyz[3 * i];
+        bool inside = true;
+        for (int a = 0; a < 3; ++a) inside = inside && p[a] >= sc->body_lo[a] - tol && p[a] <= sc->body_hi[a] + tol;
+        if (!inside) continue;
+        unsigned m = 0;
+        for (int f = 0; f < 6; ++f) {
+            const int a = f / 2;
+            const double plane = (f & 1) ? sc->body_hi[a] : sc->body_lo[a];
+            if (std::fabs(p[a] - plane) <= tol) m |= 1u << f;
+        }
+        if (!m) continue;
+        nodes.push_back((int32_t)i);
+        masks.push_back((uint8_t)m);
+    }
+    ARG(!nodes.empty(), "no Dirichlet node lies on the body box");
+    CK(ctx->surf.alloc(1));
+    CK(cudaMemcpyAsync(ctx->surf.p, &h, sizeof(h), cudaMemcpyHostToDevice, ctx->st));
+    CK(ctx->surf_node.upload(nodes.data(), nodes.size(), ctx->st));
+    CK(ctx->surf_mask.upload(masks.data(), masks.size(), ctx->st));
+    CK(cudaMemsetAsync(ctx->led.p->patch_q, 0, sizeof(ctx->led.p->patch_q) + sizeof(ctx->led.p->patch_n), ctx->st));
+    for (int a = 0; a < 3; ++a) {
+        ctx->body_lo[a] = sc->body_lo[a];
+        ctx->body_hi[a] = sc->body_hi[a];
+    }
+    ctx->surface = true;
+    ctx->prm.body_tally = 1;
+    launch_surface_apply(ctx->surf.p, (int64_t)nodes.size(), ctx->surf_node.p, ctx->surf_mask.p, ctx->phi.p, ctx->st);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(ctx->st));
+    return SCDAT_OK;
+}
+
+SCDAT_API int scdat_get_surface_state(scdat_ctx* ctx, double* V, double* Q, double* I, int64_t* counts)
+{
+    if (!ctx) return SCDAT_ERR_ARG;
+    if (!ctx->surface) {
+        ctx->err = "no surface circuit";
+        return SCDAT_ERR_STATE;
+    }
+    SurfaceDev h{};
+    LedgerDev l{};
+    CK(cudaMemcpyAsync(&h, ctx->surf.p, sizeof(h), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaMemcpyAsync(&l, ctx->led.p, sizeof(l), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    for (int f = 0; f < 6; ++f) {
+        if (V) V[f] = h.V[f];
+        if (Q) Q[f] = h.Q[f];
+        if (I) I[f] = h.I[f];
+        if (counts) counts[f] = (int64_t)l.patch_n[f];
+    }
+    return SCDAT_OK;
+}
+
 SCDAT_API int scdat_set_elastic_mcc(scdat_ctx* ctx, int32_t species, const scdat_elastic* proc)
 {
     if (!ctx) return SCDAT_ERR_ARG;
@@ -975,6 +1072,8 @@ SCDAT_API int scdat_step(scdat_ctx* ctx, int32_t n_steps)
     ARG(n_steps >= 0, "negative step count");
     for (int k = 0; k < n_steps; ++k) {
         int rc = do_push(ctx, true);
+        if (rc) return rc;
+        rc = do_surface(ctx);
         if (rc) return rc;
         rc = do_solve_field(ctx);
         if (rc) return rc;

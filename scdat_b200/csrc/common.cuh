@@ -159,6 +159,10 @@ struct LedgerDev {
     unsigned long long flags;                // device error flag word
     unsigned long long lsq_bad;              // bit 8: the nodal field had a non-finite value
     unsigned long long pad[4];
+    // charge [fixed point lo, hi] and count of particles lost into each face XMin..ZMax of the
+    // body box this step (surface circuit; cleared when the circuit advances)
+    unsigned long long patch_q[6][2];
+    unsigned long long patch_n[6];
 };
 
 enum DeviceFlag : unsigned long long {
@@ -190,6 +194,10 @@ struct PushParams {
     uint64_t seed;
     uint32_t step;
     int32_t deposit;
+    // surface circuit: particles lost into the body box [blo, bhi] are tallied per face
+    int32_t patches;
+    int32_t pad2;
+    double blo[3], bhi[3];
 };
 
 }  // namespace scdat

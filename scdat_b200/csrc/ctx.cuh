@@ -7,6 +7,7 @@
 #include "field.cuh"
 #include "mesh_setup.h"
 #include "push.cuh"
+#include "surface.cuh"
 
 #include <string>
 #include <utility>
@@ -108,6 +109,12 @@ struct scdat_ctx {
     DBuf<int> d1it, d2it;
     DBuf<double> d1rem, d2rem, d1vs, d2vs;
     unsigned dcap = 0;
+    // surface circuit of the body faces (scdat_set_surface_circuit)
+    bool surface = false;
+    double body_lo[3] = {0, 0, 0}, body_hi[3] = {0, 0, 0};
+    DBuf<SurfaceDev> surf;
+    DBuf<int32_t> surf_node;
+    DBuf<uint8_t> surf_mask;
     double uq = 1.0, ue = 1.0;
     int64_t steps = 0;
     double sim_time = 0.0;

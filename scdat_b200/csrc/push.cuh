@@ -250,7 +250,20 @@ static __device__ __noinline__ int resolve_lost(const MeshView& M, const Species
     if (!ok) status = 2;
     if (status == 0 && resolved < 0) status = 2;
     if (status == 2 && pp.body_tally) {
-        if (detect_face(M, px, py, pz, pp.otol, false, 0.0) < 0) ledger_tally(L, 6, S, pp, ke, false);
+        if (detect_face(M, px, py, pz, pp.otol, false, 0.0) < 0) {
+            ledger_tally(L, 6, S, pp, ke, false);
+            if (pp.patches) {
+                // the face of the body box nearest to where the particle left the mesh
+                const double d[6] = {fabs(px - pp.blo[0]), fabs(pp.bhi[0] - px), fabs(py - pp.blo[1]),
+                                     fabs(pp.bhi[1] - py), fabs(pz - pp.blo[2]), fabs(pp.bhi[2] - pz)};
+                int k = 0;
+#pragma unroll
+                for (int f = 1; f < 6; ++f)
+                    if (d[f] < d[k]) k = f;
+                fx_atomic_add(&L->patch_q[k][0], &L->patch_q[k][1], fx_from_double(S.q * S.w * pp.inv_uq));
+                atomicAdd(&L->patch_n[k], 1ull);
+            }
+        }
     }
     if (status == 1) return kTetAbsorbed;
     if (status == 2) return kTetEscaped;

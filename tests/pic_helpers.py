@@ -6,7 +6,9 @@ import numpy as np
 import oracle as O
 
 
-def oracle_cycle(o, mesh, sp, parts, nsteps, dt, face_bc, phi0, neighbors=True, rtol=1e-15, body_tally=False):
+def oracle_cycle(o, mesh, sp, parts, nsteps, dt, face_bc, phi0, neighbors=True, rtol=1e-15, body_tally=False,
+                 surface=None):
+    """surface: an O.SurfaceCircuit advanced after every push (body_tally implied)."""
     A = o.assemble(mesh)
     E = o.lsq(mesh, A, phi0, reg=1e-18)
     L = mesh.xyz.max(axis=0) - mesh.xyz.min(axis=0)
@@ -18,7 +20,14 @@ def oracle_cycle(o, mesh, sp, parts, nsteps, dt, face_bc, phi0, neighbors=True, 
     sc = 0.0
     rho = np.zeros(mesh.N)
     substeps = 0
+    phi_bc = mesh.phi_bc.copy()
+    if surface is not None:
+        body_tally = True
+        phi_bc = surface.apply(phi_bc)
+    lo, hi = mesh.xyz.min(axis=0), mesh.xyz.max(axis=0)
+    otol = max(1e-10, 1e-8 * float(np.max(hi - lo)))
     for _ in range(nsteps):
+        before = st["status"].copy()
         out = o.push(mesh, E, dict(parts, x=st["x"], v=st["v"], tet=st["tet"]), sp, dt, status=st["status"],
                      neighbors=neighbors)
         out = o.boundary(mesh, out, parts, sp, face_bc, period=period, neighbors=neighbors, body_tally=body_tally)
@@ -27,7 +36,15 @@ def oracle_cycle(o, mesh, sp, parts, nsteps, dt, face_bc, phi0, neighbors=True, 
         substeps += out["substeps"]
         st = dict(x=out["x"], v=out["v"], tet=out["tet"], status=out["status"])
         rho = out["rho"]
-        phi, _, _ = o.poisson(mesh, A, rho, mesh.phi_bc, rtol=rtol, phi0=phi)
+        if surface is not None:
+            # particles that left the mesh this step inside the domain box went into the body
+            x = out["x"]
+            into = (before == O.ACTIVE) & (out["status"] == O.ESCAPED) & np.all((x >= lo - otol) & (x <= hi + otol),
+                                                                                axis=1)
+            qw = np.array([sp[s].q * sp[s].w for s in parts["species"][into]])
+            surface.advance(surface.collect(x[into], qw), dt)
+            phi_bc = surface.apply(phi_bc)
+        phi, _, _ = o.poisson(mesh, A, rho, phi_bc, rtol=rtol, phi0=phi)
         E = o.lsq(mesh, A, phi)
     return dict(st, rho=rho, phi=phi, E=E, ledger=ledger, surface_charge=sc, substeps=substeps)
 

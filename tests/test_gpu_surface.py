@@ -1,0 +1,97 @@
+"""Surface circuit of the body (floating dielectric faces) on the device against the oracle.
+
+Charge of the particles lost into the body is tallied per face, advanced into FP64 face
+potentials by the reference's implicit node update, and given to the body's surface nodes
+before each field solve."""
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import rel_err
+from pic_helpers import gpu_domain, gpu_load_particles, gpu_state, oracle_cycle
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-12
+
+
+def _case():
+    n, h = (6, 6, 6), 0.05
+    mesh = O.kuhn_box(n, h, body=((2, 4), (2, 4), (2, 4)), bias=-5.0)
+    sp = O.plasma_species(3e10, 2.0, 1.0, h, 6)
+    parts = O.seed_particles(mesh, sp, 6, 21)
+    return mesh, sp, parts, (0.1, 0.1, 0.1), (0.2, 0.2, 0.2)
+
+
+def test_surface_circuit_matches_oracle(lib, orc):
+    mesh, sp, parts, blo, bhi = _case()
+    dt, nsteps, face_bc = 2e-8, 3, (1,) * 6
+    kw = dict(eps_r=[3.0, 3.0, 2.0, 4.0, 3.0, 3.0], thickness=1e-3, v0=-5.0, shunt=[0, 0, 0, 0, 1e-9, 0],
+              didv=[0, 1e-10, 0, 0, 0, 0])
+    circ = O.SurfaceCircuit(mesh, blo, bhi, **kw)
+    ref = oracle_cycle(orc, mesh, sp, parts, nsteps, dt, face_bc, mesh.phi_bc, surface=circ)
+    dom = gpu_domain(mesh, dt, face_bc=face_bc, pcg_rtol=1e-15, pcg_max_iter=20000)
+    gpu_load_particles(dom, sp, parts)
+    dom.set_surface_circuit(blo, bhi, **kw)
+    dom.set_potential(mesh.phi_bc)
+    for _ in range(nsteps):
+        dom.step(1)
+    got = dom.surface_state()
+    st = gpu_state(dom, len(sp), len(parts["tet"]))
+    rho, phi, E = dom.fields()
+    dom.close()
+    assert np.abs(circ.Q).max() > 0, "the case must collect charge"
+    np.testing.assert_allclose(got["Q"], circ.Q, rtol=TOL, atol=1e-30)
+    np.testing.assert_allclose(got["V"], circ.V, rtol=TOL, atol=1e-12)
+    assert np.array_equal(st["status"], ref["status"])
+    act = st["status"] == O.ACTIVE
+    assert np.abs(st["x"][act] - ref["x"][act]).max() <= TOL * np.abs(ref["x"]).max()
+    assert rel_err(phi, ref["phi"]) < TOL
+    assert rel_err(rho, ref["rho"]) < TOL
+
+
+def test_floating_faces_charge_and_conserve(lib):
+    """Mixed form: with no shunt and no linearisation each face potential moves by exactly its
+    collected charge over its capacitance, the faces' charges add up to the body tally, and an
+    electron-dominated current drives the faces negative."""
+    mesh, sp, parts, blo, bhi = _case()
+    dom = gpu_domain(mesh, 2e-8, face_bc=(1,) * 6, precision=1, pcg_rtol=1e-10)
+    gpu_load_particles(dom, sp, parts)
+    dom.set_surface_circuit(blo, bhi, eps_r=3.0, thickness=1e-3, v0=0.0)
+    dom.set_potential(np.where(mesh.dirichlet == 1, 0.0, 0.0))
+    dom.step(10)
+    s = dom.surface_state()
+    led = dom.ledger()
+    dom.close()
+    circ = O.SurfaceCircuit(mesh, blo, bhi, eps_r=3.0, thickness=1e-3)
+    np.testing.assert_allclose(s["V"], s["Q"] / circ.C, rtol=1e-12, atol=0)
+    np.testing.assert_allclose(s["Q"].sum(), led[6, 0] + led[6, 1], rtol=1e-12)
+    assert s["counts"].sum() == led[6, 4] + led[6, 5]
+    assert s["V"].mean() < 0.0
+
+
+def test_surface_in_batch_matches_single(lib):
+    from scdat_b200 import capi
+
+    mesh, sp, parts, blo, bhi = _case()
+
+    def make():
+        dom = gpu_domain(mesh, 2e-8, face_bc=(1,) * 6, precision=1, pcg_rtol=1e-10)
+        gpu_load_particles(dom, sp, parts)
+        dom.set_surface_circuit(blo, bhi, eps_r=3.0, thickness=1e-3, v0=-1.0)
+        dom.set_potential(mesh.phi_bc)
+        return dom
+
+    dom = make()
+    dom.step(4)
+    ref = dom.surface_state(), dom.fields()[1]
+    dom.close()
+    dom = make()
+    b = capi.Batch([dom])
+    try:
+        b.step(4)
+        got = dom.surface_state(), dom.fields()[1]
+    finally:
+        b.close()
+        dom.close()
+    assert np.array_equal(got[0]["V"], ref[0]["V"]) and np.array_equal(got[0]["Q"], ref[0]["Q"])
+    assert np.array_equal(got[1], ref[1])
