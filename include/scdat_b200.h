@@ -205,6 +205,13 @@ typedef struct {
     double didv[6];        /* plasma current linearisation dI/dV, A/V (0 = plain charge integration) */
 } scdat_surface_circuit;
 SCDAT_API int scdat_set_surface_circuit(scdat_ctx* ctx, const scdat_surface_circuit* sc);
+/* Secondary emission of electrons collected by the body (needs the surface circuit):
+ * model 1 is Sternglass's universal yield 7.4 dmax (E/Emax) exp(-2 sqrt(E/Emax)), model 2 the
+ * reference's legacyWhippleYield (Tools/Material/src/SurfaceMaterialModel.cpp:231-244), 0 off.
+ * The emitted charge delta |q| w of each collected electron returns to its face as current and
+ * is recorded in ledger row 6 as emitted electron charge (no secondary macro-particles are
+ * created). */
+SCDAT_API int scdat_set_secondary_emission(scdat_ctx* ctx, int32_t model, double delta_max, double e_max_ev);
 /* Face potentials [6], collected charge [6], last-step current [6] and the number of particles
  * collected so far [6]; any pointer may be NULL. */
 SCDAT_API int scdat_get_surface_state(scdat_ctx* ctx, double* V, double* Q, double* I, int64_t* counts);
@@ -275,6 +282,27 @@ SCDAT_API int scdat_batch_last_step_ms(const scdat_batch* b, double* ms);
 SCDAT_API int scdat_batch_stream(const scdat_batch* b, void** stream);
 /* Kernels of this library the batch's steps have launched so far. */
 SCDAT_API int scdat_batch_kernel_launches(scdat_batch* b, int64_t* launches);
+
+/* PicMccSurfaceCurrentSampler::sampleWithDerivative (Toolkit/Surface Charging/src/
+ * PicMccSurfaceCurrentSampler.cpp:641-670): three contexts holding the same scenario (mesh,
+ * species, particles, seed) run window_steps steps with the body nodes held at V - d, V and
+ * V + d, d = max(0.1, |probe_delta_v|) as in the reference, as one batch when all three are
+ * mixed-precision (one at a time otherwise).  Returns the centre window's collection current
+ * densities (charge per second per area into the body: electrons negative, ions positive,
+ * secondaries leaving positive) and the central difference of the net density over 2d. */
+typedef struct {
+    double surface_potential_v;
+    double electron_collection_a_per_m2;
+    double ion_collection_a_per_m2;
+    double emitted_electron_a_per_m2;
+    double net_collection_a_per_m2;
+    double current_derivative_a_per_m2_per_v;
+    int32_t valid;
+    int32_t window_steps;
+} scdat_current_sample;
+SCDAT_API int scdat_sample_with_derivative(scdat_ctx* const* ctx3, int64_t n_body, const int64_t* body_nodes,
+                                           double surface_potential_v, double probe_delta_v, int32_t window_steps,
+                                           double area_m2, scdat_current_sample* out);
 
 /* The CUDA stream every call of this context runs on (a cudaStream_t), for callers that
  * order their own work or events against the library.  No reference counterpart. */

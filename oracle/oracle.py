@@ -522,6 +522,24 @@ def body_face_of(x, blo, bhi):
     return np.argmin(d, axis=1)
 
 
+def see_yield(model, dmax, emax, e_ev):
+    """Secondary-electron yield: 1 Sternglass 7.4 dmax (E/Emax) exp(-2 sqrt(E/Emax)); 2 the
+    reference's legacyWhippleYield (Tools/Material/src/SurfaceMaterialModel.cpp:231-244)."""
+    e = np.asarray(e_ev, float)
+    out = np.zeros_like(e)
+    ok = (e > 0) & (dmax > 0)
+    if model == 1:
+        r = e[ok] / emax
+        out[ok] = 7.4 * dmax * r * np.exp(-2.0 * np.sqrt(r))
+    elif model == 2:
+        ep = max(1.0, emax)
+        q = 2.28 * (e[ok] / ep) ** 1.35
+        v = np.where(q > 1e-12, 2.228 * (q - 1.0 + np.exp(-q)) / np.where(q > 1e-12, q, 1.0) * dmax
+                     * (ep / e[ok]) ** 0.35, 0.0)
+        out[ok] = v
+    return out
+
+
 class SurfaceCircuit:
     """Faces of the body box as circuit nodes, C = eps0 eps_r A / d
     (DensePlasmaSurfaceCharging.cpp:6544-6552), advanced per step by the implicit node update
@@ -547,12 +565,21 @@ class SurfaceCircuit:
         self.nodes = np.nonzero(masks)[0]
         self.masks = masks[self.nodes]
 
-    def collect(self, x_lost, q_lost):
-        """Charge of this step's particles lost into the body, per face."""
+    see = (0, 0.0, 300.0)  # (model, delta_max, e_max_ev)
+
+    def collect(self, x_lost, q_lost, e_ev=None, electron=None):
+        """Charge of this step's particles lost into the body per face, plus the charge their
+        secondaries leave behind; also returns the emitted electrons' charge (negative)."""
         dq = np.zeros(6)
+        emitted = 0.0
         if len(q_lost):
-            np.add.at(dq, body_face_of(x_lost, self.blo, self.bhi), q_lost)
-        return dq
+            face = body_face_of(x_lost, self.blo, self.bhi)
+            np.add.at(dq, face, q_lost)
+            if self.see[0] and e_ev is not None:
+                em = see_yield(self.see[0], self.see[1], self.see[2], e_ev) * np.abs(q_lost) * electron
+                np.add.at(dq, face, em)
+                emitted = -float(em.sum())
+        return dq, emitted
 
     def advance(self, dq, dt):
         self.Q += dq

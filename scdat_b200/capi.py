@@ -54,6 +54,13 @@ class SurfaceCircuitC(C.Structure):
                 ("shunt_s", C.c_double * 6), ("didv", C.c_double * 6)]
 
 
+class CurrentSampleC(C.Structure):
+    _fields_ = [("surface_potential_v", C.c_double), ("electron_collection_a_per_m2", C.c_double),
+                ("ion_collection_a_per_m2", C.c_double), ("emitted_electron_a_per_m2", C.c_double),
+                ("net_collection_a_per_m2", C.c_double), ("current_derivative_a_per_m2_per_v", C.c_double),
+                ("valid", C.c_int32), ("window_steps", C.c_int32)]
+
+
 class StatsC(C.Structure):
     _fields_ = [("completed_steps", C.c_int64), ("simulation_time", C.c_double), ("total_charge", C.c_double),
                 ("total_energy", C.c_double), ("active_particles", C.c_int64), ("stored_particles", C.c_int64),
@@ -73,7 +80,8 @@ EXPORTS = ["scdat_default_params", "scdat_create", "scdat_destroy", "scdat_last_
            "scdat_batch_default_tuning", "scdat_batch_create", "scdat_batch_destroy", "scdat_batch_last_error",
            "scdat_batch_step", "scdat_batch_set_tuning", "scdat_batch_get_tuning", "scdat_batch_autotune",
            "scdat_batch_last_step_ms", "scdat_batch_stream", "scdat_batch_kernel_launches",
-           "scdat_set_surface_circuit", "scdat_get_surface_state"]
+           "scdat_set_surface_circuit", "scdat_get_surface_state", "scdat_set_secondary_emission",
+           "scdat_sample_with_derivative"]
 
 _LIB = None
 
@@ -111,6 +119,9 @@ def load():
     L.scdat_batch_stream.argtypes = [vp, C.POINTER(vp)]
     L.scdat_set_surface_circuit.argtypes = [vp, C.POINTER(SurfaceCircuitC)]
     L.scdat_get_surface_state.argtypes = [vp, vp, vp, vp, vp]
+    L.scdat_set_secondary_emission.argtypes = [vp, C.c_int32, C.c_double, C.c_double]
+    L.scdat_sample_with_derivative.argtypes = [C.POINTER(vp), C.c_int64, vp, C.c_double, C.c_double, C.c_int32,
+                                               C.c_double, C.POINTER(CurrentSampleC)]
     L.scdat_batch_kernel_launches.argtypes = [vp, C.POINTER(C.c_int64)]
     L.scdat_set_particles.argtypes = [vp, C.c_int32, C.c_int64, vp, vp, vp, vp]
     L.scdat_seed_box_particles.argtypes = [vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_double, vp, vp,
@@ -308,6 +319,10 @@ class Domain:
                 getattr(sc, name)[f] = float(arr[f])
         self._ck(self.L.scdat_set_surface_circuit(self.h, C.byref(sc)))
 
+    def set_secondary_emission(self, model, delta_max=2.0, e_max_ev=300.0):
+        """model: 0 off, 1 Sternglass, 2 Whipple (the reference's legacy form)."""
+        self._ck(self.L.scdat_set_secondary_emission(self.h, int(model), float(delta_max), float(e_max_ev)))
+
     def surface_state(self):
         V, Q, I = np.zeros(6), np.zeros(6), np.zeros(6)
         n = np.zeros(6, np.int64)
@@ -448,3 +463,17 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+def sample_with_derivative(domains, body_nodes, surface_potential_v, probe_delta_v, window_steps, area_m2):
+    """scdat_sample_with_derivative over three Domains holding the same scenario."""
+    L = load()
+    arr = (C.c_void_p * 3)(*[d.h for d in domains])
+    nodes = np.ascontiguousarray(body_nodes, np.int64)
+    out = CurrentSampleC()
+    rc = L.scdat_sample_with_derivative(arr, nodes.shape[0], _p(nodes), float(surface_potential_v),
+                                        float(probe_delta_v), int(window_steps), float(area_m2), C.byref(out))
+    if rc != 0:
+        raise ScdatError(rc, L.scdat_last_error(domains[1].h).decode())
+    return {k: getattr(out, k) for k, _ in CurrentSampleC._fields_}
+

@@ -142,6 +142,9 @@ PushParams push_params(const scdat_ctx* ctx, bool do_mcc)
     pp.step = (uint32_t)ctx->steps;
     pp.deposit = 1;
     pp.patches = ctx->surface ? 1 : 0;
+    pp.see_model = ctx->see_model;
+    pp.see_dmax = ctx->see_dmax;
+    pp.see_emax_ev = ctx->see_emax;
     for (int a = 0; a < 3; ++a) {
         pp.blo[a] = ctx->body_lo[a];
         pp.bhi[a] = ctx->body_hi[a];
@@ -988,6 +991,17 @@ SCDAT_API int scdat_set_surface_circuit(scdat_ctx* ctx, const scdat_surface_circ
     return SCDAT_OK;
 }
 
+SCDAT_API int scdat_set_secondary_emission(scdat_ctx* ctx, int32_t model, double delta_max, double e_max_ev)
+{
+    if (!ctx) return SCDAT_ERR_ARG;
+    ARG(model >= 0 && model <= 2, "model: 0 off, 1 Sternglass, 2 Whipple");
+    ARG(model == 0 || (delta_max >= 0.0 && e_max_ev > 0.0), "yield needs delta_max >= 0 and e_max > 0");
+    ctx->see_model = model;
+    ctx->see_dmax = delta_max;
+    ctx->see_emax = e_max_ev;
+    return SCDAT_OK;
+}
+
 SCDAT_API int scdat_get_surface_state(scdat_ctx* ctx, double* V, double* Q, double* I, int64_t* counts)
 {
     if (!ctx) return SCDAT_ERR_ARG;
@@ -1112,6 +1126,65 @@ SCDAT_API int scdat_get_species_charge(scdat_ctx* ctx, int32_t species, double* 
     return SCDAT_OK;
 }
 
+SCDAT_API int scdat_sample_with_derivative(scdat_ctx* const* c3, int64_t n_body, const int64_t* body_nodes,
+                                           double v, double probe_delta_v, int32_t window_steps, double area_m2,
+                                           scdat_current_sample* out)
+{
+    if (!c3 || !out || !c3[0] || !c3[1] || !c3[2]) return SCDAT_ERR_ARG;
+    scdat_ctx* ctx = c3[1];
+    ARG(n_body > 0 && body_nodes && window_steps > 0 && area_m2 > 0.0, "need body nodes, a window and an area");
+    std::memset(out, 0, sizeof(*out));
+    const double d = std::max(0.1, std::fabs(probe_delta_v));
+    const double pot[3] = {v - d, v, v + d};
+    double before[3][8], after[3][8];
+    std::vector<double> vals((size_t)n_body);
+    for (int k = 0; k < 3; ++k) {
+        std::fill(vals.begin(), vals.end(), pot[k]);
+        int rc = scdat_set_node_potentials(c3[k], n_body, body_nodes, vals.data());
+        if (rc) return rc;
+        double led[7 * 8];
+        rc = scdat_get_ledger(c3[k], led);
+        if (rc) return rc;
+        std::memcpy(before[k], led + 8 * 6, sizeof(before[k]));
+    }
+    const bool mixed = c3[0]->mixed && c3[1]->mixed && c3[2]->mixed;
+    if (mixed) {
+        scdat_batch* b = nullptr;
+        int rc = scdat_batch_create(3, c3, &b);
+        if (!rc) rc = scdat_batch_step(b, window_steps);
+        if (rc) ctx->err = b ? scdat_batch_last_error(b) : "batch failed";
+        scdat_batch_destroy(b);
+        if (rc) return rc;
+    } else {
+        for (int k = 0; k < 3; ++k) {
+            int rc = scdat_step(c3[k], window_steps);
+            if (rc) return rc;
+        }
+    }
+    double net[3];
+    for (int k = 0; k < 3; ++k) {
+        double led[7 * 8];
+        int rc = scdat_get_ledger(c3[k], led);
+        if (rc) return rc;
+        std::memcpy(after[k], led + 8 * 6, sizeof(after[k]));
+        const double span = window_steps * c3[k]->prm.dt * area_m2;
+        const double je = (after[k][0] - before[k][0]) / span, ji = (after[k][1] - before[k][1]) / span,
+                     jm = -(after[k][2] - before[k][2]) / span;
+        net[k] = je + ji + jm;
+        if (k == 1) {
+            out->electron_collection_a_per_m2 = je;
+            out->ion_collection_a_per_m2 = ji;
+            out->emitted_electron_a_per_m2 = jm;
+        }
+    }
+    out->surface_potential_v = v;
+    out->net_collection_a_per_m2 = net[1];
+    out->current_derivative_a_per_m2_per_v = (net[2] - net[0]) / (2.0 * d);
+    out->valid = 1;
+    out->window_steps = window_steps;
+    return SCDAT_OK;
+}
+
 SCDAT_API int scdat_get_ledger(scdat_ctx* ctx, double* ledger)
 {
     if (!ctx || !ledger) return SCDAT_ERR_ARG;
@@ -1122,7 +1195,7 @@ SCDAT_API int scdat_get_ledger(scdat_ctx* ctx, double* ledger)
         double* r = ledger + 8 * f;
         r[0] = fx_to_double(h.row[f][0], (long long)h.row[f][1], ctx->uq);
         r[1] = fx_to_double(h.row[f][2], (long long)h.row[f][3], ctx->uq);
-        r[2] = 0.0;
+        r[2] = fx_to_double(h.emit_q[f][0], (long long)h.emit_q[f][1], ctx->uq);
         r[3] = fx_to_double(h.row[f][4], (long long)h.row[f][5], ctx->ue);
         r[4] = (double)h.row[f][6];
         r[5] = (double)h.row[f][7];
@@ -1136,6 +1209,7 @@ SCDAT_API int scdat_reset_ledger(scdat_ctx* ctx)
 {
     if (!ctx) return SCDAT_ERR_ARG;
     CK(cudaMemsetAsync(ctx->led.p->row, 0, sizeof(ctx->led.p->row), ctx->st));
+    CK(cudaMemsetAsync(ctx->led.p->emit_q, 0, sizeof(ctx->led.p->emit_q), ctx->st));
     CK(cudaMemsetAsync(&ctx->led.p->surf_lo, 0, 2 * sizeof(unsigned long long), ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
     return SCDAT_OK;

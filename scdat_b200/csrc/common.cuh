@@ -163,6 +163,8 @@ struct LedgerDev {
     // body box this step (surface circuit; cleared when the circuit advances)
     unsigned long long patch_q[6][2];
     unsigned long long patch_n[6];
+    // charge of the secondary electrons emitted per ledger row (fixed point lo, hi)
+    unsigned long long emit_q[7][2];
 };
 
 enum DeviceFlag : unsigned long long {
@@ -196,8 +198,10 @@ struct PushParams {
     int32_t deposit;
     // surface circuit: particles lost into the body box [blo, bhi] are tallied per face
     int32_t patches;
-    int32_t pad2;
+    int32_t see_model;       // secondary emission of electrons collected by the body: 0 off,
+                             // 1 Sternglass, 2 Whipple (legacyWhippleYield)
     double blo[3], bhi[3];
+    double see_dmax, see_emax_ev;
 };
 
 }  // namespace scdat

@@ -111,6 +111,8 @@ struct scdat_ctx {
     unsigned dcap = 0;
     // surface circuit of the body faces (scdat_set_surface_circuit)
     bool surface = false;
+    int see_model = 0;
+    double see_dmax = 0.0, see_emax = 300.0;
     double body_lo[3] = {0, 0, 0}, body_hi[3] = {0, 0, 0};
     DBuf<SurfaceDev> surf;
     DBuf<int32_t> surf_node;

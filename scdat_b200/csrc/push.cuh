@@ -199,6 +199,24 @@ __device__ inline void ledger_tally(LedgerDev* L, int row, const SpeciesDev& S, 
     if (surface) fx_atomic_add(&L->surf_lo, &L->surf_hi, fq);
 }
 
+constexpr double kElementaryCharge = 1.602176634e-19;
+
+// Secondary-electron yield at incident energy e_ev.  Sternglass's universal curve
+// delta = 7.4 dmax (E/Emax) exp(-2 sqrt(E/Emax)) (peak dmax at Emax); or the reference's
+// Whipple form, legacyWhippleYield (Tools/Material/src/SurfaceMaterialModel.cpp:231-244).
+__device__ inline double see_yield(const PushParams& pp, double e_ev)
+{
+    if (!(e_ev > 0.0) || !(pp.see_dmax > 0.0)) return 0.0;
+    if (pp.see_model == 1) {
+        const double r = e_ev / pp.see_emax_ev;
+        return 7.4 * pp.see_dmax * r * exp(-2.0 * sqrt(r));
+    }
+    const double ep = fmax(1.0, pp.see_emax_ev);
+    const double q = 2.28 * pow(e_ev / ep, 1.35);
+    if (q <= 1.0e-12) return 0.0;
+    return 2.228 * (q - 1.0 + exp(-q)) / q * pp.see_dmax * pow(ep / e_ev, 0.35);
+}
+
 // PICCycle::applyRuntimeBoundaryCondition + processRuntimeBoundaryEvents for one lost
 // particle (PICCycle.cpp:1221-1379).  Updates position (periodic wrap) and returns the new
 // tet code (>= 0 active, kTetAbsorbed, kTetEscaped).
@@ -262,6 +280,14 @@ static __device__ __noinline__ int resolve_lost(const MeshView& M, const Species
                     if (d[f] < d[k]) k = f;
                 fx_atomic_add(&L->patch_q[k][0], &L->patch_q[k][1], fx_from_double(S.q * S.w * pp.inv_uq));
                 atomicAdd(&L->patch_n[k], 1ull);
+                // secondaries leave the face: it gains delta |q| w, the ledger records their charge
+                if (pp.see_model && S.electron_like) {
+                    const double emitted = see_yield(pp, ke / kElementaryCharge) * fabs(S.q) * S.w;
+                    if (emitted > 0.0) {
+                        fx_atomic_add(&L->patch_q[k][0], &L->patch_q[k][1], fx_from_double(emitted * pp.inv_uq));
+                        fx_atomic_add(&L->emit_q[6][0], &L->emit_q[6][1], fx_from_double(-emitted * pp.inv_uq));
+                    }
+                }
             }
         }
     }

@@ -41,8 +41,14 @@ def oracle_cycle(o, mesh, sp, parts, nsteps, dt, face_bc, phi0, neighbors=True, 
             x = out["x"]
             into = (before == O.ACTIVE) & (out["status"] == O.ESCAPED) & np.all((x >= lo - otol) & (x <= hi + otol),
                                                                                 axis=1)
-            qw = np.array([sp[s].q * sp[s].w for s in parts["species"][into]])
-            surface.advance(surface.collect(x[into], qw), dt)
+            spi = parts["species"][into]
+            qw = np.array([sp[s].q * sp[s].w for s in spi])
+            m = np.array([sp[s].m for s in spi])
+            ke = 0.5 * m * np.sum(out["v"][into] ** 2, axis=1) if len(spi) else np.zeros(0)
+            ele = np.array([1.0 if sp[s].kind == 0 else 0.0 for s in spi])
+            dq, emitted = surface.collect(x[into], qw, ke / O.QE, ele)
+            ledger[6, 2] += emitted
+            surface.advance(dq, dt)
             phi_bc = surface.apply(phi_bc)
         phi, _, _ = o.poisson(mesh, A, rho, phi_bc, rtol=rtol, phi0=phi)
         E = o.lsq(mesh, A, phi)
