@@ -304,6 +304,37 @@ SCDAT_API int scdat_sample_with_derivative(scdat_ctx* const* ctx3, int64_t n_bod
                                            double surface_potential_v, double probe_delta_v, int32_t window_steps,
                                            double area_m2, scdat_current_sample* out);
 
+/* ---- Adjoint window (no reference counterpart) ----
+ * Runs `steps` FP64 steps from the current state (which must follow a scdat_solve_field; MCC
+ * off, segment-cloud or nearest-point deposit) with states checkpointed every `checkpoint`
+ * steps, then the hand-written reverse pass, and returns
+ *     J = g_phi . phi_T + g_V . V_T + g_Q . Q_T
+ * (final potential; surface-circuit face potentials and collected charge) with its pathwise
+ * derivatives in the body bias (the Dirichlet value of bias_nodes, or the faces' initial
+ * potential when the surface circuit is on), the electron temperature the particles were
+ * seeded at (velocities scale with sqrt(Te)) and the secondary-yield peak.  The discrete
+ * choices of the forward run (tets, sub-step expressions, deposit points inside the post-move
+ * tet, collections) are held fixed, so a finite difference with frozen random streams agrees
+ * while it flips none of them.  The context ends at step T, as after scdat_step(steps). */
+typedef struct {
+    int32_t steps;
+    int32_t checkpoint;          /* default 10 */
+    const double* g_phi;         /* [n_nodes] or NULL */
+    double g_V[6];
+    double g_Q[6];
+    const int64_t* bias_nodes;   /* nodes held at the bias (no surface circuit) */
+    int64_t n_bias_nodes;
+    double te_ev;                /* electron temperature of the seeded velocities (0: skip dJ/dTe) */
+} scdat_adjoint_request;
+typedef struct {
+    double J;
+    double dJ_dbias;
+    double dJ_dte;
+    double dJ_ddelta_max;
+    int64_t flags;  /* 1: a particle's sub-steps overflowed the replay tape, 2: replay mismatch */
+} scdat_adjoint_result;
+SCDAT_API int scdat_adjoint_window(scdat_ctx* ctx, const scdat_adjoint_request* rq, scdat_adjoint_result* res);
+
 /* The CUDA stream every call of this context runs on (a cudaStream_t), for callers that
  * order their own work or events against the library.  No reference counterpart. */
 SCDAT_API void* scdat_stream(scdat_ctx* ctx);

@@ -24,7 +24,7 @@ HOST_DIR = os.path.join(HERE, "host")
 HOST_LIB = os.path.join(HERE, "libscdat_host.so")
 
 SOURCES = ["capi.cu", "push_f64.cu", "push_mixed.cu", "field.cu", "utils.cu", "pcg_csr.cu", "pcg_noalloc.cu",
-           "batch_field.cu", "batch_host.cu", "surface.cu", "mesh_setup.cpp"]
+           "batch_field.cu", "batch_host.cu", "surface.cu", "adjoint.cu", "mesh_setup.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
          "--expt-relaxed-constexpr", f"-I{os.path.join(ROOT, 'include')}"]

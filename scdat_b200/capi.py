@@ -61,6 +61,16 @@ class CurrentSampleC(C.Structure):
                 ("valid", C.c_int32), ("window_steps", C.c_int32)]
 
 
+class AdjointRequestC(C.Structure):
+    _fields_ = [("steps", C.c_int32), ("checkpoint", C.c_int32), ("g_phi", C.c_void_p), ("g_V", C.c_double * 6),
+                ("g_Q", C.c_double * 6), ("bias_nodes", C.c_void_p), ("n_bias_nodes", C.c_int64), ("te_ev", C.c_double)]
+
+
+class AdjointResultC(C.Structure):
+    _fields_ = [("J", C.c_double), ("dJ_dbias", C.c_double), ("dJ_dte", C.c_double), ("dJ_ddelta_max", C.c_double),
+                ("flags", C.c_int64)]
+
+
 class StatsC(C.Structure):
     _fields_ = [("completed_steps", C.c_int64), ("simulation_time", C.c_double), ("total_charge", C.c_double),
                 ("total_energy", C.c_double), ("active_particles", C.c_int64), ("stored_particles", C.c_int64),
@@ -81,7 +91,7 @@ EXPORTS = ["scdat_default_params", "scdat_create", "scdat_destroy", "scdat_last_
            "scdat_batch_step", "scdat_batch_set_tuning", "scdat_batch_get_tuning", "scdat_batch_autotune",
            "scdat_batch_last_step_ms", "scdat_batch_stream", "scdat_batch_kernel_launches",
            "scdat_set_surface_circuit", "scdat_get_surface_state", "scdat_set_secondary_emission",
-           "scdat_sample_with_derivative"]
+           "scdat_sample_with_derivative", "scdat_adjoint_window"]
 
 _LIB = None
 
@@ -120,6 +130,7 @@ def load():
     L.scdat_set_surface_circuit.argtypes = [vp, C.POINTER(SurfaceCircuitC)]
     L.scdat_get_surface_state.argtypes = [vp, vp, vp, vp, vp]
     L.scdat_set_secondary_emission.argtypes = [vp, C.c_int32, C.c_double, C.c_double]
+    L.scdat_adjoint_window.argtypes = [vp, C.POINTER(AdjointRequestC), C.POINTER(AdjointResultC)]
     L.scdat_sample_with_derivative.argtypes = [C.POINTER(vp), C.c_int64, vp, C.c_double, C.c_double, C.c_int32,
                                                C.c_double, C.POINTER(CurrentSampleC)]
     L.scdat_batch_kernel_launches.argtypes = [vp, C.POINTER(C.c_int64)]
@@ -328,6 +339,24 @@ class Domain:
         n = np.zeros(6, np.int64)
         self._ck(self.L.scdat_get_surface_state(self.h, _p(V), _p(Q), _p(I), _p(n)))
         return dict(V=V, Q=Q, I=I, counts=n)
+
+    def adjoint_window(self, steps, checkpoint=10, g_phi=None, g_V=(0.0,) * 6, g_Q=(0.0,) * 6, bias_nodes=None,
+                       te_ev=0.0):
+        """scdat_adjoint_window: J and dJ/d(bias, Te, delta_max) over `steps` FP64 steps."""
+        rq = AdjointRequestC()
+        rq.steps, rq.checkpoint = int(steps), int(checkpoint)
+        gp = None if g_phi is None else np.ascontiguousarray(g_phi, np.float64)
+        bn = None if bias_nodes is None else np.ascontiguousarray(bias_nodes, np.int64)
+        rq.g_phi = None if gp is None else gp.ctypes.data
+        for f in range(6):
+            rq.g_V[f] = float(g_V[f])
+            rq.g_Q[f] = float(g_Q[f])
+        rq.bias_nodes = None if bn is None else bn.ctypes.data
+        rq.n_bias_nodes = 0 if bn is None else bn.shape[0]
+        rq.te_ev = float(te_ev)
+        res = AdjointResultC()
+        self._ck(self.L.scdat_adjoint_window(self.h, C.byref(rq), C.byref(res)))
+        return dict(J=res.J, dbias=res.dJ_dbias, dte=res.dJ_dte, ddelta=res.dJ_ddelta_max, flags=res.flags)
 
     def set_elastic(self, s, n_target, sigma, mode=0, alpha=0.0, e_ref=1.0, e_th=0.0, enabled=True):
         proc = ElasticC(n_target, sigma, e_ref, alpha, e_th, 1 if enabled else 0, mode)

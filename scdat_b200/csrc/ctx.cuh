@@ -141,4 +141,10 @@ SpeciesDev species_dev(const scdat_ctx* ctx, int s);
 PushParams push_params(const scdat_ctx* ctx, bool do_mcc);
 int check_flags(scdat_ctx* ctx);
 int do_sort(scdat_ctx* ctx, int s);
+int do_push(scdat_ctx* ctx, bool do_mcc);
+int do_surface(scdat_ctx* ctx);
+int do_solve_field(scdat_ctx* ctx);
+int do_lsq(scdat_ctx* ctx, double reg);
+int refresh_tet_field(scdat_ctx* ctx);
+int run_pcg64(scdat_ctx* ctx, const double* bvec, double* xvec, double rtol, int max_iter, int& iters, double& relres);
 }  // namespace scdat
