@@ -17,6 +17,11 @@ Workloads (all synthetic, seeded; the reference publishes no dataset):
                 Ti log-uniform in 0.1..10 eV, 8..64 ppc per species, dt = 0.1 / omega_pe;
                 mixed form, timed against the plain FP64 form of the same scenarios run one at
                 a time
+  surface256    256 x 256 x 128 cells of one Debye length (50M tets), a 32 x 32 x 16-cell body
+                whose 6 faces are floating dielectric patches (eps_r 3, 1 mm) integrating their
+                collected charge into FP64 potentials, n = 1e9 m^-3, Te = Ti = 5 eV, 16 ppc,
+                dt = 0.1 / omega_pe; mixed form, with the FP64 form's face potentials after the
+                same steps as the error reference
 Every rank runs an independent replica ("replicas only": the path has no exchange step).
 """
 from __future__ import annotations
@@ -43,6 +48,8 @@ CONFIGS = {
     "plain32": dict(n=32, L=1.6, body=(12, 20), bias=-10.0, ppc=20, dt=2e-8, precision=0, rtol=1e-8, density=1e10,
                     te=1.0, ti=1.0, sort_interval=8),
     "batched64": dict(scenarios=64, seed=2026, precision=1, rtol=1e-10, sort_interval=4),
+    "surface256": dict(cells=(256, 256, 128), body=((112, 144), (112, 144), (56, 72)), ppc=16, density=1e9, te=5.0,
+                       ti=5.0, precision=1, rtol=1e-10, sort_interval=4, eps_r=3.0, thickness=1e-3),
 }
 EPS0 = 8.8541878128e-12
 
@@ -416,6 +423,109 @@ def run_batched(args, cfg):
         print(json.dumps(out))
 
 
+def build_surface_domain(cfg, precision, capi):
+    nx, ny, nz = cfg["cells"]
+    h = float(np.sqrt(EPS0 * cfg["te"] / (cfg["density"] * QE)))
+    dt = 0.1 / float(np.sqrt(cfg["density"] * QE * QE / (EPS0 * ME)))
+    body = cfg["body"]
+    m = capi.kuhn_box_mesh((nx, ny, nz), h, body=body, bias=0.0, wall=0.0)
+    dom = capi.Domain(m["xyz"], m["tet"], m["dirichlet"], dt, precision=precision, face_bc=(1,) * 6,
+                      pcg_rtol=cfg["rtol"], pcg_max_iter=20000, sort_interval=cfg["sort_interval"])
+
+    class Sp:
+        def __init__(self, q, mass, w):
+            self.q, self.m, self.w = q, mass, w
+
+    w = cfg["density"] * h ** 3 / cfg["ppc"]
+    dom.set_species([Sp(-QE, ME, w), Sp(QE, MP, w)])
+    dom.seed_box(0, (nx, ny, nz), h, body, cfg["ppc"], cfg["te"], 4242)
+    dom.seed_box(1, (nx, ny, nz), h, body, cfg["ppc"], cfg["ti"], 4242)
+    dom.set_potential(m["phi"])
+    dom.set_surface_circuit(tuple(b[0] * h for b in body), tuple(b[1] * h for b in body), eps_r=cfg["eps_r"],
+                            thickness=cfg["thickness"], v0=0.0)
+    dom.solve_field(allow_not_converged=True)
+    return dom, dt
+
+
+def run_surface(args, cfg):
+    """Large surface-charging run: the FP64 form first (its face potentials after W + K steps
+    are the error reference and its K steps the 1x), then the mixed form on the same seeded
+    state; value = the mixed form's particle-steps/s."""
+    import torch
+
+    from scdat_b200 import build, capi
+
+    build.build()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=900))
+    res = {}
+    clk = None
+    for prec in (0, 1):
+        dom, dt = build_surface_domain(cfg, prec, capi)
+        stream = torch.cuda.ExternalStream(dom.stream())
+        for _ in range(args.warmup):
+            dom.step(1)
+        torch.cuda.synchronize()
+        if prec == 1 and dist:
+            dist.barrier()
+        clocks = ClockSampler(local)
+        if prec == 1:
+            clocks.start()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        ps = 0
+        for _ in range(args.steps):
+            dom.step(1)
+            ps += dom.stats()["active_particles"]
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        if prec == 1:
+            clk = clocks.stop()
+        ms = ev0.elapsed_time(ev1)
+        srf = dom.surface_state()
+        res[prec] = dict(ms=ms, ps=ps, V=srf["V"], Q=srf["Q"], particles=int(sum(dom.count(s) for s in range(2))),
+                         tets=dom.T, dt=dt)
+        dom.close()
+    v64, v32 = res[0]["V"], res[1]["V"]
+    err = float(np.abs(v32 - v64).max() / max(np.abs(v64).max(), 1e-300))
+    t_local = res[1]["ms"] / 1e3
+    if dist:
+        t = torch.tensor([t_local, float(res[1]["ps"])], device="cuda", dtype=torch.float64)
+        tmax = t.clone()
+        dist.all_reduce(tmax[:1], op=dist.ReduceOp.MAX)
+        dist.all_reduce(t[1:], op=dist.ReduceOp.SUM)
+        t_max, total_ps = float(tmax[0]), float(t[1])
+    else:
+        t_max, total_ps = t_local, float(res[1]["ps"])
+    out = {
+        "metric": "PIC particle-steps/s on 1 B200 (mixed/batched vs plain FP64 at equal error)",
+        "value": total_ps / t_max, "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_max * 1e3 / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded, no dataset)",
+        "config": {"workload": "surface256", "cells": list(cfg["cells"]), "tets": res[1]["tets"],
+                   "particles": res[1]["particles"], "dt": res[1]["dt"], "precision": "mixed",
+                   "surface": "6 floating dielectric faces (eps_r 3, 1 mm), FP64 charge and potential",
+                   "l2": "inputs larger than L2 (particle state > 126 MB)", "parallelism": f"replicas x{world}"},
+        "fp64_form": {"value": res[0]["ps"] / (res[0]["ms"] / 1e3), "unit": "particle-steps/s",
+                      "ms_per_step": res[0]["ms"] / args.steps},
+        "floating_potential": {"mixed_V": v32.tolist(), "fp64_V": v64.tolist(), "rel_err_vs_fp64": err,
+                               "after_steps": args.warmup + args.steps},
+        "clocks": clk,
+    }
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out))
+
+
 def fp64_compare(cfg, args):
     """The plain FP64 form on the same workload (the 1x of the mixed-form speed-up)."""
     import torch
@@ -532,11 +642,13 @@ def main():
     ap.add_argument("--scenarios", type=int, default=0, help="batched64: number of scenarios (default 64)")
     args = ap.parse_args()
     cfg = dict(CONFIGS[args.config])
-    if args.config == "batched64":
+    if args.config in ("batched64", "surface256"):
         if args.impl == "reference":
             run_reference(args, dict(CONFIGS["precision128"]))
-        else:
+        elif args.config == "batched64":
             run_batched(args, cfg)
+        else:
+            run_surface(args, cfg)
         return
     if args.n:
         f = args.n / cfg["n"]

@@ -200,7 +200,8 @@ __device__ __forceinline__ void defer_store_d(const ParticleStore& P, const Defe
 }
 
 // Pass 1: every stored particle, at most kCap1 sub-steps.
-__global__ void __launch_bounds__(256) k_push_f64(MeshView M, ParticleStore P, SpeciesDev S, PushParams pp,
+__global__ void __launch_bounds__(256) k_push_f64(const __grid_constant__ MeshView M, ParticleStore P,
+    const __grid_constant__ SpeciesDev S, const __grid_constant__ PushParams pp,
                                                   DeferList D, ChargeAcc A,
                                                   LedgerDev* L, double* ke_part)
 {
@@ -245,7 +246,8 @@ __global__ void __launch_bounds__(256) k_push_f64(MeshView M, ParticleStore P, S
 }
 
 // Passes 2 and 3 over a deferred list (see k_push_mixed_more).
-__global__ void __launch_bounds__(256) k_push_f64_more(MeshView M, ParticleStore P, SpeciesDev S, PushParams pp,
+__global__ void __launch_bounds__(256) k_push_f64_more(const __grid_constant__ MeshView M, ParticleStore P,
+    const __grid_constant__ SpeciesDev S, const __grid_constant__ PushParams pp,
                                                        DeferList Din, DeferList Dout, int cap, ChargeAcc A, LedgerDev* L, double* ke_part)
 {
     const int64_t n = (int64_t)min(*Din.count, Din.cap);

@@ -430,7 +430,8 @@ __device__ __forceinline__ void push_more_warp(const MeshView& M, const Particle
 }
 
 // Pass 1: every stored particle.
-__global__ void __launch_bounds__(256, 4) k_push_mixed(MeshView M, ParticleStore P, SpeciesDev S, PushParams pp,
+__global__ void __launch_bounds__(256, 4) k_push_mixed(const __grid_constant__ MeshView M, ParticleStore P,
+    const __grid_constant__ SpeciesDev S, const __grid_constant__ PushParams pp,
                                                     DeferList D, ChargeAcc A,
                                                     LedgerDev* L, double* ke_part)
 {
@@ -443,7 +444,8 @@ __global__ void __launch_bounds__(256, 4) k_push_mixed(MeshView M, ParticleStore
 }
 
 // Passes 2 and 3.
-__global__ void __launch_bounds__(256, 4) k_push_mixed_more(MeshView M, ParticleStore P, SpeciesDev S, PushParams pp,
+__global__ void __launch_bounds__(256, 4) k_push_mixed_more(const __grid_constant__ MeshView M, ParticleStore P,
+    const __grid_constant__ SpeciesDev S, const __grid_constant__ PushParams pp,
                                                          DeferList Din, DeferList Dout, int cap,
                                                          ChargeAcc A,
                                                          LedgerDev* L, double* ke_part)
