@@ -231,9 +231,13 @@ __device__ __forceinline__ int advance_f(const MeshView& M, const SpeciesDev& S,
     const float qm = (float)S.qm;
     const float floor_ratio = (float)pp.floor_ratio;
     const double qw = S.q * S.w;
-    TetRec R = load_rec(M, f.cur);
+    // only J^-1 stays in registers; E0, the E differences and the node ids are read from the
+    // record (already in L1) where they are used
+    const float4* rec = reinterpret_cast<const float4*>(M.trec + 64 * (int64_t)f.cur);
+    float J[9];
+    load_j(M, f.cur, J);
     float l[4];
-    baryj(R.j, f.rx, f.ry, f.rz, l);
+    baryj(J, f.rx, f.ry, f.rz, l);
     bool in = inside_f(l);
     int k = 0;
     while (f.rem > 1e-20f && f.it < kMaxSubsteps) {
@@ -242,9 +246,10 @@ __device__ __forceinline__ int advance_f(const MeshView& M, const SpeciesDev& S,
         ++f.it;
         float Ex = 0.f, Ey = 0.f, Ez = 0.f;
         if (in) {  // E = E0 + sum_i lambda_i (E_i - E0), i = 1..3
-            Ex = fmaf(l[1], R.d[0], fmaf(l[2], R.d[3], fmaf(l[3], R.d[6], R.e0[0])));
-            Ey = fmaf(l[1], R.d[1], fmaf(l[2], R.d[4], fmaf(l[3], R.d[7], R.e0[1])));
-            Ez = fmaf(l[1], R.d[2], fmaf(l[2], R.d[5], fmaf(l[3], R.d[8], R.e0[2])));
+            const float4 c = __ldg(rec + 2), d = __ldg(rec + 3), e = __ldg(rec + 4), g = __ldg(rec + 5);
+            Ex = fmaf(l[1], d.x, fmaf(l[2], d.w, fmaf(l[3], e.z, c.y)));
+            Ey = fmaf(l[1], d.y, fmaf(l[2], e.x, fmaf(l[3], e.w, c.z)));
+            Ez = fmaf(l[1], d.z, fmaf(l[2], e.y, fmaf(l[3], g.x, c.w)));
         }
         float adt = f.rem;
         float Em = sqrtf(Ex * Ex + Ey * Ey + Ez * Ez);
@@ -265,7 +270,7 @@ __device__ __forceinline__ int advance_f(const MeshView& M, const SpeciesDev& S,
         f.ry = fmaf(f.vy, adt, f.ry);
         f.rz = fmaf(f.vz, adt, f.rz);
         float le[4];
-        baryj(R.j, f.rx, f.ry, f.rz, le);
+        baryj(J, f.rx, f.ry, f.rz, le);
         if (inside_f(le)) {
             if (pp.deposit) {
                 if (in) {
@@ -274,7 +279,8 @@ __device__ __forceinline__ int advance_f(const MeshView& M, const SpeciesDev& S,
 #pragma unroll
                     for (int q = 0; q < 4; ++q) {
                         float lk = tiny ? l[q] : (pp.dep_kernel == 0 ? le[q] : 0.5f * (l[q] + le[q]));
-                        fx_red(A, R.nd[q], fx_from_double((qw * (double)lk) * pp.inv_uq));
+                        const int nd = __float_as_int(__ldg(reinterpret_cast<const float*>(rec) + 21 + q));
+                        fx_red(A, nd, fx_from_double((qw * (double)lk) * pp.inv_uq));
                     }
                 } else {
                     deposit_traj_f(M, S, pp, f.cur, sx, sy, sz, f.rx, f.ry, f.rz, A);
@@ -287,9 +293,10 @@ __device__ __forceinline__ int advance_f(const MeshView& M, const SpeciesDev& S,
             int nt = relocate_f(M, f.cur, f.rx, f.ry, f.rz, sx, sy, sz);
             if (nt < 0) return kLost;
             f.cur = nt;
-            R = load_rec(M, nt);
+            rec = reinterpret_cast<const float4*>(M.trec + 64 * (int64_t)nt);
+            load_j(M, nt, J);
             if (pp.deposit) deposit_traj_f(M, S, pp, nt, sx, sy, sz, f.rx, f.ry, f.rz, A);
-            baryj(R.j, f.rx, f.ry, f.rz, l);
+            baryj(J, f.rx, f.ry, f.rz, l);
             in = inside_f(l);
         }
         f.rem -= adt;
