@@ -8,7 +8,8 @@ Workloads (all synthetic, seeded; the reference publishes no dataset):
                 conducting body at -10 V, outer faces 0 V, electrons + H+ at n = 1e10 m^-3,
                 Te = Ti = 1 eV, 64 particles per cell per species (~268M), dt = 2e-8 s,
                 FP32 cell-relative push, fixed-point deposit, FP32-SpMV PCG under FP64
-                refinement to 1e-10, elastic MCC (sigma 1e-19 m^2, n_n 1e14 m^-3)   [default]
+                refinement to 1e-10, elastic MCC (sigma 1e-19 m^2, n_n 1e14 m^-3), re-sorted
+                by tet every 2 steps (electrons cross ~0.7 cells per step)   [default]
   plain32       32^3 cells, h = 0.05 m, 8^3-cell body, 20 ppc, FP64, Jacobi-PCG to 1e-8
   batched64     64 independent scenarios stepped together (one launch per kernel over all of
                 them, one CUDA-graph launch per step, launch shapes autotuned): box edge
@@ -44,7 +45,7 @@ QE, ME, MP = 1.602176634e-19, 9.1093837015e-31, 1.67262192369e-27
 
 CONFIGS = {
     "precision128": dict(n=128, L=1.6, body=(48, 80), bias=-10.0, ppc=64, dt=2e-8, precision=1, rtol=1e-10,
-                         density=1e10, te=1.0, ti=1.0, sort_interval=4),
+                         density=1e10, te=1.0, ti=1.0, sort_interval=2),
     "plain32": dict(n=32, L=1.6, body=(12, 20), bias=-10.0, ppc=20, dt=2e-8, precision=0, rtol=1e-8, density=1e10,
                     te=1.0, ti=1.0, sort_interval=8),
     "batched64": dict(scenarios=64, seed=2026, precision=1, rtol=1e-10, sort_interval=4),
@@ -227,12 +228,56 @@ def run_ours(args, cfg):
     peak, peak_kind = load_peaks()
     achieved = bytes_push / (push_ms / 1e3) / 1e9
     traffic = None
-    tr_file = os.path.join(ROOT, "profiles", "push_traffic.json")
-    if os.path.exists(tr_file):
-        d = json.load(open(tr_file))
+    # DRAM bytes of one step's push launches from an ncu capture of this workload
+    # (profiles/push_dram_precision128.md, line "dram_bytes_per_particle_<form>: <value>"),
+    # scaled to this run's particles
+    tr_file = os.path.join(ROOT, "profiles", f"push_dram_{args.config}.md")
+    if os.path.exists(tr_file) and not args.n and not args.ppc:
+        import re
+
         key = "mixed" if prec == 1 else "fp64"
-        if key in d:
-            traffic = d[key]["dram_bytes_per_particle"] * parts_per_launch
+        m = re.search(rf"dram_bytes_per_particle_{key}:\s*([0-9.eE+]+)", open(tr_file).read())
+        if m:
+            traffic = float(m.group(1)) * parts_per_launch
+    # The same workload as a one-scenario batch: the whole step (three push launches, charge,
+    # the refinement and PCG loops, field) is one CUDA-graph launch with device-side loop
+    # control, bitwise the same results as the stepped context above.  The headline value is
+    # this form; the stepped run above gives the per-stage split and the push roofline.
+    graph = None
+    runner = dom
+    if prec == 1:
+        batch = capi.Batch([dom])
+        for _ in range(2):
+            batch.step(1)
+        gstream = torch.cuda.ExternalStream(batch.stream())
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        l0 = batch.kernel_launches()
+        clocks = ClockSampler(local)
+        clocks.start()
+        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        g0.record(gstream)
+        gps = 0
+        for _ in range(args.steps):
+            batch.step(1)
+            gps += dom.stats()["active_particles"]
+        g1.record(gstream)
+        torch.cuda.synchronize()
+        gms = g0.elapsed_time(g1)
+        clk = clocks.stop()
+        graph = dict(ms=gms, ps=gps, launches=batch.kernel_launches() - l0)
+        runner = batch
+        t_local = gms / 1e3
+        if dist:
+            t = torch.tensor([t_local, float(gps)], device="cuda", dtype=torch.float64)
+            tmax = t.clone()
+            dist.all_reduce(tmax[:1], op=dist.ReduceOp.MAX)
+            dist.all_reduce(t[1:], op=dist.ReduceOp.SUM)
+            t_max, total_psteps = float(tmax[0]), float(t[1])
+        else:
+            t_max, total_psteps = t_local, float(gps)
+        value = total_psteps / t_max
     # end-to-end through the C ABI with host buffers: per step, Dirichlet potentials in from
     # pinned host memory, then the ledger, statistics and the nodal potential back
     dir_nodes = np.nonzero(mesh["dirichlet"])[0].astype(np.int64)
@@ -245,7 +290,7 @@ def run_ours(args, cfg):
     e2e_ps = 0
     for _ in range(e2e_steps):
         dom.L.scdat_set_node_potentials(dom.h, len(dir_nodes), h_nodes.data_ptr(), h_vals.data_ptr())
-        dom.step(1)
+        runner.step(1)
         led = dom.ledger()
         st = dom.stats()
         dom.L.scdat_get_fields(dom.h, None, h_phi.data_ptr(), None)
@@ -254,6 +299,8 @@ def run_ours(args, cfg):
     e2e_val = e2e_ps / (t1 - t0)
     h2d = len(dir_nodes) * 16
     d2h = dom.N * 8 + 7 * 8 * 8 + 120
+    if graph is not None:
+        batch.close()
     out = {
         "metric": "PIC particle-steps/s on 1 B200 (mixed/batched vs plain FP64 at equal error)",
         "value": value,
@@ -267,6 +314,8 @@ def run_ours(args, cfg):
         "vs_baseline": None,
         "dtype": "f32" if prec == 1 else "f64",
         "data": "synthetic (seeded Kuhn-box plasma, no dataset)",
+        "step_form": "one CUDA-graph launch per step (one-scenario batch)" if graph else "stepped context",
+        "stepped_ms_per_step": ms / args.steps,
         "config": {"workload": args.config, "cells": cfg["n"] ** 3, "tets": dom.T, "nodes": dom.N,
                    "particles": int(sum(dom.count(s) for s in range(dom.nspecies))), "ppc_per_species": cfg["ppc"],
                    "precision": "mixed" if prec == 1 else "fp64", "pcg_rtol": cfg["rtol"],
@@ -276,7 +325,7 @@ def run_ours(args, cfg):
                      "traffic": traffic, "peak_kind": peak_kind, "kernel": "push (gather+boris+relocate+deposit+mcc)",
                      "alg_bytes_per_launch": bytes_push, "launch_ms": push_ms},
         "stage_ms_per_step": {"push": tm["push_ms"] / args.steps, "field": tm["field_ms"] / args.steps},
-        "gpu_launches": int(tm["kernel_launches"]),
+        "gpu_launches": int(graph["launches"] if graph else tm["kernel_launches"]),
         "clocks": clk,
         "e2e": {"value": e2e_val, "unit": "particle-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
     }
@@ -491,7 +540,7 @@ def run_surface(args, cfg):
         ms = ev0.elapsed_time(ev1)
         srf = dom.surface_state()
         res[prec] = dict(ms=ms, ps=ps, V=srf["V"], Q=srf["Q"], particles=int(sum(dom.count(s) for s in range(2))),
-                         tets=dom.T, dt=dt)
+                         tets=dom.T, dt=dt, collected=int(np.asarray(srf["counts"]).sum()))
         dom.close()
     v64, v32 = res[0]["V"], res[1]["V"]
     err = float(np.abs(v32 - v64).max() / max(np.abs(v64).max(), 1e-300))
@@ -516,7 +565,8 @@ def run_surface(args, cfg):
         "fp64_form": {"value": res[0]["ps"] / (res[0]["ms"] / 1e3), "unit": "particle-steps/s",
                       "ms_per_step": res[0]["ms"] / args.steps},
         "floating_potential": {"mixed_V": v32.tolist(), "fp64_V": v64.tolist(), "rel_err_vs_fp64": err,
-                               "after_steps": args.warmup + args.steps},
+                               "after_steps": args.warmup + args.steps,
+                               "particles_collected": {"mixed": res[1]["collected"], "fp64": res[0]["collected"]}},
         "clocks": clk,
     }
     if dist:
@@ -600,7 +650,51 @@ def cpu_baseline(cfg, args):
         nt = 1
         kind, sample = "port", (f"C oracle push+deposit (1 thread) of {P} particles x {steps} steps on a 16^3-cell "
                                 f"box at the workload's cell size, plasma and ppc; field solve excluded")
-    return {"value": P * steps / total, "unit": "particle-steps/s", "cores": nt, "kind": kind, "sample": sample}
+    out = {"value": P * steps / total, "unit": "particle-steps/s", "cores": nt, "kind": kind, "sample": sample}
+    if kind == "reference" and not args.no_cpu_components:
+        out["components"] = cpu_components(O, cfg, mesh, sp, parts, E)
+    return out
+
+
+def cpu_components(O, cfg, mesh, sp, parts, E):
+    """The other CPU figures of the path, each on a bounded sample (a few seconds apiece): the
+    reference push as shipped (serial), the reference background MCC step, the Poisson solve by
+    the CPU restatement (the reference's dense solve is infeasible at this size), and the full
+    reference step (push, dense Poisson, field, statistics) on a 12^3-cell box."""
+    comp = {}
+    ref = O.Reference(omp=False)
+    sub = {k: (v[:8192] if isinstance(v, np.ndarray) else v) for k, v in parts.items()}
+    t0 = time.perf_counter()
+    ref.push(mesh, E, sub, sp, cfg["dt"])
+    dt_push = time.perf_counter() - t0
+    comp["push_serial"] = {"value": 8192 / dt_push, "unit": "particle-steps/s", "cores": 1,
+                           "sample": "reference CrossTetrahedron push+deposit as shipped (serial), 8192 particles x 1 step"}
+    ve = parts["v"][parts["species"] == 0]
+    t0 = time.perf_counter()
+    ref.mcc_count(ve, 0, sp[0].w, 1e-19, 1e14, cfg["dt"], 7, 1)
+    dt_mcc = time.perf_counter() - t0
+    comp["mcc"] = {"value": ve.shape[0] / dt_mcc, "unit": "particles/s", "cores": 1,
+                   "sample": f"reference MonteCarloCollisionHandler elastic step over {ve.shape[0]} electrons"}
+    o = O.Oracle()
+    A = o.assemble(mesh)
+    rho = np.random.default_rng(5).normal(0.0, 1e-12, mesh.N)
+    t0 = time.perf_counter()
+    o.poisson(mesh, A, rho, mesh.phi_bc, rtol=1e-8)
+    dt_pois = time.perf_counter() - t0
+    comp["poisson_restatement"] = {"value": 1.0 / dt_pois, "unit": "solves/s", "cores": 1,
+                                   "sample": f"C restatement Jacobi-PCG to 1e-8 on the {mesh.N}-node sample mesh"}
+    n = 12
+    h = cfg["L"] / cfg["n"]
+    m12 = O.kuhn_box((n, n, n), h, body=((4, 8), (4, 8), (4, 8)), bias=cfg["bias"])
+    sp12 = O.plasma_species(cfg["density"], cfg["te"], cfg["ti"], h, 2)
+    p12 = O.seed_particles(m12, sp12, 2, 11)
+    r = ref.cycle(m12, p12, sp12, 1, cfg["dt"], (1,) * 6, m12.phi_bc)
+    ref.close()
+    comp["full_step_12cubed"] = {"value": p12["x"].shape[0] / r["seconds"], "unit": "particle-steps/s",
+                                 "seconds_per_step": r["seconds"], "cores": 1,
+                                 "sample": f"reference PICCycle::executeTimeStep (dense Poisson on {m12.N} nodes) with "
+                                           f"{p12['x'].shape[0]} particles, 1 step"}
+    return comp
 
 
 def run_reference(args, cfg):
@@ -638,6 +732,7 @@ def main():
     ap.add_argument("--n", type=int, default=0, help="override the number of cells per edge")
     ap.add_argument("--ppc", type=int, default=0, help="override particles per cell per species")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-cpu-components", action="store_true", help="CPU baseline without its component figures")
     ap.add_argument("--no-fp64-compare", dest="fp64_compare", action="store_false")
     ap.add_argument("--scenarios", type=int, default=0, help="batched64: number of scenarios (default 64)")
     args = ap.parse_args()

@@ -163,6 +163,24 @@ SCDAT_API int scdat_kuhn_box_mesh(int32_t nx, int32_t ny, int32_t nz, double h, 
                                   double* node_xyz, int32_t* tet_nodes, uint8_t* node_dirichlet, double* node_phi,
                                   int32_t* hex_ijk, int64_t* n_cells);
 
+/* ParticleSource-style injection on any tet mesh: n_per_tet particles of the species in each
+ * of the n_tets listed tets (tets == NULL and n_tets == 0: every tet), positions uniform in the
+ * tet from Dirichlet(1,1,1,1) weights e_k / sum e, e_k = -log(max(1e-12, u_k)) as
+ * samplePointInTetra (Toolkit/Surface Charging/src/PicMccSurfaceCurrentSampler.cpp:270-287),
+ * velocities a Maxwellian of temp_ev plus drift[3] (nullable); Philox(seed) keyed by the id
+ * (tet_index * n_species + species) * n_per_tet + k.  Replaces the species' particles. */
+SCDAT_API int scdat_seed_tet_particles(scdat_ctx* ctx, int32_t species, int64_t n_tets, const int32_t* tets,
+                                       int32_t n_per_tet, double temp_ev, const double* drift, uint64_t seed);
+
+/* Result files in the reference's columnar CSV layout (ResultExporter / CSVExporter,
+ * Tools/Output/src/CSVExporter.cpp:11-47: header "axis,series..." with the series in name order,
+ * one row per axis value, %.8e).  The layer profile is the PIC-MCC driver's output
+ * (Main/main_PICcore.cpp:312-334): n_layers equal z slabs with the mean potential and E_z of
+ * their nodes, electron and ion densities and the electron temperature (m <v^2> / 3e). */
+SCDAT_API int scdat_export_layer_profile_csv(scdat_ctx* ctx, const char* path, int32_t n_layers);
+/* Every node: position, potential, charge and field. */
+SCDAT_API int scdat_export_nodes_csv(scdat_ctx* ctx, const char* path);
+
 /* ParticleContainer iteration (ParticleManager.h:113-126): copy one species back. */
 SCDAT_API int scdat_get_particle_count(scdat_ctx* ctx, int32_t species, int64_t* n);
 SCDAT_API int scdat_get_particles(scdat_ctx* ctx, int32_t species, int64_t capacity, double* x, double* v,

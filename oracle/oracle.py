@@ -598,3 +598,25 @@ class SurfaceCircuit:
             phi[i] = s / len(faces)
         return phi
 
+
+def seed_tets(mesh, species_index, n_species, n_per_tet, sigma, seed, tets=None, drift=(0.0, 0.0, 0.0)):
+    """Restated samplePointInTetra injection (PicMccSurfaceCurrentSampler.cpp:270-287) with the
+    Philox draws of scdat_seed_tet_particles: positions, velocities and tets of every particle."""
+    tl = np.arange(mesh.T) if tets is None else np.asarray(tets)
+    c = np.repeat(np.arange(len(tl)), n_per_tet)
+    j = np.tile(np.arange(n_per_tet), len(tl))
+    ids = ((c * n_species + species_index) * n_per_tet + j).astype(np.uint64)
+    u01, u23 = uniforms2(seed, ids, 0, 0), uniforms2(seed, ids, 0, 1)
+    g01, g23 = uniforms2(seed, ids, 0, 4), uniforms2(seed, ids, 0, 5)
+    u = np.concatenate([u01, u23], axis=1)
+    e = -np.log(np.maximum(1e-12, u))
+    es = ((e[:, 0] + e[:, 1]) + e[:, 2]) + e[:, 3]
+    t = tl[c]
+    x = np.zeros((len(ids), 3))
+    for q in range(4):
+        x += (e[:, q] / es)[:, None] * mesh.xyz[mesh.tet[t, q]]
+    r1, r2 = np.sqrt(-2.0 * np.log(g01[:, 0])), np.sqrt(-2.0 * np.log(g23[:, 0]))
+    tp = 6.283185307179586476925286766559
+    v = np.stack([drift[0] + sigma * r1 * np.cos(tp * g01[:, 1]), drift[1] + sigma * r1 * np.sin(tp * g01[:, 1]),
+                  drift[2] + sigma * r2 * np.cos(tp * g23[:, 1])], axis=1)
+    return x, v, t.astype(np.int32)

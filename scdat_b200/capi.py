@@ -91,7 +91,8 @@ EXPORTS = ["scdat_default_params", "scdat_create", "scdat_destroy", "scdat_last_
            "scdat_batch_step", "scdat_batch_set_tuning", "scdat_batch_get_tuning", "scdat_batch_autotune",
            "scdat_batch_last_step_ms", "scdat_batch_stream", "scdat_batch_kernel_launches",
            "scdat_set_surface_circuit", "scdat_get_surface_state", "scdat_set_secondary_emission",
-           "scdat_sample_with_derivative", "scdat_adjoint_window"]
+           "scdat_sample_with_derivative", "scdat_adjoint_window", "scdat_seed_tet_particles",
+           "scdat_export_layer_profile_csv", "scdat_export_nodes_csv"]
 
 _LIB = None
 
@@ -130,6 +131,9 @@ def load():
     L.scdat_set_surface_circuit.argtypes = [vp, C.POINTER(SurfaceCircuitC)]
     L.scdat_get_surface_state.argtypes = [vp, vp, vp, vp, vp]
     L.scdat_set_secondary_emission.argtypes = [vp, C.c_int32, C.c_double, C.c_double]
+    L.scdat_seed_tet_particles.argtypes = [vp, C.c_int32, C.c_int64, vp, C.c_int32, C.c_double, vp, C.c_uint64]
+    L.scdat_export_layer_profile_csv.argtypes = [vp, C.c_char_p, C.c_int32]
+    L.scdat_export_nodes_csv.argtypes = [vp, C.c_char_p]
     L.scdat_adjoint_window.argtypes = [vp, C.POINTER(AdjointRequestC), C.POINTER(AdjointResultC)]
     L.scdat_sample_with_derivative.argtypes = [C.POINTER(vp), C.c_int64, vp, C.c_double, C.c_double, C.c_int32,
                                                C.c_double, C.POINTER(CurrentSampleC)]
@@ -315,6 +319,19 @@ class Domain:
 
     def set_seed(self, seed):
         self._ck(self.L.scdat_set_seed(self.h, int(seed)))
+
+    def seed_tets(self, s, n_per_tet, temp_ev, seed, tets=None, drift=None):
+        """scdat_seed_tet_particles (all tets when `tets` is None)."""
+        t = None if tets is None else np.ascontiguousarray(tets, np.int32)
+        d = None if drift is None else np.ascontiguousarray(drift, np.float64)
+        self._ck(self.L.scdat_seed_tet_particles(self.h, s, 0 if t is None else t.shape[0], _p(t), int(n_per_tet),
+                                                 float(temp_ev), _p(d), int(seed)))
+
+    def export_layer_profile(self, path, n_layers):
+        self._ck(self.L.scdat_export_layer_profile_csv(self.h, str(path).encode(), int(n_layers)))
+
+    def export_nodes(self, path):
+        self._ck(self.L.scdat_export_nodes_csv(self.h, str(path).encode()))
 
     def set_surface_circuit(self, body_lo, body_hi, eps_r=3.0, thickness=1e-3, v0=0.0, shunt=0.0, didv=0.0,
                             area=0.0):

@@ -24,7 +24,7 @@ struct PushJob {
     PushParams pp;
     ChargeAcc A;
     LedgerDev* L;
-    double* ke_part;
+    unsigned long long* ke_acc;  // kinetic energy of the push, exact fixed point (lo, hi)
     DeferList D1, D2;
 };
 
@@ -34,8 +34,7 @@ struct FieldJob {
     int S;
     // per-step accumulators
     unsigned long long *l0, *l1, *h;  // charge limbs [S*N]
-    double* ke_part;                  // per-block kinetic-energy partials of the push
-    int ke_n;
+    unsigned long long* ke_acc;       // kinetic energy of the push, exact fixed point (lo, hi)
     unsigned long long* led_active;
     unsigned long long* lsq_bad;
     // charge finalisation
@@ -78,11 +77,13 @@ struct BlockMap {
     int blocks;
 };
 
-// push (push_mixed.cu); chunk_prefix[j] = first 256-particle chunk of job j, computed on the
-// device from the live counts by launch_batch_prefix.
-void launch_batch_prefix(const PushJob* jobs, int njobs, int pass, int64_t* chunk_prefix, cudaStream_t st);
-void launch_push_mixed_batch(const PushJob* jobs, int njobs, const int64_t* chunk_prefix, int pass, int grid,
-                             cudaStream_t st);
+// push (push_mixed.cu); chunk_prefix[j] = first 32-particle chunk of job j, computed on the
+// device from the live counts by launch_batch_prefix, which also zeroes the pass's work counter
+// ctr[pass - 1].
+void launch_batch_prefix(const PushJob* jobs, int njobs, int pass, int64_t* chunk_prefix, unsigned* ctr,
+                         cudaStream_t st);
+void launch_push_mixed_batch(const PushJob* jobs, int njobs, const int64_t* chunk_prefix, unsigned* ctr, int pass,
+                             int grid, cudaStream_t st);
 void launch_batch_refresh_trec(const FieldJob* jobs, const BlockMap& tets, cudaStream_t st);
 
 // field (batch_field.cu).  cond_* are CUDA-graph conditional handles (0 outside a graph);

@@ -36,8 +36,9 @@ __global__ void k_batch_zero(const FieldJob* __restrict__ jobs, const PushJob* _
         h[i] = 0ull;
     }
     if (blockIdx.x == 0) {
-        for (int i = threadIdx.x; i < J.ke_n; i += blockDim.x) J.ke_part[i] = 0.0;
         if (threadIdx.x == 0) {
+            J.ke_acc[0] = 0ull;
+            J.ke_acc[1] = 0ull;
             *J.led_active = 0ull;
             J.totq[0] = 0ull;
             J.totq[1] = 0ull;
@@ -100,7 +101,7 @@ __global__ void k_batch_residual(const FieldJob* __restrict__ jobs, BlockMap m)
 }
 
 // One thread per scenario: converged, out of iterations or out of refinement passes ends the
-// scenario's loop; otherwise start an FP32 solve of A e = r to 1e-4.  Sets the inner loop's
+// scenario's loop; otherwise start an FP32 solve of A e = r to the tolerance this pass needs.  Sets the inner loop's
 // condition to "some scenario still solving" (run_pcg_mixed in capi.cu is the same loop
 // driven from the host).
 __global__ void k_batch_inner_setup(const FieldJob* __restrict__ jobs, int njobs, unsigned long long cond,
@@ -116,7 +117,7 @@ __global__ void k_batch_inner_setup(const FieldJob* __restrict__ jobs, int njobs
             continue;
         }
         PcgScalars* s = jobs[k].sc;
-        s->rtol = 1e-4;
+        s->rtol = inner_rtol(o->rr, bb, o->rtol);
         s->max_iter = max(1, o->max_iter - o->iter);
         s->abs_thr2 = 0.0;
         s->done = 0;

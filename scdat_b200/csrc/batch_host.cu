@@ -59,6 +59,7 @@ struct scdat_batch {
     DBuf<PushJob> pjobs;
     DBuf<FieldJob> fjobs;
     DBuf<int64_t> prefix;
+    DBuf<unsigned> pass_ctr;  // work counters of the three push passes
     DBuf<PcgScalars> sco;
     DBuf<int> any;
     DBuf<unsigned long long> passes;  // [outer passes, inner double-iterations]
@@ -117,7 +118,7 @@ int upload_jobs(scdat_batch* b)
         J.pp = push_params(c, true);
         J.A = ChargeAcc{c->acc_l0.p + s * N, c->acc_l1.p + s * N, c->acc_h.p + s * N};
         J.L = c->led.p;
-        J.ke_part = c->ke_part.p;
+        J.ke_acc = c->ke_acc.p;
         DeferBufs& d = *b->defer[j];
         const unsigned cap = (unsigned)d.idx[0].n;
         J.D1 = DeferList{b->dcount.p + 2 * j, cap, d.idx[0].p, d.it[0].p, d.rem[0].p, d.vs[0].p};
@@ -134,8 +135,7 @@ int upload_jobs(scdat_batch* b)
         F.l0 = c->acc_l0.p;
         F.l1 = c->acc_l1.p;
         F.h = c->acc_h.p;
-        F.ke_part = c->ke_part.p;
-        F.ke_n = (int)c->ke_part.n;
+        F.ke_acc = c->ke_acc.p;
         F.led_active = &c->led.p->active;
         F.lsq_bad = &c->led.p->lsq_bad;
         F.uq = c->uq;
@@ -202,8 +202,8 @@ void enqueue_front(scdat_batch* b, cudaStream_t s)
     launch_batch_zero(b->fjobs.p, b->pjobs.p, nc, nj, b->nsm * 2, s);
     const int grid = b->nsm * b->tune.push_blocks_per_sm;
     for (int pass = 1; pass <= 3; ++pass) {
-        launch_batch_prefix(b->pjobs.p, nj, pass, b->prefix.p, s);
-        launch_push_mixed_batch(b->pjobs.p, nj, b->prefix.p, pass, grid, s);
+        launch_batch_prefix(b->pjobs.p, nj, pass, b->prefix.p, b->pass_ctr.p, s);
+        launch_push_mixed_batch(b->pjobs.p, nj, b->prefix.p, b->pass_ctr.p, pass, grid, s);
     }
     launch_batch_surface(b->fjobs.p, nc, s);
     launch_batch_finalize_rhs(b->fjobs.p, b->nodes.view, b->rows.view, s);
@@ -400,6 +400,7 @@ SCDAT_API int scdat_batch_create(int32_t n, scdat_ctx* const* ctxs, scdat_batch*
     BCK(b->pjobs.alloc((size_t)njobs));
     BCK(b->fjobs.alloc((size_t)n));
     BCK(b->prefix.alloc((size_t)njobs + 1));
+    BCK(b->pass_ctr.alloc(3));
     BCK(b->sco.alloc((size_t)n));
     BCK(cudaMemsetAsync(b->sco.p, 0, sizeof(PcgScalars) * n, b->st));
     BCK(b->any.alloc(1));
@@ -427,8 +428,8 @@ SCDAT_API const char* scdat_batch_last_error(const scdat_batch* b) { return b ? 
 SCDAT_API int scdat_batch_set_tuning(scdat_batch* b, const scdat_batch_tuning* t)
 {
     if (!b || !t) return SCDAT_ERR_ARG;
-    // each push block writes one kinetic-energy partial per scenario (grid_push slots), each
-    // field block one reduction partial per scenario (grid_red slots)
+    // each field block writes one reduction partial per scenario (grid_red slots); push launches
+    // keep the same bound (8 blocks per SM, twice what is resident)
     const int push_max = b->ctx[0]->grid_push / b->nsm, field_max = b->ctx[0]->grid_red / b->nsm;
     if (t->push_blocks_per_sm < 1 || t->push_blocks_per_sm > push_max || t->field_blocks_per_sm < 1 ||
         t->field_blocks_per_sm > field_max) {

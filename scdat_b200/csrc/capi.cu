@@ -20,13 +20,13 @@
 
 namespace scdat {
 void launch_push_f64(const MeshView& M, const ParticleStore& P, const SpeciesDev& S, const PushParams& pp,
-                     const DeferList& D1, const DeferList& D2, ChargeAcc A, LedgerDev* L, double* ke_part, int grid,
-                     cudaStream_t st);
+                     const DeferList& D1, const DeferList& D2, ChargeAcc A, LedgerDev* L, unsigned long long* ke_acc,
+                     unsigned* ctr, int grid, cudaStream_t st);
 void launch_mcc_f64(const ParticleStore& P, const SpeciesDev& S, const PushParams& pp, LedgerDev* L, int grid,
                     cudaStream_t st);
 void launch_push_mixed(const MeshView& M, const ParticleStore& P, const SpeciesDev& S, const PushParams& pp,
-                       const DeferList& D1, const DeferList& D2, ChargeAcc A, LedgerDev* L, double* ke_part, int grid,
-                       cudaStream_t st);
+                       const DeferList& D1, const DeferList& D2, ChargeAcc A, LedgerDev* L,
+                       unsigned long long* ke_acc, unsigned* ctr, int grid, cudaStream_t st);
 void launch_mcc_mixed(const ParticleStore& P, const SpeciesDev& S, const PushParams& pp, LedgerDev* L, int grid,
                       cudaStream_t st);
 void launch_refresh_erec(int64_t T, const int4* tet, const double* E, double* erec, cudaStream_t st);
@@ -38,10 +38,16 @@ void launch_from_mixed(const MeshView& M, int64_t n, const ParticleStore& P, dou
 void launch_seed_box(const int32_t* hex_ijk, int64_t ncell, int32_t ppc, int32_t S_total, int32_t s, double h,
                      double sigma, uint64_t seed, const ParticleStore& P, bool mixed, const MeshView& M,
                      cudaStream_t st);
+void launch_seed_tets(const int32_t* tets, int64_t ntet, int32_t per_tet, int32_t S_total, int32_t s, double sigma,
+                      const double drift[3], uint64_t seed, const ParticleStore& P, bool mixed, const MeshView& M,
+                      cudaStream_t st);
+void launch_layer_moments(const ParticleStore& P, int64_t n, bool mixed, const MeshView& M, double z0, double z1,
+                          int n_layers, double* cnt, double* v2, cudaStream_t st);
 void launch_sort_keys(int64_t n, const int32_t* tet, uint32_t inactive_key, uint32_t* keys, uint32_t* vals,
                       int64_t* active, cudaStream_t st);
 template <typename T>
-void launch_gather(int64_t n, const uint32_t* perm, const T* in, T* out, cudaStream_t st);
+void launch_gather_store(int64_t n, const int64_t* active, const uint32_t* perm, const GatherArrays<T>& in,
+                         const GatherArrays<T>& out, cudaStream_t st);
 void launch_scatter_values(int64_t n, const int64_t* idx, const double* v, double* dst, cudaStream_t st);
 }  // namespace scdat
 
@@ -176,7 +182,7 @@ int do_push(scdat_ctx* ctx, bool do_mcc)
     CK(cudaMemsetAsync(ctx->acc_l0.p, 0, sizeof(unsigned long long) * S * N, ctx->st));
     CK(cudaMemsetAsync(ctx->acc_l1.p, 0, sizeof(unsigned long long) * S * N, ctx->st));
     CK(cudaMemsetAsync(ctx->acc_h.p, 0, sizeof(unsigned long long) * S * N, ctx->st));
-    CK(cudaMemsetAsync(ctx->ke_part.p, 0, sizeof(double) * ctx->grid_push, ctx->st));
+    CK(cudaMemsetAsync(ctx->ke_acc.p, 0, 2 * sizeof(unsigned long long), ctx->st));
     CK(cudaMemsetAsync(&ctx->led.p->active, 0, sizeof(unsigned long long), ctx->st));
     PushParams pp = push_params(ctx, do_mcc);
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -190,15 +196,18 @@ int do_push(scdat_ctx* ctx, bool do_mcc)
         ctx->push_particles += ctx->species[s].n;
         ParticleStore P = store_of(ctx, s);
         SpeciesDev sd = species_dev(ctx, s);
-        CK(cudaMemsetAsync(ctx->dcount.p, 0, 2 * sizeof(unsigned), ctx->st));
+        // defer-list counts [0, 1] and the three passes' work counters [2, 5)
+        CK(cudaMemsetAsync(ctx->dcount.p, 0, 5 * sizeof(unsigned), ctx->st));
         DeferList d1{ctx->dcount.p, ctx->dcap, ctx->d1idx.p, ctx->d1it.p, ctx->d1rem.p, ctx->d1vs.p};
         DeferList d2{ctx->dcount.p + 1, ctx->dcap, ctx->d2idx.p, ctx->d2it.p, ctx->d2rem.p, ctx->d2vs.p};
         ctx->launches += 3;
         ChargeAcc acc{ctx->acc_l0.p + s * N, ctx->acc_l1.p + s * N, ctx->acc_h.p + s * N};
         if (ctx->mixed)
-            launch_push_mixed(ctx->mv, P, sd, pp, d1, d2, acc, ctx->led.p, ctx->ke_part.p, ctx->grid_push, ctx->st);
+            launch_push_mixed(ctx->mv, P, sd, pp, d1, d2, acc, ctx->led.p, ctx->ke_acc.p, ctx->dcount.p + 2,
+                              ctx->grid_push, ctx->st);
         else
-            launch_push_f64(ctx->mv, P, sd, pp, d1, d2, acc, ctx->led.p, ctx->ke_part.p, ctx->grid_push, ctx->st);
+            launch_push_f64(ctx->mv, P, sd, pp, d1, d2, acc, ctx->led.p, ctx->ke_acc.p, ctx->dcount.p + 2,
+                            ctx->grid_push, ctx->st);
     }
     CK(cudaGetLastError());
     if (ctx->timing) {
@@ -303,10 +312,10 @@ int run_pcg_mixed(scdat_ctx* ctx, double rtol, int max_iter, int& iters, double&
         double bb = h.bb > 0.0 ? h.bb : 1.0;
         relres = std::sqrt(h.rr / bb);
         if (h.rr <= rtol * rtol * bb || iters >= max_iter) break;
-        // inner FP32 solve A e = r to 1e-4 relative, from e = 0
+        // inner FP32 solve A e = r from e = 0, to the tolerance this pass needs
         ctx->launches += 2;
         launch_zero_f32(R, ctx->xf.p, ctx->grid_red, ctx->st);
-        rc = pcg_scalars_init(ctx, 1e-4, std::max(1, max_iter - iters), 0.0);
+        rc = pcg_scalars_init(ctx, inner_rtol(h.rr, bb, rtol), std::max(1, max_iter - iters), 0.0);
         if (rc) return rc;
         launch_pcg_init32(A, ctx->rf.p, ctx->xf.p, ctx->qf.p, ctx->zf.p, ctx->sc.p, ctx->part.p, ctx->grid_red,
                           ctx->st);
@@ -414,7 +423,7 @@ int do_sort(scdat_ctx* ctx, int s)
     const uint32_t inactive = (uint32_t)ctx->hm.T;  // keys: tet, T (no hint), T+1 (inactive)
     int bits = 1;
     while (((uint64_t)1 << bits) <= (uint64_t)inactive + 1) ++bits;
-    ctx->launches += 9;  // keys + 8 gathers (the radix sort itself is CUB's)
+    ctx->launches += 2;  // keys + one gather of the whole store (the radix sort itself is CUB's)
     launch_sort_keys(n, S.tet.p, inactive, ctx->kin.p, ctx->vin.p, ctx->nact.p, ctx->st);
     size_t tmp = 0;
     CK(cub::DeviceRadixSort::SortPairs(nullptr, tmp, ctx->kin.p, ctx->kout.p, ctx->vin.p, ctx->vout.p, (int)n, 0, bits,
@@ -423,26 +432,34 @@ int do_sort(scdat_ctx* ctx, int s)
     CK(cub::DeviceRadixSort::SortPairs(ctx->cub_tmp.p, tmp, ctx->kin.p, ctx->kout.p, ctx->vin.p, ctx->vout.p, (int)n,
                                        0, bits, ctx->st));
     const uint32_t* perm = ctx->vout.p;
+    if (ctx->scratchi.n < S.tet.n) CK(ctx->scratchi.alloc(S.tet.n));
+    if (ctx->scratchu.n < S.id.n) CK(ctx->scratchu.alloc(S.id.n));
     if (ctx->mixed) {
         DBuf<float>* fa[6] = {&S.xf, &S.yf, &S.zf, &S.vxf, &S.vyf, &S.vzf};
-        for (auto* a : fa) {
-            if (ctx->scratch32.n < a->n) CK(ctx->scratch32.alloc(a->n));
-            launch_gather<float>(n, perm, a->p, ctx->scratch32.p, ctx->st);
-            a->swap(ctx->scratch32);
+        GatherArrays<float> in{}, out{};
+        for (int a = 0; a < 6; ++a) {
+            if (ctx->shadow32[a].n < fa[a]->n) CK(ctx->shadow32[a].alloc(fa[a]->n));
+            in.v[a] = fa[a]->p;
+            out.v[a] = ctx->shadow32[a].p;
         }
+        in.tet = S.tet.p; in.id = S.id.p;
+        out.tet = ctx->scratchi.p; out.id = ctx->scratchu.p;
+        launch_gather_store<float>(n, ctx->nact.p, perm, in, out, ctx->st);
+        for (int a = 0; a < 6; ++a) fa[a]->swap(ctx->shadow32[a]);
     } else {
         DBuf<double>* da[6] = {&S.x, &S.y, &S.z, &S.vx, &S.vy, &S.vz};
-        for (auto* a : da) {
-            if (ctx->scratch64.n < a->n) CK(ctx->scratch64.alloc(a->n));
-            launch_gather<double>(n, perm, a->p, ctx->scratch64.p, ctx->st);
-            a->swap(ctx->scratch64);
+        GatherArrays<double> in{}, out{};
+        for (int a = 0; a < 6; ++a) {
+            if (ctx->shadow64[a].n < da[a]->n) CK(ctx->shadow64[a].alloc(da[a]->n));
+            in.v[a] = da[a]->p;
+            out.v[a] = ctx->shadow64[a].p;
         }
+        in.tet = S.tet.p; in.id = S.id.p;
+        out.tet = ctx->scratchi.p; out.id = ctx->scratchu.p;
+        launch_gather_store<double>(n, ctx->nact.p, perm, in, out, ctx->st);
+        for (int a = 0; a < 6; ++a) da[a]->swap(ctx->shadow64[a]);
     }
-    if (ctx->scratchi.n < S.tet.n) CK(ctx->scratchi.alloc(S.tet.n));
-    launch_gather<int32_t>(n, perm, S.tet.p, ctx->scratchi.p, ctx->st);
     S.tet.swap(ctx->scratchi);
-    if (ctx->scratchu.n < S.id.n) CK(ctx->scratchu.alloc(S.id.n));
-    launch_gather<uint32_t>(n, perm, S.id.p, ctx->scratchu.p, ctx->st);
     S.id.swap(ctx->scratchu);
     CK(cudaGetLastError());
     int64_t act = 0;
@@ -626,7 +643,8 @@ SCDAT_API int scdat_create(const scdat_mesh_desc* mesh, const scdat_params* para
     CK(ctx->totq.alloc(2));
     CK(ctx->led.alloc(1));
     CK(cudaMemsetAsync(ctx->led.p, 0, sizeof(LedgerDev), st));
-    CK(ctx->ke_part.alloc((size_t)ctx->grid_push));
+    CK(ctx->ke_acc.alloc(2));
+    CK(cudaMemsetAsync(ctx->ke_acc.p, 0, 2 * sizeof(unsigned long long), ctx->st));
     CK(ctx->nact.alloc(1));
     CK(cudaStreamSynchronize(st));
     *out = holder.release();
@@ -695,7 +713,7 @@ static int alloc_species(scdat_ctx* ctx, int s, int64_t n)
     // only means the overflow finishes in the earlier pass)
     unsigned want = (unsigned)std::min<int64_t>(cap / 4 + 4096, 0x7fffffff);
     if (want > ctx->dcap) {
-        CK(ctx->dcount.alloc(2));
+        CK(ctx->dcount.alloc(5));
         CK(ctx->d1idx.alloc(want));
         CK(ctx->d2idx.alloc(want));
         CK(ctx->d1it.alloc(want));
@@ -706,7 +724,8 @@ static int alloc_species(scdat_ctx* ctx, int s, int64_t n)
         CK(ctx->d2vs.alloc(want));
         ctx->dcap = want;
     }
-    // sort scratch must cover the largest species
+    // sort scratch and re-sort targets must cover the largest species (allocated here, not in
+    // the first re-sort of a timed run)
     size_t need = (size_t)cap;
     if (ctx->kin.n < need) {
         CK(ctx->kin.alloc(need));
@@ -714,6 +733,18 @@ static int alloc_species(scdat_ctx* ctx, int s, int64_t n)
         CK(ctx->vin.alloc(need));
         CK(ctx->vout.alloc(need));
     }
+    for (int a = 0; a < 6; ++a) {
+        if (ctx->mixed && ctx->shadow32[a].n < need) CK(ctx->shadow32[a].alloc(need));
+        if (!ctx->mixed && ctx->shadow64[a].n < need) CK(ctx->shadow64[a].alloc(need));
+    }
+    if (ctx->scratchi.n < need) CK(ctx->scratchi.alloc(need));
+    if (ctx->scratchu.n < need) CK(ctx->scratchu.alloc(need));
+    int bits = 1;
+    while (((uint64_t)1 << bits) <= (uint64_t)ctx->hm.T + 1) ++bits;
+    size_t tmp = 0;
+    CK(cub::DeviceRadixSort::SortPairs(nullptr, tmp, ctx->kin.p, ctx->kout.p, ctx->vin.p, ctx->vout.p, (int)cap, 0,
+                                       bits, ctx->st));
+    if (tmp > ctx->cub_tmp.n) CK(ctx->cub_tmp.alloc(tmp));
     return SCDAT_OK;
 }
 
@@ -761,6 +792,151 @@ SCDAT_API int scdat_set_particles(scdat_ctx* ctx, int32_t species, int64_t n, co
     }
     CK(cudaStreamSynchronize(ctx->st));
     return SCDAT_OK;
+}
+
+SCDAT_API int scdat_seed_tet_particles(scdat_ctx* ctx, int32_t species, int64_t n_tets, const int32_t* tets,
+                                       int32_t n_per_tet, double temp_ev, const double* drift, uint64_t seed)
+{
+    if (!ctx) return SCDAT_ERR_ARG;
+    ARG(species >= 0 && species < (int)ctx->species.size(), "bad species index");
+    ARG(n_per_tet >= 0 && temp_ev >= 0.0, "bad count or temperature");
+    ARG(tets ? n_tets >= 0 : n_tets == 0, "give the tet list and its length, or neither (all tets)");
+    const int64_t nt = tets ? n_tets : ctx->hm.T;
+    std::vector<int32_t> list;
+    if (tets) {
+        for (int64_t k = 0; k < n_tets; ++k) ARG(tets[k] >= 0 && tets[k] < ctx->hm.T, "tet index out of range");
+        list.assign(tets, tets + n_tets);
+    }
+    const int64_t n = nt * n_per_tet;
+    ARG(n < (int64_t)0xffffffffLL, "too many particles for 32-bit ids");
+    int rc = alloc_species(ctx, species, n);
+    if (rc) return rc;
+    if (n == 0) return SCDAT_OK;
+    DBuf<int32_t> dl;
+    if (tets) CK(dl.upload(list.data(), list.size(), ctx->st));
+    const double sigma = std::sqrt(temp_ev * 1.602176634e-19 / ctx->species[species].sp.mass);
+    const double zero[3] = {0.0, 0.0, 0.0};
+    launch_seed_tets(tets ? dl.p : nullptr, nt, n_per_tet, (int32_t)ctx->species.size(), species, sigma,
+                     drift ? drift : zero, seed, store_of(ctx, species), ctx->mixed, ctx->mv, ctx->st);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(ctx->st));
+    return SCDAT_OK;
+}
+
+// ResultExporter / CSVExporter columnar layout (Tools/Output/src/CSVExporter.cpp:11-47): a header
+// "axis,series..." with the series in name order, then one row per axis value, %.8e.
+static int write_columns(scdat_ctx* ctx, const char* path, const std::string& axis, const std::vector<double>& av,
+                         const std::vector<std::pair<std::string, std::vector<double>>>& series)
+{
+    FILE* f = std::fopen(path, "w");
+    if (!f) {
+        ctx->err = std::string("cannot open ") + path;
+        return SCDAT_ERR_ARG;
+    }
+    std::fprintf(f, "%s", axis.c_str());
+    for (auto& s : series) std::fprintf(f, ",%s", s.first.c_str());
+    std::fprintf(f, "\n");
+    for (size_t r = 0; r < av.size(); ++r) {
+        std::fprintf(f, "%.8e", av[r]);
+        for (auto& s : series) std::fprintf(f, ",%.8e", s.second[r]);
+        std::fprintf(f, "\n");
+    }
+    std::fclose(f);
+    return SCDAT_OK;
+}
+
+SCDAT_API int scdat_export_layer_profile_csv(scdat_ctx* ctx, const char* path, int32_t n_layers)
+{
+    if (!ctx) return SCDAT_ERR_ARG;
+    ARG(path && n_layers > 0, "need a path and at least one layer");
+    const int64_t N = ctx->hm.N;
+    const double z0 = ctx->hg.bmin[2], z1 = ctx->hg.bmax[2];
+    std::vector<double> phi((size_t)N), E(3 * (size_t)N);
+    CK(cudaMemcpyAsync(phi.data(), ctx->phi.p, sizeof(double) * N, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaMemcpyAsync(E.data(), ctx->E.p, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, ctx->st));
+    // node layers by z
+    std::vector<double> ps(n_layers, 0.0), es(n_layers, 0.0), nn(n_layers, 0.0);
+    CK(cudaStreamSynchronize(ctx->st));
+    for (int64_t i = 0; i < N; ++i) {
+        const double z = ctx->hm.xyz[3 * i + 2];
+        int l = (int)((z - z0) / (z1 - z0) * n_layers);
+        l = std::min(std::max(l, 0), n_layers - 1);
+        ps[l] += phi[i];
+        es[l] += E[3 * i + 2];
+        nn[l] += 1.0;
+    }
+    // particle moments per species and layer
+    const double lv = (ctx->hg.bmax[0] - ctx->hg.bmin[0]) * (ctx->hg.bmax[1] - ctx->hg.bmin[1]) * (z1 - z0) / n_layers;
+    std::vector<double> ne(n_layers, 0.0), ni(n_layers, 0.0), te(n_layers, 0.0);
+    DBuf<double> cnt, v2;
+    CK(cnt.alloc(n_layers));
+    CK(v2.alloc(n_layers));
+    for (int s = 0; s < (int)ctx->species.size(); ++s) {
+        if (ctx->species[s].n == 0) continue;
+        CK(cudaMemsetAsync(cnt.p, 0, sizeof(double) * n_layers, ctx->st));
+        CK(cudaMemsetAsync(v2.p, 0, sizeof(double) * n_layers, ctx->st));
+        launch_layer_moments(store_of(ctx, s), ctx->species[s].n, ctx->mixed, ctx->mv, z0, z1, n_layers, cnt.p, v2.p,
+                             ctx->st);
+        CK(cudaGetLastError());
+        std::vector<double> c(n_layers), v(n_layers);
+        CK(cudaMemcpyAsync(c.data(), cnt.p, sizeof(double) * n_layers, cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaMemcpyAsync(v.data(), v2.p, sizeof(double) * n_layers, cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+        const auto& sp = ctx->species[s].sp;
+        for (int l = 0; l < n_layers; ++l) {
+            const double dens = c[l] * sp.weight / lv;
+            if (sp.electron_like) {
+                ne[l] += dens;
+                // 3/2 kT = 1/2 m <v^2> (the electrons' thermal plus drift energy), in eV
+                if (c[l] > 0) te[l] = sp.mass * (v[l] / c[l]) / (3.0 * 1.602176634e-19);
+            } else if (sp.charge > 0.0) {
+                ni[l] += dens;
+            }
+        }
+    }
+    std::vector<double> zc(n_layers), pm(n_layers), em(n_layers);
+    for (int l = 0; l < n_layers; ++l) {
+        zc[l] = z0 + (l + 0.5) * (z1 - z0) / n_layers;
+        pm[l] = nn[l] > 0 ? ps[l] / nn[l] : 0.0;
+        em[l] = nn[l] > 0 ? es[l] / nn[l] : 0.0;
+    }
+    // series in name order, as the reference's std::map keeps them
+    return write_columns(ctx, path, "z_m", zc,
+                         {{"electric_field_z_v_per_m", em},
+                          {"electron_density_m3", ne},
+                          {"electron_temperature_ev", te},
+                          {"ion_density_m3", ni},
+                          {"potential_v", pm}});
+}
+
+SCDAT_API int scdat_export_nodes_csv(scdat_ctx* ctx, const char* path)
+{
+    if (!ctx) return SCDAT_ERR_ARG;
+    ARG(path, "need a path");
+    const int64_t N = ctx->hm.N;
+    std::vector<double> rho((size_t)N), phi((size_t)N), E(3 * (size_t)N);
+    int rc = scdat_get_fields(ctx, rho.data(), phi.data(), E.data());
+    if (rc) return rc;
+    std::vector<double> id((size_t)N), x((size_t)N), y((size_t)N), z((size_t)N), ex((size_t)N), ey((size_t)N),
+        ez((size_t)N);
+    for (int64_t i = 0; i < N; ++i) {
+        id[i] = (double)i;
+        x[i] = ctx->hm.xyz[3 * i];
+        y[i] = ctx->hm.xyz[3 * i + 1];
+        z[i] = ctx->hm.xyz[3 * i + 2];
+        ex[i] = E[3 * i];
+        ey[i] = E[3 * i + 1];
+        ez[i] = E[3 * i + 2];
+    }
+    return write_columns(ctx, path, "node", id,
+                         {{"charge_c", rho},
+                          {"electric_field_x_v_per_m", ex},
+                          {"electric_field_y_v_per_m", ey},
+                          {"electric_field_z_v_per_m", ez},
+                          {"potential_v", phi},
+                          {"x_m", x},
+                          {"y_m", y},
+                          {"z_m", z}});
 }
 
 SCDAT_API int scdat_get_particle_count(scdat_ctx* ctx, int32_t species, int64_t* n)
@@ -1247,19 +1423,17 @@ SCDAT_API int scdat_get_statistics(scdat_ctx* ctx, scdat_stats* st)
 {
     if (!ctx || !st) return SCDAT_ERR_ARG;
     LedgerDev h{};
-    std::vector<double> ke((size_t)ctx->grid_push);
+    unsigned long long ke[2] = {0, 0};
     unsigned long long tq[2] = {0, 0};
     CK(cudaMemcpyAsync(&h, ctx->led.p, sizeof(h), cudaMemcpyDeviceToHost, ctx->st));
-    CK(cudaMemcpyAsync(ke.data(), ctx->ke_part.p, sizeof(double) * ke.size(), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaMemcpyAsync(ke, ctx->ke_acc.p, sizeof(ke), cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaMemcpyAsync(tq, ctx->totq.p, sizeof(tq), cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
     std::memset(st, 0, sizeof(*st));
     st->completed_steps = ctx->steps;
     st->simulation_time = ctx->sim_time;
     st->total_charge = fx_to_double(tq[0], (long long)tq[1], ctx->uq);
-    double e = 0.0;
-    for (double k : ke) e += k;
-    st->total_energy = e;
+    st->total_energy = fx_to_double(ke[0], (long long)ke[1], kKeUnit);
     st->active_particles = (int64_t)h.active;
     int64_t stored = 0;
     for (auto& S : ctx->species) stored += S.n;

@@ -56,6 +56,16 @@ __device__ inline void fx_atomic_add(unsigned long long* lo_acc, unsigned long l
     if (h) atomicAdd(hi_acc, h);
 }
 
+// A species' particle store as the re-sort gather sees it: six coordinate arrays (positions,
+// then velocities), tet ids and particle ids.
+template <typename T>
+struct GatherArrays {
+    T* v[6];
+    int32_t* tet;
+    uint32_t* id;
+};
+
+
 // Node charge accumulators: each 128-bit contribution is split into 32-bit limbs that go
 // into three 64-bit words with return-free atomic adds (no thread waits on an atomic), and
 // the limbs are recombined exactly when the charge is read.  2^32 contributions per node

@@ -93,12 +93,12 @@ struct scdat_ctx {
     std::vector<SpeciesState> species;
     DBuf<int64_t> counts;
     DBuf<LedgerDev> led;
-    DBuf<double> ke_part;
+    DBuf<unsigned long long> ke_acc;  // kinetic energy of the last push, fixed point (lo, hi)
     // sort scratch
     DBuf<uint32_t> kin, kout, vin, vout;
     DBuf<unsigned char> cub_tmp;
-    DBuf<double> scratch64;
-    DBuf<float> scratch32;
+    DBuf<double> shadow64[6];  // re-sort targets, swapped with the store's arrays
+    DBuf<float> shadow32[6];
     DBuf<int32_t> scratchi;
     DBuf<uint32_t> scratchu;
     DBuf<int64_t> nact;

@@ -31,6 +31,17 @@ struct PcgScalars {
     unsigned int pad2[3];
 };
 
+// Relative tolerance of the next FP32 inner solve of the mixed refinement, from the FP64
+// residual rr = |r|^2 against bb = |b|^2: enough for the corrected residual to clear the target
+// rtol in this pass with a factor-4 margin, but no tighter than 1e-5 (what an FP32 Jacobi-PCG
+// reliably reaches) and no looser than 1e-1.  The host-driven and the graph-driven loops both
+// call it, so they take the same passes.
+__host__ __device__ inline double inner_rtol(double rr, double bb, double rtol)
+{
+    const double need = 0.25 * rtol * sqrt(bb / rr);
+    return fmin(1e-1, fmax(1e-5, need));
+}
+
 void launch_finalize_rho(int64_t N, int S, const unsigned long long* l0, const unsigned long long* l1,
                          const unsigned long long* h, double unit, double* rho, unsigned long long* tlo,
                          unsigned long long* thi, int grid, cudaStream_t st);

@@ -354,10 +354,79 @@ struct DeferList {
 
 enum { kDone = 0, kCapped = 1, kLost = 2 };
 
+// Per-lane push statistics.  ke is the kinetic energy of the lane's particle in the current
+// 32-particle chunk; warp_chunk_end folds it, converted to the exact fixed point, into the
+// warp's total, so the energy sum does not depend on which warp took which chunk.
 struct PushStats {
-    double ke_sum;
+    double ke;
     unsigned long long nsub, nlost, nhit, nact;
 };
+
+// Kinetic energy accumulates as 128-bit fixed point with a unit of 2^-60 J: a 1 eV particle is
+// resolved to 1e-19 of itself and the sum can reach 8 J.
+constexpr double kKeInvUnit = 1152921504606846976.0;  // 2^60
+constexpr double kKeUnit = 8.673617379884035e-19;     // 2^-60
+
+// the warp's fixed-point kinetic-energy total for the kernel (one slot per warp of the block)
+__device__ __forceinline__ Fx128& warp_ke_slot()
+{
+    __shared__ Fx128 slot[32];
+    return slot[threadIdx.x >> 5];
+}
+
+// start of a push kernel; every lane calls it
+__device__ __forceinline__ void warp_stats_begin()
+{
+    if ((threadIdx.x & 31) == 0) warp_ke_slot() = Fx128{0ull, 0ll};
+    __syncwarp();
+}
+
+// end of a chunk; every lane calls it: the lanes' energies as fixed point, summed exactly
+__device__ __forceinline__ void warp_chunk_end(PushStats& c)
+{
+    const Fx128 v = fx_from_double(c.ke * kKeInvUnit);
+    c.ke = 0.0;
+    unsigned long long lo = v.lo;
+    long long hi = v.hi;
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long lo2 = __shfl_down_sync(0xffffffffu, lo, o);
+        const long long hi2 = __shfl_down_sync(0xffffffffu, hi, o);
+        const unsigned long long s = lo + lo2;
+        hi += hi2 + (s < lo ? 1 : 0);
+        lo = s;
+    }
+    if ((threadIdx.x & 31) == 0) fx_add(warp_ke_slot(), Fx128{lo, hi});
+}
+
+// Flush the warp's statistics into a ledger and its kinetic-energy accumulator (lo, hi words);
+// every lane calls it.  Integer sums only, so the totals do not depend on the schedule.
+__device__ __forceinline__ void warp_stats_flush(PushStats& c, LedgerDev* L, unsigned long long* ke_acc)
+{
+    unsigned long long v[4] = {c.nsub, c.nlost, c.nhit, c.nact};
+    for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (v[0]) atomicAdd(&L->substeps, v[0]);
+        if (v[1]) atomicAdd(&L->lost_events, v[1]);
+        if (v[2]) atomicAdd(&L->mcc_hits, v[2]);
+        if (v[3]) atomicAdd(&L->active, v[3]);
+        Fx128& k = warp_ke_slot();
+        fx_atomic_add(ke_acc, ke_acc + 1, k);
+        k = Fx128{0ull, 0ll};
+    }
+    __syncwarp();
+    c = PushStats{0.0, 0ull, 0ull, 0ull, 0ull};
+}
+
+// next 32-particle chunk of a launch's work counter (the same value in every lane)
+__device__ __forceinline__ unsigned next_chunk(unsigned* ctr)
+{
+    unsigned g = 0;
+    if ((threadIdx.x & 31) == 0) g = atomicAdd(ctr, 1u);
+    return __shfl_sync(0xffffffffu, g, 0);
+}
 
 // warp-aggregated append to a deferred list; every lane of the warp calls it
 __device__ __forceinline__ unsigned warp_append(bool want, unsigned* cnt)
@@ -371,41 +440,6 @@ __device__ __forceinline__ unsigned warp_append(bool want, unsigned* cnt)
         base = __shfl_sync(0xffffffffu, base, leader);
     }
     return base + (unsigned)__popc(m & ((1u << lane) - 1u));
-}
-
-// block reduction of the push statistics in a fixed order (deterministic)
-__device__ __forceinline__ void block_stats(const PushStats& c, LedgerDev* L, double* ke_part)
-{
-    __shared__ double sk[8];
-    __shared__ unsigned long long sc[4][8];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    double ke = c.ke_sum;
-    unsigned long long v[4] = {c.nsub, c.nlost, c.nhit, c.nact};
-    for (int o = 16; o > 0; o >>= 1) {
-        ke += __shfl_down_sync(0xffffffffu, ke, o);
-#pragma unroll
-        for (int k = 0; k < 4; ++k) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
-    }
-    if (lane == 0) {
-        sk[warp] = ke;
-#pragma unroll
-        for (int k = 0; k < 4; ++k) sc[k][warp] = v[k];
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double s = 0.0;
-        unsigned long long a[4] = {0, 0, 0, 0};
-        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
-            s += sk[w];
-#pragma unroll
-            for (int k = 0; k < 4; ++k) a[k] += sc[k][w];
-        }
-        ke_part[blockIdx.x] += s;
-        if (a[0]) atomicAdd(&L->substeps, a[0]);
-        if (a[1]) atomicAdd(&L->lost_events, a[1]);
-        if (a[2]) atomicAdd(&L->mcc_hits, a[2]);
-        if (a[3]) atomicAdd(&L->active, a[3]);
-    }
 }
 
 constexpr int kCap1 = 2;   // sub-steps every particle gets in pass 1

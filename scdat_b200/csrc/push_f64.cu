@@ -177,7 +177,7 @@ __device__ __forceinline__ void finish_d(const MeshView& M, const ParticleStore&
         ++c.nlost;
         tet_out = resolve_lost(M, S, pp, L, f.px, f.py, f.pz, ke, f.cur);
     }
-    c.ke_sum += ke;  // updateStatistics counts every stored particle (PICCycle.cpp:941-966)
+    c.ke += ke;  // updateStatistics counts every stored particle (PICCycle.cpp:941-966)
     if (tet_out >= 0) {
         ++c.nact;
         if (pp.do_mcc && S.mcc_enabled && mcc_elastic(S, pp, P.id[i], f.vx, f.vy, f.vz)) ++c.nhit;
@@ -203,14 +203,15 @@ __device__ __forceinline__ void defer_store_d(const ParticleStore& P, const Defe
 __global__ void __launch_bounds__(256) k_push_f64(const __grid_constant__ MeshView M, ParticleStore P,
     const __grid_constant__ SpeciesDev S, const __grid_constant__ PushParams pp,
                                                   DeferList D, ChargeAcc A,
-                                                  LedgerDev* L, double* ke_part)
+                                                  LedgerDev* L, unsigned long long* ke_acc, unsigned* ctr)
 {
     const int64_t n = *P.count;
     PushStats c{0.0, 0ull, 0ull, 0ull, 0ull};
     const int lane = threadIdx.x & 31;
-    const int64_t gwarp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t base = gwarp * 32; base < n; base += nwarps * 32) {
+    warp_stats_begin();
+    for (;;) {
+        const int64_t base = (int64_t)next_chunk(ctr) * 32;
+        if (base >= n) break;
         const int64_t i = base + lane;
         int st = -1;
         FlightD f;
@@ -219,7 +220,7 @@ __global__ void __launch_bounds__(256) k_push_f64(const __grid_constant__ MeshVi
             f.vx = P.vx[i]; f.vy = P.vy[i]; f.vz = P.vz[i];
             if (t0 <= kTetAbsorbed) {
                 // updateStatistics sums every particle the container still holds (PICCycle.cpp:941-966)
-                c.ke_sum += 0.5 * S.m * (f.vx * f.vx + f.vy * f.vy + f.vz * f.vz);
+                c.ke += 0.5 * S.m * (f.vx * f.vx + f.vy * f.vy + f.vz * f.vz);
             } else {
                 f.px = P.x[i]; f.py = P.y[i]; f.pz = P.z[i];
                 f.vstart = sqrt(f.vx * f.vx + f.vy * f.vy + f.vz * f.vz);
@@ -241,22 +242,25 @@ __global__ void __launch_bounds__(256) k_push_f64(const __grid_constant__ MeshVi
             if (st == kCapped) st = advance_d(M, S, pp, f, 0x7fffffff, A, c.nsub);
             finish_d(M, P, S, pp, L, i, f, st, c);
         }
+        warp_chunk_end(c);
     }
-    block_stats(c, L, ke_part);
+    warp_stats_flush(c, L, ke_acc);
 }
 
 // Passes 2 and 3 over a deferred list (see k_push_mixed_more).
 __global__ void __launch_bounds__(256) k_push_f64_more(const __grid_constant__ MeshView M, ParticleStore P,
     const __grid_constant__ SpeciesDev S, const __grid_constant__ PushParams pp,
-                                                       DeferList Din, DeferList Dout, int cap, ChargeAcc A, LedgerDev* L, double* ke_part)
+                                                       DeferList Din, DeferList Dout, int cap, ChargeAcc A, LedgerDev* L,
+                                                       unsigned long long* ke_acc, unsigned* ctr)
 {
     const int64_t n = (int64_t)min(*Din.count, Din.cap);
     PushStats c{0.0, 0ull, 0ull, 0ull, 0ull};
     const int lane = threadIdx.x & 31;
-    const int64_t gwarp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     const bool chain = Dout.count != nullptr;
-    for (int64_t base = gwarp * 32; base < n; base += nwarps * 32) {
+    warp_stats_begin();
+    for (;;) {
+        const int64_t base = (int64_t)next_chunk(ctr) * 32;
+        if (base >= n) break;
         const int64_t e = base + lane;
         int st = -1;
         FlightD f;
@@ -278,8 +282,9 @@ __global__ void __launch_bounds__(256) k_push_f64_more(const __grid_constant__ M
             if (st == kCapped) st = advance_d(M, S, pp, f, 0x7fffffff, A, c.nsub);
             finish_d(M, P, S, pp, L, i, f, st, c);
         }
+        warp_chunk_end(c);
     }
-    block_stats(c, L, ke_part);
+    warp_stats_flush(c, L, ke_acc);
 }
 
 // Standalone MCC pass (executeBackgroundMccStep, CollisionPicAdapter.cpp:338-434).
@@ -315,13 +320,13 @@ __global__ void k_refresh_erec(int64_t T, const int4* __restrict__ tet, const do
 }
 
 void launch_push_f64(const MeshView& M, const ParticleStore& P, const SpeciesDev& S, const PushParams& pp,
-                     const DeferList& D1, const DeferList& D2, ChargeAcc A,
-                     LedgerDev* L, double* ke_part, int grid, cudaStream_t st)
+                     const DeferList& D1, const DeferList& D2, ChargeAcc A, LedgerDev* L, unsigned long long* ke_acc,
+                     unsigned* ctr, int grid, cudaStream_t st)
 {
-    k_push_f64<<<grid, 256, 0, st>>>(M, P, S, pp, D1, A, L, ke_part);
-    k_push_f64_more<<<grid, 256, 0, st>>>(M, P, S, pp, D1, D2, kCap2, A, L, ke_part);
+    k_push_f64<<<grid, 256, 0, st>>>(M, P, S, pp, D1, A, L, ke_acc, ctr);
+    k_push_f64_more<<<grid, 256, 0, st>>>(M, P, S, pp, D1, D2, kCap2, A, L, ke_acc, ctr + 1);
     DeferList none{};
-    k_push_f64_more<<<grid, 256, 0, st>>>(M, P, S, pp, D2, none, 0, A, L, ke_part);
+    k_push_f64_more<<<grid, 256, 0, st>>>(M, P, S, pp, D2, none, 0, A, L, ke_acc, ctr + 2);
 }
 
 void launch_mcc_f64(const ParticleStore& P, const SpeciesDev& S, const PushParams& pp, LedgerDev* L, int grid,

@@ -334,7 +334,7 @@ __device__ __forceinline__ void finish_f(const MeshView& M, const ParticleStore&
             f.rx = (float)px; f.ry = (float)py; f.rz = (float)pz;
         }
     }
-    c.ke_sum += ke;
+    c.ke += ke;
     if (tet_out >= 0) {
         ++c.nact;
         if (pp.do_mcc && S.mcc_enabled && mcc_elastic(S, pp, P.id[i], dvx, dvy, dvz)) {
@@ -374,7 +374,7 @@ __device__ __forceinline__ void push1_warp(const MeshView& M, const ParticleStor
         if (f.cur <= kTetAbsorbed) {
             // updateStatistics sums every particle the container still holds (PICCycle.cpp:941-966)
             double ux = f.vx, uy = f.vy, uz = f.vz;
-            c.ke_sum += 0.5 * S.m * (ux * ux + uy * uy + uz * uz);
+            c.ke += 0.5 * S.m * (ux * ux + uy * uy + uz * uz);
         } else {
             f.rx = P.xf[i]; f.ry = P.yf[i]; f.rz = P.zf[i];
             f.vstart = sqrtf(f.vx * f.vx + f.vy * f.vy + f.vz * f.vz);
@@ -403,6 +403,7 @@ __device__ __forceinline__ void push1_warp(const MeshView& M, const ParticleStor
         if (st == kCapped) st = advance_f(M, S, pp, f, 0x7fffffff, A, c.nsub);
         finish_f(M, P, S, pp, L, i, f, st, c);
     }
+    warp_chunk_end(c);
 }
 
 // Passes 2 and 3 for entries [base, base + 32) of list Din (up to `cap` sub-steps, then
@@ -434,40 +435,48 @@ __device__ __forceinline__ void push_more_warp(const MeshView& M, const Particle
         if (st == kCapped) st = advance_f(M, S, pp, f, 0x7fffffff, A, c.nsub);
         finish_f(M, P, S, pp, L, i, f, st, c);
     }
+    warp_chunk_end(c);
 }
 
-// Pass 1: every stored particle.
+// Pass 1: every stored particle.  Warps take 32-particle chunks from the launch's work
+// counter until none are left, so no warp idles while another still has work.
 __global__ void __launch_bounds__(256, 4) k_push_mixed(const __grid_constant__ MeshView M, ParticleStore P,
-    const __grid_constant__ SpeciesDev S, const __grid_constant__ PushParams pp,
-                                                    DeferList D, ChargeAcc A,
-                                                    LedgerDev* L, double* ke_part)
+                                                    const __grid_constant__ SpeciesDev S,
+                                                    const __grid_constant__ PushParams pp, DeferList D, ChargeAcc A,
+                                                    LedgerDev* L, unsigned long long* ke_acc, unsigned* ctr)
 {
     const int64_t n = *P.count;
     PushStats c{0.0, 0ull, 0ull, 0ull, 0ull};
-    const int64_t gwarp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t base = gwarp * 32; base < n; base += nwarps * 32) push1_warp(M, P, S, pp, D, A, L, base, n, c);
-    block_stats(c, L, ke_part);
+    warp_stats_begin();
+    for (;;) {
+        const int64_t base = (int64_t)next_chunk(ctr) * 32;
+        if (base >= n) break;
+        push1_warp(M, P, S, pp, D, A, L, base, n, c);
+    }
+    warp_stats_flush(c, L, ke_acc);
 }
 
 // Passes 2 and 3.
 __global__ void __launch_bounds__(256, 4) k_push_mixed_more(const __grid_constant__ MeshView M, ParticleStore P,
-    const __grid_constant__ SpeciesDev S, const __grid_constant__ PushParams pp,
-                                                         DeferList Din, DeferList Dout, int cap,
-                                                         ChargeAcc A,
-                                                         LedgerDev* L, double* ke_part)
+                                                         const __grid_constant__ SpeciesDev S,
+                                                         const __grid_constant__ PushParams pp, DeferList Din,
+                                                         DeferList Dout, int cap, ChargeAcc A, LedgerDev* L,
+                                                         unsigned long long* ke_acc, unsigned* ctr)
 {
     const int64_t n = (int64_t)min(*Din.count, Din.cap);
     PushStats c{0.0, 0ull, 0ull, 0ull, 0ull};
-    const int64_t gwarp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t base = gwarp * 32; base < n; base += nwarps * 32)
+    warp_stats_begin();
+    for (;;) {
+        const int64_t base = (int64_t)next_chunk(ctr) * 32;
+        if (base >= n) break;
         push_more_warp(M, P, S, pp, Din, Dout, cap, A, L, base, n, c);
-    block_stats(c, L, ke_part);
+    }
+    warp_stats_flush(c, L, ke_acc);
 }
 
 // ---- batched step: all (scenario, species) jobs in one launch per pass -----------------
-__global__ void k_batch_prefix(const PushJob* __restrict__ jobs, int njobs, int pass, int64_t* __restrict__ pre)
+__global__ void k_batch_prefix(const PushJob* __restrict__ jobs, int njobs, int pass, int64_t* __restrict__ pre,
+                               unsigned* __restrict__ ctr)
 {
     __shared__ int64_t cnt[kMaxBatchJobs];
     for (int j = threadIdx.x; j < njobs; j += blockDim.x) {
@@ -479,7 +488,7 @@ __global__ void k_batch_prefix(const PushJob* __restrict__ jobs, int njobs, int 
             n = min((int64_t)*J.D1.count, (int64_t)J.D1.cap);
         else
             n = min((int64_t)*J.D2.count, (int64_t)J.D2.cap);
-        cnt[j] = (n + 255) / 256;
+        cnt[j] = (n + 31) / 32;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -489,24 +498,27 @@ __global__ void k_batch_prefix(const PushJob* __restrict__ jobs, int njobs, int 
             a += cnt[j];
         }
         pre[njobs] = a;
+        ctr[pass - 1] = 0u;
     }
 }
 
-// Pass `pass` (1, 2 or 3) of every job.  Chunk g of the global index belongs to the job j
-// with pre[j] <= g < pre[j + 1]; a block flushes its statistics into a job's ledger when it
-// moves on to the next job.
+// Pass `pass` (1, 2 or 3) of every job.  Warps take 32-particle chunks g of the global index
+// from the pass's work counter; chunk g belongs to the job j with pre[j] <= g < pre[j + 1], and a
+// warp flushes its statistics into a job's ledger when it moves on to another job.
 template <int PASS>
 __global__ void __launch_bounds__(256, 4) k_push_mixed_batch(const PushJob* __restrict__ jobs, int njobs,
-                                                          const int64_t* __restrict__ pre)
+                                                          const int64_t* __restrict__ pre, unsigned* __restrict__ ctr)
 {
     __shared__ int64_t spre[kMaxBatchJobs + 1];
     for (int j = threadIdx.x; j <= njobs; j += blockDim.x) spre[j] = pre[j];
     __syncthreads();
     const int64_t total = spre[njobs];
     PushStats c{0.0, 0ull, 0ull, 0ull, 0ull};
+    warp_stats_begin();
     int cur = -1;
-    const int warp = threadIdx.x >> 5;
-    for (int64_t g = blockIdx.x; g < total; g += gridDim.x) {
+    for (;;) {
+        const int64_t g = (int64_t)next_chunk(ctr + PASS - 1);
+        if (g >= total) break;
         int lo = 0, hi = njobs;  // spre[lo] <= g < spre[hi]
         while (hi - lo > 1) {
             const int mid = (lo + hi) >> 1;
@@ -516,14 +528,11 @@ __global__ void __launch_bounds__(256, 4) k_push_mixed_batch(const PushJob* __re
                 hi = mid;
         }
         if (lo != cur) {
-            if (cur >= 0) {
-                block_stats(c, jobs[cur].L, jobs[cur].ke_part);
-                c = PushStats{0.0, 0ull, 0ull, 0ull, 0ull};
-            }
+            if (cur >= 0) warp_stats_flush(c, jobs[cur].L, jobs[cur].ke_acc);
             cur = lo;
         }
         const PushJob& J = jobs[cur];
-        const int64_t base = (g - spre[cur]) * 256 + warp * 32;
+        const int64_t base = (g - spre[cur]) * 32;
         if (PASS == 1) {
             push1_warp(J.M, J.P, J.S, J.pp, J.D1, J.A, J.L, base, *J.P.count, c);
         } else if (PASS == 2) {
@@ -534,7 +543,7 @@ __global__ void __launch_bounds__(256, 4) k_push_mixed_batch(const PushJob* __re
             push_more_warp(J.M, J.P, J.S, J.pp, J.D2, DeferList{}, 0, J.A, J.L, base, n, c);
         }
     }
-    if (cur >= 0) block_stats(c, jobs[cur].L, jobs[cur].ke_part);
+    if (cur >= 0) warp_stats_flush(c, jobs[cur].L, jobs[cur].ke_acc);
 }
 
 // nodal E -> tet records of every scenario (tets block map)
@@ -602,13 +611,13 @@ __global__ void k_refresh_trec(int64_t T, const int4* __restrict__ tet, const do
 }
 
 void launch_push_mixed(const MeshView& M, const ParticleStore& P, const SpeciesDev& S, const PushParams& pp,
-                       const DeferList& D1, const DeferList& D2, ChargeAcc A,
-                       LedgerDev* L, double* ke_part, int grid, cudaStream_t st)
+                       const DeferList& D1, const DeferList& D2, ChargeAcc A, LedgerDev* L,
+                       unsigned long long* ke_acc, unsigned* ctr, int grid, cudaStream_t st)
 {
-    k_push_mixed<<<grid, 256, 0, st>>>(M, P, S, pp, D1, A, L, ke_part);
-    k_push_mixed_more<<<grid, 256, 0, st>>>(M, P, S, pp, D1, D2, kCap2, A, L, ke_part);
+    k_push_mixed<<<grid, 256, 0, st>>>(M, P, S, pp, D1, A, L, ke_acc, ctr);
+    k_push_mixed_more<<<grid, 256, 0, st>>>(M, P, S, pp, D1, D2, kCap2, A, L, ke_acc, ctr + 1);
     DeferList none{};
-    k_push_mixed_more<<<grid, 256, 0, st>>>(M, P, S, pp, D2, none, 0, A, L, ke_part);
+    k_push_mixed_more<<<grid, 256, 0, st>>>(M, P, S, pp, D2, none, 0, A, L, ke_acc, ctr + 2);
 }
 
 void launch_mcc_mixed(const ParticleStore& P, const SpeciesDev& S, const PushParams& pp, LedgerDev* L, int grid,
@@ -629,20 +638,21 @@ void launch_from_mixed(const MeshView& M, int64_t n, const ParticleStore& P, dou
     k_from_mixed<<<148 * 4, 256, 0, st>>>(M, n, P, x, y, z, vx, vy, vz);
 }
 
-void launch_batch_prefix(const PushJob* jobs, int njobs, int pass, int64_t* chunk_prefix, cudaStream_t st)
+void launch_batch_prefix(const PushJob* jobs, int njobs, int pass, int64_t* chunk_prefix, unsigned* ctr,
+                         cudaStream_t st)
 {
-    k_batch_prefix<<<1, 1024, 0, st>>>(jobs, njobs, pass, chunk_prefix);
+    k_batch_prefix<<<1, 1024, 0, st>>>(jobs, njobs, pass, chunk_prefix, ctr);
 }
 
-void launch_push_mixed_batch(const PushJob* jobs, int njobs, const int64_t* chunk_prefix, int pass, int grid,
-                             cudaStream_t st)
+void launch_push_mixed_batch(const PushJob* jobs, int njobs, const int64_t* chunk_prefix, unsigned* ctr, int pass,
+                             int grid, cudaStream_t st)
 {
     if (pass == 1)
-        k_push_mixed_batch<1><<<grid, 256, 0, st>>>(jobs, njobs, chunk_prefix);
+        k_push_mixed_batch<1><<<grid, 256, 0, st>>>(jobs, njobs, chunk_prefix, ctr);
     else if (pass == 2)
-        k_push_mixed_batch<2><<<grid, 256, 0, st>>>(jobs, njobs, chunk_prefix);
+        k_push_mixed_batch<2><<<grid, 256, 0, st>>>(jobs, njobs, chunk_prefix, ctr);
     else
-        k_push_mixed_batch<3><<<grid, 256, 0, st>>>(jobs, njobs, chunk_prefix);
+        k_push_mixed_batch<3><<<grid, 256, 0, st>>>(jobs, njobs, chunk_prefix, ctr);
 }
 
 void launch_batch_refresh_trec(const FieldJob* jobs, const BlockMap& tets, cudaStream_t st)

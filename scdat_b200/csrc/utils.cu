@@ -32,24 +32,40 @@ void launch_sort_keys(int64_t n, const int32_t* tet, uint32_t inactive_key, uint
     k_sort_keys<<<grid, 256, 0, st>>>(n, tet, inactive_key + 1u, keys, vals, reinterpret_cast<unsigned long long*>(active));
 }
 
+// One pass of the re-sort permutation over a species' whole store: the six coordinate arrays,
+// the tet ids and the particle ids move together, and only the active prefix (the particles the
+// sort keeps) is written.
 template <typename T>
-__global__ void k_gather(int64_t n, const uint32_t* __restrict__ perm, const T* __restrict__ in, T* __restrict__ out)
+__global__ void k_gather_store(const int64_t* __restrict__ active, const uint32_t* __restrict__ perm,
+                               GatherArrays<T> in, GatherArrays<T> out)
 {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        out[i] = in[perm[i]];
+    const int64_t n = *active;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t j = __ldg(perm + i);
+        T v[6];
+#pragma unroll
+        for (int a = 0; a < 6; ++a) v[a] = __ldg(in.v[a] + j);
+        const int32_t t = __ldg(in.tet + j);
+        const uint32_t id = __ldg(in.id + j);
+#pragma unroll
+        for (int a = 0; a < 6; ++a) out.v[a][i] = v[a];
+        out.tet[i] = t;
+        out.id[i] = id;
+    }
 }
 
 template <typename T>
-void launch_gather(int64_t n, const uint32_t* perm, const T* in, T* out, cudaStream_t st)
+void launch_gather_store(int64_t n, const int64_t* active, const uint32_t* perm, const GatherArrays<T>& in,
+                         const GatherArrays<T>& out, cudaStream_t st)
 {
     int grid = (int)std::min<int64_t>((n + 255) / 256, 148 * 16);
     if (grid < 1) grid = 1;
-    k_gather<T><<<grid, 256, 0, st>>>(n, perm, in, out);
+    k_gather_store<T><<<grid, 256, 0, st>>>(active, perm, in, out);
 }
-template void launch_gather<double>(int64_t, const uint32_t*, const double*, double*, cudaStream_t);
-template void launch_gather<float>(int64_t, const uint32_t*, const float*, float*, cudaStream_t);
-template void launch_gather<int32_t>(int64_t, const uint32_t*, const int32_t*, int32_t*, cudaStream_t);
-template void launch_gather<uint32_t>(int64_t, const uint32_t*, const uint32_t*, uint32_t*, cudaStream_t);
+template void launch_gather_store<double>(int64_t, const int64_t*, const uint32_t*, const GatherArrays<double>&,
+                                          const GatherArrays<double>&, cudaStream_t);
+template void launch_gather_store<float>(int64_t, const int64_t*, const uint32_t*, const GatherArrays<float>&,
+                                         const GatherArrays<float>&, cudaStream_t);
 
 __global__ void k_scatter_values(int64_t n, const int64_t* __restrict__ idx, const double* __restrict__ v, double* dst)
 {
@@ -106,6 +122,94 @@ __global__ void k_seed_box(const int32_t* __restrict__ hex_ijk, int64_t ncell, i
         P.tet[k] = tet;
         P.id[k] = (uint32_t)id;
     }
+}
+
+// ParticleSource sampling on a tet mesh: n_per_tet particles in each listed tet (all tets when
+// tets == nullptr), positions uniform in the tet from Dirichlet(1,1,1,1) barycentric weights
+// w_k = e_k / sum e, e_k = -log(max(1e-12, u_k)) (samplePointInTetra,
+// Toolkit/Surface Charging/src/PicMccSurfaceCurrentSampler.cpp:270-287), velocities a drifting
+// Maxwellian by Box-Muller; draws from Philox(seed) keyed by id = (tet_index * S + s) * n_per_tet + k.
+__global__ void k_seed_tets(const int32_t* __restrict__ tets, int64_t ntet, int32_t per_tet, int32_t S_total, int32_t s,
+                            double sigma, double dx, double dy, double dz, uint64_t seed, ParticleStore P, int mixed,
+                            MeshView M)
+{
+    const int64_t n = ntet * per_tet;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t c = k / per_tet, j = k % per_tet;
+        const int tet = tets ? tets[c] : (int)c;
+        const uint64_t id = ((uint64_t)c * S_total + s) * per_tet + j;
+        double u[4], g[4];
+        uniform2(seed, id, 0u, 0u, u[0], u[1]);
+        uniform2(seed, id, 0u, 1u, u[2], u[3]);
+        uniform2(seed, id, 0u, 4u, g[0], g[1]);
+        uniform2(seed, id, 0u, 5u, g[2], g[3]);
+        double e[4], es = 0.0;
+        for (int q = 0; q < 4; ++q) {
+            e[q] = -log(fmax(1.0e-12, u[q]));
+            es += e[q];
+        }
+        const int4 tn = M.tet[tet];
+        const int nd[4] = {tn.x, tn.y, tn.z, tn.w};
+        double x = 0.0, y = 0.0, z = 0.0;
+        for (int q = 0; q < 4; ++q) {
+            const double w = e[q] / es;
+            x += w * M.xyz[3 * nd[q]];
+            y += w * M.xyz[3 * nd[q] + 1];
+            z += w * M.xyz[3 * nd[q] + 2];
+        }
+        const double r1 = sqrt(-2.0 * log(g[0])), r2 = sqrt(-2.0 * log(g[2]));
+        const double tp = 6.283185307179586476925286766559;
+        const double vx = dx + sigma * r1 * cos(tp * g[1]), vy = dy + sigma * r1 * sin(tp * g[1]),
+                     vz = dz + sigma * r2 * cos(tp * g[3]);
+        if (mixed) {
+            P.xf[k] = (float)(x - M.xyz[3 * nd[0]]);
+            P.yf[k] = (float)(y - M.xyz[3 * nd[0] + 1]);
+            P.zf[k] = (float)(z - M.xyz[3 * nd[0] + 2]);
+            P.vxf[k] = (float)vx; P.vyf[k] = (float)vy; P.vzf[k] = (float)vz;
+        } else {
+            P.x[k] = x; P.y[k] = y; P.z[k] = z;
+            P.vx[k] = vx; P.vy[k] = vy; P.vz[k] = vz;
+        }
+        P.tet[k] = tet;
+        P.id[k] = (uint32_t)id;
+    }
+}
+
+void launch_seed_tets(const int32_t* tets, int64_t ntet, int32_t per_tet, int32_t S_total, int32_t s, double sigma,
+                      const double drift[3], uint64_t seed, const ParticleStore& P, bool mixed, const MeshView& M,
+                      cudaStream_t st)
+{
+    k_seed_tets<<<148 * 8, 256, 0, st>>>(tets, ntet, per_tet, S_total, s, sigma, drift[0], drift[1], drift[2], seed, P,
+                                         mixed ? 1 : 0, M);
+}
+
+// Per-layer particle moments for the z-layer profile: weight and weight * v^2 of one species
+// in n_layers equal slabs of [z0, z1] (double atomics: output only).
+__global__ void k_layer_moments(ParticleStore P, int64_t n, int mixed, MeshView M, double z0, double z1, int n_layers,
+                                double* __restrict__ cnt, double* __restrict__ v2)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int t = P.tet[i];
+        if (t < 0) continue;
+        double z, vx, vy, vz;
+        if (mixed) {
+            z = M.xyz[3 * __ldg(&M.tet[t].x) + 2] + (double)P.zf[i];
+            vx = P.vxf[i]; vy = P.vyf[i]; vz = P.vzf[i];
+        } else {
+            z = P.z[i];
+            vx = P.vx[i]; vy = P.vy[i]; vz = P.vz[i];
+        }
+        int l = (int)((z - z0) / (z1 - z0) * n_layers);
+        l = l < 0 ? 0 : (l >= n_layers ? n_layers - 1 : l);
+        atomicAdd(cnt + l, 1.0);
+        atomicAdd(v2 + l, vx * vx + vy * vy + vz * vz);
+    }
+}
+
+void launch_layer_moments(const ParticleStore& P, int64_t n, bool mixed, const MeshView& M, double z0, double z1,
+                          int n_layers, double* cnt, double* v2, cudaStream_t st)
+{
+    k_layer_moments<<<148 * 4, 256, 0, st>>>(P, n, mixed ? 1 : 0, M, z0, z1, n_layers, cnt, v2);
 }
 
 void launch_seed_box(const int32_t* hex_ijk, int64_t ncell, int32_t ppc, int32_t S_total, int32_t s, double h,

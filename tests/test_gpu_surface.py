@@ -152,3 +152,49 @@ def test_sample_with_derivative_matches_single_windows(lib):
             d.close()
     assert m["valid"] == 1 and np.isfinite(m["current_derivative_a_per_m2_per_v"])
     assert abs(m["net_collection_a_per_m2"] - nets[1]) <= 0.05 * abs(nets[1])
+
+
+def test_tet_injection_matches_oracle_and_exports(lib, tmp_path):
+    """scdat_seed_tet_particles against the restated samplePointInTetra draws (FP64: positions
+    to rounding, every particle inside its tet), and the columnar CSV outputs."""
+    mesh = O.kuhn_box((4, 3, 5), 0.05, body=((1, 2), (1, 2), (1, 3)), bias=-3.0)
+    sp = O.plasma_species(1e10, 2.0, 1.0, 0.05, 3)
+    dom = gpu_domain(mesh, 2e-8, face_bc=(1,) * 6)
+    dom.set_species(sp)
+    tets = np.arange(0, mesh.T, 3, dtype=np.int32)
+    sigma = np.sqrt(2.0 * O.QE / O.ME)
+    dom.seed_tets(0, 5, 2.0, 77, tets=tets, drift=(1e4, 0.0, -2e4))
+    dom.seed_tets(1, 2, 1.0, 77)
+    g = dom.get_particles(0)
+    x, v, t = O.seed_tets(mesh, 0, 2, 5, sigma, 77, tets=tets, drift=(1e4, 0.0, -2e4))
+    order = np.argsort(g["id"])
+    assert np.array_equal(g["tet"][order], t)
+    assert np.abs(g["x"][order] - x).max() <= 1e-15 * np.abs(x).max() * 10
+    assert rel_err(g["v"][order], v) < 1e-14
+    # every point inside its tet
+    for k in range(0, len(t), 7):
+        assert orc_inside(mesh, t[k], x[k])
+    assert dom.count(1) == 2 * mesh.T
+    dom.set_potential(mesh.phi_bc)
+    dom.step(2)
+    dom.export_nodes(tmp_path / "nodes.csv")
+    dom.export_layer_profile(tmp_path / "layers.csv", 5)
+    rho, phi, E = dom.fields()
+    dom.close()
+    head = open(tmp_path / "nodes.csv").readline().strip().split(",")
+    assert head == ["node", "charge_c", "electric_field_x_v_per_m", "electric_field_y_v_per_m",
+                    "electric_field_z_v_per_m", "potential_v", "x_m", "y_m", "z_m"]
+    tab = np.loadtxt(tmp_path / "nodes.csv", delimiter=",", skiprows=1)
+    assert tab.shape == (mesh.N, 9)
+    np.testing.assert_allclose(tab[:, 5], phi, rtol=1e-8, atol=1e-12)
+    lay = np.loadtxt(tmp_path / "layers.csv", delimiter=",", skiprows=1)
+    assert open(tmp_path / "layers.csv").readline().strip() == (
+        "z_m,electric_field_z_v_per_m,electron_density_m3,electron_temperature_ev,ion_density_m3,potential_v")
+    assert lay.shape == (5, 6) and np.all(lay[:, 2] >= 0) and np.all(np.isfinite(lay))
+
+
+def orc_inside(mesh, t, p):
+    a = mesh.xyz[mesh.tet[t]]
+    T = np.stack([a[1] - a[0], a[2] - a[0], a[3] - a[0]], axis=1)
+    lam = np.linalg.solve(T, p - a[0])
+    return np.all(lam >= -1e-9) and lam.sum() <= 1 + 1e-9
