@@ -254,6 +254,13 @@ SCDAT_API int scdat_solve_field(scdat_ctx* ctx);
 SCDAT_API int scdat_collide(scdat_ctx* ctx);
 SCDAT_API int scdat_compact(scdat_ctx* ctx);
 
+/* Re-sort one species only every `interval` steps instead of every params.sort_interval steps
+ * (no reference counterpart: the reference does not sort).  A species that crosses few tets
+ * per step (ions beside electrons of the same temperature move ~43x slower) stays ordered for
+ * many steps, so sorting it at the electrons' rate costs time and buys nothing.  interval must
+ * be a positive multiple of params.sort_interval, or 0 to follow it. */
+SCDAT_API int scdat_set_species_sort_interval(scdat_ctx* ctx, int32_t species, int32_t interval);
+
 /* PICCycle::getChargeDensity/getPotential/getElectricField (PICCycle.h:79-90); any pointer
  * may be NULL.  rho is nodal charge [C]; E is [n_nodes*3]. */
 SCDAT_API int scdat_get_fields(scdat_ctx* ctx, double* rho, double* phi, double* E);

@@ -84,6 +84,7 @@ EXPORTS = ["scdat_default_params", "scdat_create", "scdat_destroy", "scdat_last_
            "scdat_set_particles", "scdat_seed_box_particles", "scdat_kuhn_box_mesh", "scdat_get_particle_count",
            "scdat_get_particles", "scdat_set_potential", "scdat_set_node_potentials", "scdat_set_electric_field",
            "scdat_set_elastic_mcc", "scdat_step", "scdat_push", "scdat_solve_field", "scdat_collide", "scdat_compact",
+           "scdat_set_species_sort_interval",
            "scdat_get_fields", "scdat_get_species_charge", "scdat_get_ledger", "scdat_reset_ledger",
            "scdat_get_statistics", "scdat_version", "scdat_stream", "scdat_set_timing", "scdat_get_timing",
            "scdat_pcg_csr", "scdat_pcg_csr_noalloc", "scdat_set_charge_density", "scdat_set_dt", "scdat_set_seed",
@@ -153,6 +154,7 @@ def load():
     for f in ("scdat_push", "scdat_solve_field", "scdat_collide", "scdat_compact", "scdat_reset_ledger"):
         getattr(L, f).argtypes = [vp]
     L.scdat_step.argtypes = [vp, C.c_int32]
+    L.scdat_set_species_sort_interval.argtypes = [vp, C.c_int32, C.c_int32]
     L.scdat_get_fields.argtypes = [vp, vp, vp, vp]
     L.scdat_get_species_charge.argtypes = [vp, C.c_int32, vp]
     L.scdat_get_ledger.argtypes = [vp, vp]
@@ -393,6 +395,10 @@ class Domain:
 
     def compact(self):
         self._ck(self.L.scdat_compact(self.h))
+
+    def set_species_sort_interval(self, species, interval):
+        """scdat_set_species_sort_interval: re-sort this species every `interval` steps."""
+        self._ck(self.L.scdat_set_species_sort_interval(self.h, int(species), int(interval)))
 
     def step(self, n=1):
         self._ck(self.L.scdat_step(self.h, n))

@@ -324,6 +324,7 @@ int after_steps(scdat_batch* b, int n)
         const int si = c->prm.sort_interval;
         if (si > 0 && c->steps / si != before / si) {
             for (int s = 0; s < (int)c->species.size(); ++s) {
+                if (!species_sorts_now(c, s)) continue;
                 int rc = do_sort(c, s);
                 if (rc) {
                     b->err = c->err;

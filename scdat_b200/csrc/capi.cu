@@ -415,6 +415,16 @@ int do_surface(scdat_ctx* ctx)
     return SCDAT_OK;
 }
 
+}  // namespace scdat
+
+bool species_sorts_now(const scdat_ctx* ctx, int s)
+{
+    const int si = ctx->species[s].sort_interval > 0 ? ctx->species[s].sort_interval : ctx->prm.sort_interval;
+    return si > 0 && ctx->steps % si == 0;
+}
+
+namespace scdat {
+
 int do_sort(scdat_ctx* ctx, int s)
 {
     SpeciesState& S = ctx->species[s];
@@ -1246,6 +1256,17 @@ SCDAT_API int scdat_collide(scdat_ctx* ctx)
     return SCDAT_OK;
 }
 
+SCDAT_API int scdat_set_species_sort_interval(scdat_ctx* ctx, int32_t species, int32_t interval)
+{
+    if (!ctx) return SCDAT_ERR_ARG;
+    ARG(species >= 0 && species < (int)ctx->species.size(), "species out of range");
+    const int si = ctx->prm.sort_interval;
+    ARG(interval == 0 || (interval > 0 && si > 0 && interval % si == 0),
+        "species sort interval must be 0 or a positive multiple of params.sort_interval");
+    ctx->species[species].sort_interval = interval;
+    return SCDAT_OK;
+}
+
 SCDAT_API int scdat_compact(scdat_ctx* ctx)
 {
     if (!ctx) return SCDAT_ERR_ARG;
@@ -1270,8 +1291,11 @@ SCDAT_API int scdat_step(scdat_ctx* ctx, int32_t n_steps)
         ctx->steps += 1;
         ctx->sim_time += ctx->prm.dt;
         if (ctx->prm.sort_interval > 0 && ctx->steps % ctx->prm.sort_interval == 0) {
-            rc = scdat_compact(ctx);
-            if (rc) return rc;
+            for (int s = 0; s < (int)ctx->species.size(); ++s) {
+                if (!species_sorts_now(ctx, s)) continue;
+                rc = do_sort(ctx, s);
+                if (rc) return rc;
+            }
         }
     }
     CK(cudaStreamSynchronize(ctx->st));

@@ -15,6 +15,12 @@
 
 using namespace scdat;
 
+struct SpeciesState;
+struct scdat_ctx;
+// true when species s re-sorts at the context's current step count (a multiple of the
+// context's sort interval)
+bool species_sorts_now(const scdat_ctx* ctx, int s);
+
 template <typename T>
 struct DBuf {
     T* p = nullptr;
@@ -55,6 +61,7 @@ struct SpeciesState {
     scdat_elastic mcc{};
     int64_t cap = 0;
     int64_t n = 0;  // host view of the stored count (updated on set/compact)
+    int sort_interval = 0;  // 0: the context's params.sort_interval
     DBuf<double> x, y, z, vx, vy, vz;
     DBuf<float> xf, yf, zf, vxf, vyf, vzf;
     DBuf<int32_t> tet;

@@ -322,8 +322,16 @@ __device__ inline bool mcc_elastic(const SpeciesDev& S, const PushParams& pp, ui
         double p = fmin(fmax(nu * pp.dt, 0.0), 1.0);
         hit = (u0 < p) && !(u1 >= p);
     } else {
-        double p = 1.0 - exp(-nu * pp.dt);
-        hit = u0 < p;
+        // p = 1 - exp(-x) <= x, and the computed p exceeds x by at most 2^-52 (exp within one
+        // ulp near 1, the subtraction exact), so u0 >= x + 1e-15 already decides "no hit"
+        // without the exponential; otherwise p is evaluated as before
+        const double x = nu * pp.dt;
+        if (u0 >= x + 1e-15) {
+            hit = false;
+        } else {
+            double p = 1.0 - exp(-x);
+            hit = u0 < p;
+        }
     }
     if (!hit) return false;
     double w0, w1;
@@ -354,38 +362,46 @@ struct DeferList {
 
 enum { kDone = 0, kCapped = 1, kLost = 2 };
 
-// Per-lane push statistics.  ke is the kinetic energy of the lane's particle in the current
-// 32-particle chunk; warp_chunk_end folds it, converted to the exact fixed point, into the
-// warp's total, so the energy sum does not depend on which warp took which chunk.
+// Per-lane push statistics of the current 32-particle chunk (one particle per lane): its
+// kinetic energy, its sub-steps and its events (kEvLost | kEvActive | kEvHit).
+// warp_chunk_end folds them into the warp's totals in shared memory (kinetic energy as exact
+// fixed point), so the lanes carry only a few registers and the sums do not depend on which
+// warp took which chunk.
 struct PushStats {
     double ke;
-    unsigned long long nsub, nlost, nhit, nact;
+    unsigned nsub, ev;
 };
+enum : unsigned { kEvLost = 1u, kEvActive = 2u, kEvHit = 4u };
 
 // Kinetic energy accumulates as 128-bit fixed point with a unit of 2^-60 J: a 1 eV particle is
 // resolved to 1e-19 of itself and the sum can reach 8 J.
 constexpr double kKeInvUnit = 1152921504606846976.0;  // 2^60
 constexpr double kKeUnit = 8.673617379884035e-19;     // 2^-60
 
-// the warp's fixed-point kinetic-energy total for the kernel (one slot per warp of the block)
-__device__ __forceinline__ Fx128& warp_ke_slot()
+// the warp's totals for the kernel: kinetic energy; sub-steps, lost, MCC hits, active
+struct WarpStats {
+    Fx128 ke;
+    unsigned long long n[4];
+};
+
+__device__ __forceinline__ WarpStats& warp_slot()
 {
-    __shared__ Fx128 slot[32];
+    __shared__ WarpStats slot[32];
     return slot[threadIdx.x >> 5];
 }
 
 // start of a push kernel; every lane calls it
 __device__ __forceinline__ void warp_stats_begin()
 {
-    if ((threadIdx.x & 31) == 0) warp_ke_slot() = Fx128{0ull, 0ll};
+    if ((threadIdx.x & 31) == 0) warp_slot() = WarpStats{Fx128{0ull, 0ll}, {0ull, 0ull, 0ull, 0ull}};
     __syncwarp();
 }
 
-// end of a chunk; every lane calls it: the lanes' energies as fixed point, summed exactly
+// end of a chunk; every lane calls it: energies as fixed point summed exactly, counts by
+// warp reductions and ballots
 __device__ __forceinline__ void warp_chunk_end(PushStats& c)
 {
     const Fx128 v = fx_from_double(c.ke * kKeInvUnit);
-    c.ke = 0.0;
     unsigned long long lo = v.lo;
     long long hi = v.hi;
     for (int o = 16; o > 0; o >>= 1) {
@@ -395,32 +411,44 @@ __device__ __forceinline__ void warp_chunk_end(PushStats& c)
         hi += hi2 + (s < lo ? 1 : 0);
         lo = s;
     }
-    if ((threadIdx.x & 31) == 0) fx_add(warp_ke_slot(), Fx128{lo, hi});
+    const unsigned sub = __reduce_add_sync(0xffffffffu, c.nsub);
+    const unsigned lost = __popc(__ballot_sync(0xffffffffu, c.ev & kEvLost));
+    const unsigned hit = __popc(__ballot_sync(0xffffffffu, c.ev & kEvHit));
+    const unsigned act = __popc(__ballot_sync(0xffffffffu, c.ev & kEvActive));
+    if ((threadIdx.x & 31) == 0) {
+        WarpStats& w = warp_slot();
+        fx_add(w.ke, Fx128{lo, hi});
+        w.n[0] += sub;
+        w.n[1] += lost;
+        w.n[2] += hit;
+        w.n[3] += act;
+    }
+    c = PushStats{0.0, 0u, 0u};
 }
 
-// Flush the warp's statistics into a ledger and its kinetic-energy accumulator (lo, hi words);
-// every lane calls it.  Integer sums only, so the totals do not depend on the schedule.
-__device__ __forceinline__ void warp_stats_flush(PushStats& c, LedgerDev* L, unsigned long long* ke_acc)
+// Flush the warp's totals into a ledger and its kinetic-energy accumulator (lo, hi words);
+// every lane calls it, after warp_chunk_end.  Integer sums only, so the totals do not depend
+// on the schedule.
+__device__ __forceinline__ void warp_stats_flush(LedgerDev* L, unsigned long long* ke_acc)
 {
-    unsigned long long v[4] = {c.nsub, c.nlost, c.nhit, c.nact};
-    for (int o = 16; o > 0; o >>= 1) {
-#pragma unroll
-        for (int k = 0; k < 4; ++k) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
-    }
     if ((threadIdx.x & 31) == 0) {
-        if (v[0]) atomicAdd(&L->substeps, v[0]);
-        if (v[1]) atomicAdd(&L->lost_events, v[1]);
-        if (v[2]) atomicAdd(&L->mcc_hits, v[2]);
-        if (v[3]) atomicAdd(&L->active, v[3]);
-        Fx128& k = warp_ke_slot();
-        fx_atomic_add(ke_acc, ke_acc + 1, k);
-        k = Fx128{0ull, 0ll};
+        WarpStats& w = warp_slot();
+        if (w.n[0]) atomicAdd(&L->substeps, w.n[0]);
+        if (w.n[1]) atomicAdd(&L->lost_events, w.n[1]);
+        if (w.n[2]) atomicAdd(&L->mcc_hits, w.n[2]);
+        if (w.n[3]) atomicAdd(&L->active, w.n[3]);
+        fx_atomic_add(ke_acc, ke_acc + 1, w.ke);
+        w = WarpStats{Fx128{0ull, 0ll}, {0ull, 0ull, 0ull, 0ull}};
     }
     __syncwarp();
-    c = PushStats{0.0, 0ull, 0ull, 0ull, 0ull};
 }
 
-// next 32-particle chunk of a launch's work counter (the same value in every lane)
+// Pass 1 hands out runs of kRun consecutive 32-particle chunks: a warp's next chunk then lies
+// in the tets of its previous one (particles are sorted by tet), so the records it needs are
+// still in L1, and the work counter sees one atomic per 256 particles.
+constexpr int kRun = 8;
+
+// next chunk (or run) of a launch's work counter (the same value in every lane)
 __device__ __forceinline__ unsigned next_chunk(unsigned* ctr)
 {
     unsigned g = 0;

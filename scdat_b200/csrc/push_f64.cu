@@ -93,7 +93,7 @@ struct FlightD {
 // ran in this call.
 __device__ __forceinline__ int advance_d(const MeshView& M, const SpeciesDev& S, const PushParams& pp, FlightD& f,
                                          int cap, ChargeAcc A,
-                                         unsigned long long& nsub)
+                                         unsigned& nsub)
 {
     const double qm = S.qm;
     const double qw = S.q * S.w;
@@ -174,13 +174,13 @@ __device__ __forceinline__ void finish_d(const MeshView& M, const ParticleStore&
     const double ke = 0.5 * S.m * (f.vx * f.vx + f.vy * f.vy + f.vz * f.vz);
     int tet_out = f.cur;
     if (st == kLost) {
-        ++c.nlost;
+        c.ev |= kEvLost;
         tet_out = resolve_lost(M, S, pp, L, f.px, f.py, f.pz, ke, f.cur);
     }
     c.ke += ke;  // updateStatistics counts every stored particle (PICCycle.cpp:941-966)
     if (tet_out >= 0) {
-        ++c.nact;
-        if (pp.do_mcc && S.mcc_enabled && mcc_elastic(S, pp, P.id[i], f.vx, f.vy, f.vz)) ++c.nhit;
+        c.ev |= kEvActive;
+        if (pp.do_mcc && S.mcc_enabled && mcc_elastic(S, pp, P.id[i], f.vx, f.vy, f.vz)) c.ev |= kEvHit;
     }
     P.x[i] = f.px; P.y[i] = f.py; P.z[i] = f.pz;
     P.vx[i] = f.vx; P.vy[i] = f.vy; P.vz[i] = f.vz;
@@ -206,45 +206,48 @@ __global__ void __launch_bounds__(256) k_push_f64(const __grid_constant__ MeshVi
                                                   LedgerDev* L, unsigned long long* ke_acc, unsigned* ctr)
 {
     const int64_t n = *P.count;
-    PushStats c{0.0, 0ull, 0ull, 0ull, 0ull};
+    PushStats c{0.0, 0u, 0u};
     const int lane = threadIdx.x & 31;
     warp_stats_begin();
     for (;;) {
-        const int64_t base = (int64_t)next_chunk(ctr) * 32;
-        if (base >= n) break;
-        const int64_t i = base + lane;
-        int st = -1;
-        FlightD f;
-        if (i < n) {
-            int t0 = P.tet[i];
-            f.vx = P.vx[i]; f.vy = P.vy[i]; f.vz = P.vz[i];
-            if (t0 <= kTetAbsorbed) {
-                // updateStatistics sums every particle the container still holds (PICCycle.cpp:941-966)
-                c.ke += 0.5 * S.m * (f.vx * f.vx + f.vy * f.vy + f.vz * f.vz);
-            } else {
-                f.px = P.x[i]; f.py = P.y[i]; f.pz = P.z[i];
-                f.vstart = sqrt(f.vx * f.vx + f.vy * f.vy + f.vz * f.vz);
-                f.rem = pp.dt;
-                f.it = 0;
-                f.cur = locate(M, f.px, f.py, f.pz, t0);
-                if (f.cur < 0) {
-                    f.cur = 0;  // result.final_element stays 0 (PICParticleAlgorithms.cpp:543,577)
-                    st = kLost;
+        // runs of kRun chunks, as in the mixed form
+        const int64_t b0 = (int64_t)next_chunk(ctr) * (32 * kRun);
+        if (b0 >= n) break;
+        for (int64_t base = b0; base < b0 + 32 * kRun && base < n; base += 32) {
+            const int64_t i = base + lane;
+            int st = -1;
+            FlightD f;
+            if (i < n) {
+                int t0 = P.tet[i];
+                f.vx = P.vx[i]; f.vy = P.vy[i]; f.vz = P.vz[i];
+                if (t0 <= kTetAbsorbed) {
+                    // updateStatistics sums every particle the container still holds (PICCycle.cpp:941-966)
+                    c.ke += 0.5 * S.m * (f.vx * f.vx + f.vy * f.vy + f.vz * f.vz);
                 } else {
-                    st = advance_d(M, S, pp, f, kCap1, A, c.nsub);
+                    f.px = P.x[i]; f.py = P.y[i]; f.pz = P.z[i];
+                    f.vstart = sqrt(f.vx * f.vx + f.vy * f.vy + f.vz * f.vz);
+                    f.rem = pp.dt;
+                    f.it = 0;
+                    f.cur = locate(M, f.px, f.py, f.pz, t0);
+                    if (f.cur < 0) {
+                        f.cur = 0;  // result.final_element stays 0 (PICParticleAlgorithms.cpp:543,577)
+                        st = kLost;
+                    } else {
+                        st = advance_d(M, S, pp, f, kCap1, A, c.nsub);
+                    }
                 }
             }
+            unsigned slot = warp_append(st == kCapped, D.count);
+            if (st == kCapped && slot < D.cap) {
+                defer_store_d(P, D, slot, i, f);
+            } else if (st >= 0) {
+                if (st == kCapped) st = advance_d(M, S, pp, f, 0x7fffffff, A, c.nsub);
+                finish_d(M, P, S, pp, L, i, f, st, c);
+            }
+            warp_chunk_end(c);
         }
-        unsigned slot = warp_append(st == kCapped, D.count);
-        if (st == kCapped && slot < D.cap) {
-            defer_store_d(P, D, slot, i, f);
-        } else if (st >= 0) {
-            if (st == kCapped) st = advance_d(M, S, pp, f, 0x7fffffff, A, c.nsub);
-            finish_d(M, P, S, pp, L, i, f, st, c);
-        }
-        warp_chunk_end(c);
     }
-    warp_stats_flush(c, L, ke_acc);
+    warp_stats_flush(L, ke_acc);
 }
 
 // Passes 2 and 3 over a deferred list (see k_push_mixed_more).
@@ -254,7 +257,7 @@ __global__ void __launch_bounds__(256) k_push_f64_more(const __grid_constant__ M
                                                        unsigned long long* ke_acc, unsigned* ctr)
 {
     const int64_t n = (int64_t)min(*Din.count, Din.cap);
-    PushStats c{0.0, 0ull, 0ull, 0ull, 0ull};
+    PushStats c{0.0, 0u, 0u};
     const int lane = threadIdx.x & 31;
     const bool chain = Dout.count != nullptr;
     warp_stats_begin();
@@ -284,7 +287,7 @@ __global__ void __launch_bounds__(256) k_push_f64_more(const __grid_constant__ M
         }
         warp_chunk_end(c);
     }
-    warp_stats_flush(c, L, ke_acc);
+    warp_stats_flush(L, ke_acc);
 }
 
 // Standalone MCC pass (executeBackgroundMccStep, CollisionPicAdapter.cpp:338-434).

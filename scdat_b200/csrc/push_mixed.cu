@@ -109,12 +109,20 @@ __device__ __forceinline__ void dep_point_f(Fx128 acc[4], bool& any, const float
     any = true;
 }
 
+// Result of a relocation: the new tet (or -1), the offset r and the carried start offset s
+// re-based to its origin.  Returned by value so that the caller's flight state stays in
+// registers across the out-of-line call.
+struct Reloc {
+    int t;
+    float rx, ry, rz, sx, sy, sz;
+};
+
 // Relocate the FP32 offset r (relative to the origin of `cur`) by a straight walk across the
 // most violated face, re-basing r (and the carried start offset s) with each neighbour's
 // stored origin shift; a walk that meets a boundary face or runs long falls back to the FP64
-// locate on the absolute position.  Returns the new tet or -1.
-static __device__ __noinline__ int relocate_f(const MeshView& M, int cur, float& rx, float& ry, float& rz, float& sx,
-                                              float& sy, float& sz)
+// locate on the absolute position.
+static __device__ __noinline__ Reloc relocate_f(const MeshView& M, int cur, float rx, float ry, float rz, float sx,
+                                                float sy, float sz)
 {
     int t = cur;
     float qx = rx, qy = ry, qz = rz, ox = 0.f, oy = 0.f, oz = 0.f;
@@ -135,30 +143,24 @@ static __device__ __noinline__ int relocate_f(const MeshView& M, int cur, float&
         t = nt;
         load_j(M, t, j);
         baryj(j, qx, qy, qz, l);
-        if (inside_f(l)) {
-            rx = qx; ry = qy; rz = qz;
-            sx += ox; sy += oy; sz += oz;
-            return t;
-        }
+        if (inside_f(l)) return Reloc{t, qx, qy, qz, sx + ox, sy + oy, sz + oz};
         if (!(l[0] == l[0])) break;
     }
     const double3 oc = origin(M, cur);
     double px = oc.x + (double)rx, py = oc.y + (double)ry, pz = oc.z + (double)rz;
     int tt = locate_far(M, px, py, pz, cur);
-    if (tt < 0) return -1;
+    if (tt < 0) return Reloc{-1, rx, ry, rz, sx, sy, sz};
     double3 on = origin(M, tt);
     float dx = (float)(oc.x - on.x), dy = (float)(oc.y - on.y), dz = (float)(oc.z - on.z);
-    rx = (float)(px - on.x); ry = (float)(py - on.y); rz = (float)(pz - on.z);
-    sx += dx; sy += dy; sz += dz;
-    return tt;
+    return Reloc{tt, (float)(px - on.x), (float)(py - on.y), (float)(pz - on.z), sx + dx, sy + dy, sz + dz};
 }
 
 // Deposit along start -> end (both FP32 offsets from the origin of t) into t: the sample
 // points that lie in t (the sub-step changed tet), summed in FP32 per node, then converted
 // once to fixed point.
-static __device__ __noinline__ void deposit_traj_f(const MeshView& M, const SpeciesDev& S, const PushParams& pp,
-                                                   int t, float sx, float sy, float sz, float rx, float ry, float rz,
-                                                   ChargeAcc A)
+__device__ __forceinline__ void deposit_traj_f(const MeshView& M, const SpeciesDev& S, const PushParams& pp, int t,
+                                               float sx, float sy, float sz, float rx, float ry, float rz,
+                                               ChargeAcc A)
 {
     float j[9];
     load_j(M, t, j);
@@ -226,7 +228,7 @@ struct FlightF {
 // ran in this call.
 __device__ __forceinline__ int advance_f(const MeshView& M, const SpeciesDev& S, const PushParams& pp, FlightF& f,
                                          int cap, ChargeAcc A,
-                                         unsigned long long& nsub)
+                                         unsigned& nsub)
 {
     const float qm = (float)S.qm;
     const float floor_ratio = (float)pp.floor_ratio;
@@ -290,8 +292,11 @@ __device__ __forceinline__ int advance_f(const MeshView& M, const SpeciesDev& S,
             for (int q = 0; q < 4; ++q) l[q] = le[q];
             in = true;
         } else {
-            int nt = relocate_f(M, f.cur, f.rx, f.ry, f.rz, sx, sy, sz);
+            const Reloc rl = relocate_f(M, f.cur, f.rx, f.ry, f.rz, sx, sy, sz);
+            const int nt = rl.t;
             if (nt < 0) return kLost;
+            f.rx = rl.rx; f.ry = rl.ry; f.rz = rl.rz;
+            sx = rl.sx; sy = rl.sy; sz = rl.sz;
             f.cur = nt;
             rec = reinterpret_cast<const float4*>(M.trec + 64 * (int64_t)nt);
             load_j(M, nt, J);
@@ -315,7 +320,7 @@ __device__ __forceinline__ void finish_f(const MeshView& M, const ParticleStore&
     const double ke = 0.5 * S.m * (dvx * dvx + dvy * dvy + dvz * dvz);
     int tet_out = f.cur;
     if (st == kLost) {
-        ++c.nlost;
+        c.ev |= kEvLost;
         double px, py, pz;
         int hint = f.cur;
         if (f.cur >= 0) {
@@ -336,9 +341,9 @@ __device__ __forceinline__ void finish_f(const MeshView& M, const ParticleStore&
     }
     c.ke += ke;
     if (tet_out >= 0) {
-        ++c.nact;
+        c.ev |= kEvActive;
         if (pp.do_mcc && S.mcc_enabled && mcc_elastic(S, pp, P.id[i], dvx, dvy, dvz)) {
-            ++c.nhit;
+            c.ev |= kEvHit;
             f.vx = (float)dvx; f.vy = (float)dvy; f.vz = (float)dvz;
         }
     }
@@ -438,22 +443,23 @@ __device__ __forceinline__ void push_more_warp(const MeshView& M, const Particle
     warp_chunk_end(c);
 }
 
-// Pass 1: every stored particle.  Warps take 32-particle chunks from the launch's work
-// counter until none are left, so no warp idles while another still has work.
+// Pass 1: every stored particle.  Warps take runs of kRun 32-particle chunks from the launch's
+// work counter until none are left, so no warp idles while another still has work.
 __global__ void __launch_bounds__(256, 4) k_push_mixed(const __grid_constant__ MeshView M, ParticleStore P,
                                                     const __grid_constant__ SpeciesDev S,
                                                     const __grid_constant__ PushParams pp, DeferList D, ChargeAcc A,
                                                     LedgerDev* L, unsigned long long* ke_acc, unsigned* ctr)
 {
     const int64_t n = *P.count;
-    PushStats c{0.0, 0ull, 0ull, 0ull, 0ull};
+    PushStats c{0.0, 0u, 0u};
     warp_stats_begin();
     for (;;) {
-        const int64_t base = (int64_t)next_chunk(ctr) * 32;
-        if (base >= n) break;
-        push1_warp(M, P, S, pp, D, A, L, base, n, c);
+        const int64_t b0 = (int64_t)next_chunk(ctr) * (32 * kRun);
+        if (b0 >= n) break;
+        for (int64_t base = b0; base < b0 + 32 * kRun && base < n; base += 32)
+            push1_warp(M, P, S, pp, D, A, L, base, n, c);
     }
-    warp_stats_flush(c, L, ke_acc);
+    warp_stats_flush(L, ke_acc);
 }
 
 // Passes 2 and 3.
@@ -464,14 +470,14 @@ __global__ void __launch_bounds__(256, 4) k_push_mixed_more(const __grid_constan
                                                          unsigned long long* ke_acc, unsigned* ctr)
 {
     const int64_t n = (int64_t)min(*Din.count, Din.cap);
-    PushStats c{0.0, 0ull, 0ull, 0ull, 0ull};
+    PushStats c{0.0, 0u, 0u};
     warp_stats_begin();
     for (;;) {
         const int64_t base = (int64_t)next_chunk(ctr) * 32;
         if (base >= n) break;
         push_more_warp(M, P, S, pp, Din, Dout, cap, A, L, base, n, c);
     }
-    warp_stats_flush(c, L, ke_acc);
+    warp_stats_flush(L, ke_acc);
 }
 
 // ---- batched step: all (scenario, species) jobs in one launch per pass -----------------
@@ -488,7 +494,8 @@ __global__ void k_batch_prefix(const PushJob* __restrict__ jobs, int njobs, int 
             n = min((int64_t)*J.D1.count, (int64_t)J.D1.cap);
         else
             n = min((int64_t)*J.D2.count, (int64_t)J.D2.cap);
-        cnt[j] = (n + 31) / 32;
+        const int64_t unit = pass == 1 ? 32 * kRun : 32;  // particles per counter value
+        cnt[j] = (n + unit - 1) / unit;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -502,9 +509,10 @@ __global__ void k_batch_prefix(const PushJob* __restrict__ jobs, int njobs, int 
     }
 }
 
-// Pass `pass` (1, 2 or 3) of every job.  Warps take 32-particle chunks g of the global index
-// from the pass's work counter; chunk g belongs to the job j with pre[j] <= g < pre[j + 1], and a
-// warp flushes its statistics into a job's ledger when it moves on to another job.
+// Pass `pass` (1, 2 or 3) of every job.  Warps take units g of the global index from the pass's
+// work counter (pass 1: runs of kRun 32-particle chunks; passes 2 and 3: single chunks); unit g
+// belongs to the job j with pre[j] <= g < pre[j + 1], and a warp flushes its statistics into a
+// job's ledger when it moves on to another job.
 template <int PASS>
 __global__ void __launch_bounds__(256, 4) k_push_mixed_batch(const PushJob* __restrict__ jobs, int njobs,
                                                           const int64_t* __restrict__ pre, unsigned* __restrict__ ctr)
@@ -513,7 +521,7 @@ __global__ void __launch_bounds__(256, 4) k_push_mixed_batch(const PushJob* __re
     for (int j = threadIdx.x; j <= njobs; j += blockDim.x) spre[j] = pre[j];
     __syncthreads();
     const int64_t total = spre[njobs];
-    PushStats c{0.0, 0ull, 0ull, 0ull, 0ull};
+    PushStats c{0.0, 0u, 0u};
     warp_stats_begin();
     int cur = -1;
     for (;;) {
@@ -528,14 +536,18 @@ __global__ void __launch_bounds__(256, 4) k_push_mixed_batch(const PushJob* __re
                 hi = mid;
         }
         if (lo != cur) {
-            if (cur >= 0) warp_stats_flush(c, jobs[cur].L, jobs[cur].ke_acc);
+            if (cur >= 0) warp_stats_flush(jobs[cur].L, jobs[cur].ke_acc);
             cur = lo;
         }
         const PushJob& J = jobs[cur];
-        const int64_t base = (g - spre[cur]) * 32;
         if (PASS == 1) {
-            push1_warp(J.M, J.P, J.S, J.pp, J.D1, J.A, J.L, base, *J.P.count, c);
-        } else if (PASS == 2) {
+            const int64_t n = *J.P.count, b0 = (g - spre[cur]) * (32 * kRun);
+            for (int64_t base = b0; base < b0 + 32 * kRun && base < n; base += 32)
+                push1_warp(J.M, J.P, J.S, J.pp, J.D1, J.A, J.L, base, n, c);
+            continue;
+        }
+        const int64_t base = (g - spre[cur]) * 32;
+        if (PASS == 2) {
             const int64_t n = min((int64_t)*J.D1.count, (int64_t)J.D1.cap);
             push_more_warp(J.M, J.P, J.S, J.pp, J.D1, J.D2, kCap2, J.A, J.L, base, n, c);
         } else {
@@ -543,7 +555,7 @@ __global__ void __launch_bounds__(256, 4) k_push_mixed_batch(const PushJob* __re
             push_more_warp(J.M, J.P, J.S, J.pp, J.D2, DeferList{}, 0, J.A, J.L, base, n, c);
         }
     }
-    if (cur >= 0) warp_stats_flush(c, jobs[cur].L, jobs[cur].ke_acc);
+    if (cur >= 0) warp_stats_flush(jobs[cur].L, jobs[cur].ke_acc);
 }
 
 // nodal E -> tet records of every scenario (tets block map)

@@ -196,22 +196,31 @@ def test_deterministic_and_sort_invariant(lib):
     sp = O.plasma_species(1e10, 1.0, 1.0, 0.05, 6)
     parts = O.seed_particles(mesh, sp, 6, 99)
     out = []
-    for sort_interval in (0, 0, 1):
+    # (re-sort interval, ion re-sort interval): none twice, every step, ions every third step
+    for sort_interval, ion_interval in ((0, 0), (0, 0), (1, 0), (1, 3)):
         dom = gpu_domain(mesh, 2e-8, face_bc=(2, 2, 2, 2, 1, 1), sort_interval=sort_interval)
         gpu_load_particles(dom, sp, parts)
+        if ion_interval:
+            dom.set_species_sort_interval(1, ion_interval)
         dom.set_potential(mesh.phi_bc)
         dom.solve_field()
         dom.step(4)
         rho, phi, E = dom.fields()
         st = gpu_state(dom, len(sp), len(parts["tet"]))
-        out.append((rho, phi, E, st, dom.ledger()))
+        out.append((rho, phi, E, st, dom.ledger(), dom.stats()))
         dom.close()
-    for k in (1, 2):
+    for k in (1, 2, 3):
         assert np.array_equal(out[0][0], out[k][0])  # fixed-point deposit: bitwise
         assert np.array_equal(out[0][4], out[k][4])
         act = out[0][3]["status"] == O.ACTIVE
         assert np.array_equal(out[0][3]["x"][act], out[k][3]["x"][act])
+        for key in ("active_particles", "total_charge"):
+            assert out[0][5][key] == out[k][5][key], key
     assert np.array_equal(out[0][1], out[1][1]) and np.array_equal(out[0][2], out[1][2])
+    # the kinetic energy is an integer sum, the same whichever warp took which particles (a
+    # re-sort drops the inactive particles whose energy the statistics still count, so it is
+    # compared between the two unsorted runs)
+    assert out[0][5]["total_energy"] == out[1][5]["total_energy"]
 
 
 def test_mixed_precision_error_bounded(lib):
