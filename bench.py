@@ -84,6 +84,20 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
+def reduce_over_ranks(dist, t_local, units, device="cuda"):
+    """(the slowest rank's time, the units all ranks processed); every rank calls it, in the
+    same order.  dist is torch.distributed (or None for one process)."""
+    if dist is None:
+        return t_local, float(units)
+    import torch
+
+    t = torch.tensor([t_local], device=device, dtype=torch.float64)
+    u = torch.tensor([float(units)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dist.all_reduce(u, op=dist.ReduceOp.SUM)
+    return float(t[0]), float(u[0])
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled during the timed region."""
 
@@ -215,14 +229,7 @@ def run_ours(args, cfg):
     tm = dom.timing()
     clk = clocks.stop()
     t_local = ms / 1e3
-    if dist:
-        t = torch.tensor([t_local, float(psteps)], device="cuda", dtype=torch.float64)
-        tmax = t.clone()
-        dist.all_reduce(tmax[:1], op=dist.ReduceOp.MAX)
-        dist.all_reduce(t[1:], op=dist.ReduceOp.SUM)
-        t_max, total_psteps = float(tmax[0]), float(t[1])
-    else:
-        t_max, total_psteps = t_local, float(psteps)
+    t_max, total_psteps = reduce_over_ranks(dist, t_local, psteps)
     value = total_psteps / t_max
     # roofline of the dominant kernel (the push), timed with events on the library stream
     push_ms = tm["push_ms"] / max(tm["push_launches"], 1)
@@ -270,14 +277,7 @@ def run_ours(args, cfg):
         gms = g0.elapsed_time(g1)
         gclk = clocks.stop()
         g_local = gms / 1e3
-        if dist:
-            t = torch.tensor([g_local, float(gps)], device="cuda", dtype=torch.float64)
-            tmax = t.clone()
-            dist.all_reduce(tmax[:1], op=dist.ReduceOp.MAX)
-            dist.all_reduce(t[1:], op=dist.ReduceOp.SUM)
-            g_max, g_total = float(tmax[0]), float(t[1])
-        else:
-            g_max, g_total = g_local, float(gps)
+        g_max, g_total = reduce_over_ranks(dist, g_local, gps)
         graph = {"value": g_total / g_max, "unit": "particle-steps/s", "ms_per_step": g_max * 1e3 / args.steps,
                  "gpu_launches": int(batch.kernel_launches() - l0), "clocks": gclk,
                  "form": "one CUDA-graph launch per step (one-scenario batch), steps after the stepped run"}
@@ -437,14 +437,7 @@ def run_batched(args, cfg):
     for d in doms:
         d.close()
     t_local = ms / 1e3
-    if dist:
-        t = torch.tensor([t_local, float(ps)], device="cuda", dtype=torch.float64)
-        tmax = t.clone()
-        dist.all_reduce(tmax[:1], op=dist.ReduceOp.MAX)
-        dist.all_reduce(t[1:], op=dist.ReduceOp.SUM)
-        t_max, total_ps = float(tmax[0]), float(t[1])
-    else:
-        t_max, total_ps = t_local, float(ps)
+    t_max, total_ps = reduce_over_ranks(dist, t_local, ps)
     out = {
         "metric": "PIC particle-steps/s on 1 B200 (mixed/batched vs plain FP64 at equal error)",
         "value": total_ps / t_max,
@@ -551,14 +544,7 @@ def run_surface(args, cfg):
     v64, v32 = res[0]["V"], res[1]["V"]
     err = float(np.abs(v32 - v64).max() / max(np.abs(v64).max(), 1e-300))
     t_local = res[1]["ms"] / 1e3
-    if dist:
-        t = torch.tensor([t_local, float(res[1]["ps"])], device="cuda", dtype=torch.float64)
-        tmax = t.clone()
-        dist.all_reduce(tmax[:1], op=dist.ReduceOp.MAX)
-        dist.all_reduce(t[1:], op=dist.ReduceOp.SUM)
-        t_max, total_ps = float(tmax[0]), float(t[1])
-    else:
-        t_max, total_ps = t_local, float(res[1]["ps"])
+    t_max, total_ps = reduce_over_ranks(dist, t_local, res[1]["ps"])
     out = {
         "metric": "PIC particle-steps/s on 1 B200 (mixed/batched vs plain FP64 at equal error)",
         "value": total_ps / t_max, "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps,
@@ -634,7 +620,7 @@ def cpu_baseline(cfg, args):
         ref = O.Reference(omp=True)
         total, steps, nt = 0.0, 0, 1
         cur = parts
-        while total < 10.0 and steps < 20:
+        while total < args.cpu_seconds and steps < 20:
             out, secs, nt = ref.push_parallel(mesh, E, cur, sp, cfg["dt"])
             cur = dict(parts, x=out["x"], v=out["v"], tet=np.where(out["lost"] == 1, -1, out["tet"]))
             total += secs
@@ -648,7 +634,7 @@ def cpu_baseline(cfg, args):
         t0 = time.perf_counter()
         steps = 0
         cur = parts
-        while time.perf_counter() - t0 < 10.0 and steps < 20:
+        while time.perf_counter() - t0 < args.cpu_seconds and steps < 20:
             out = o.push(mesh, E, cur, sp, cfg["dt"])
             cur = dict(parts, x=out["x"], v=out["v"], tet=np.where(out["lost"] == 1, -1, out["tet"]))
             steps += 1
@@ -707,6 +693,9 @@ def run_reference(args, cfg):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
+    # torchrun gives every rank one OpenMP thread; rank 0 alone runs the reference arm, on all
+    # the host's threads (set before the reference library and its OpenMP runtime load)
+    os.environ["OMP_NUM_THREADS"] = str(os.cpu_count() or 1)
     cb = cpu_baseline(cfg, args)
     out = {
         "impl": "reference",
@@ -739,6 +728,7 @@ def main():
     ap.add_argument("--ppc", type=int, default=0, help="override particles per cell per species")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-cpu-components", action="store_true", help="CPU baseline without its component figures")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU baseline: seconds of reference push timed")
     ap.add_argument("--no-fp64-compare", dest="fp64_compare", action="store_false")
     ap.add_argument("--scenarios", type=int, default=0, help="batched64: number of scenarios (default 64)")
     args = ap.parse_args()

@@ -55,26 +55,34 @@ __device__ __forceinline__ TetRec load_rec(const MeshView& M, int t)
     return R;
 }
 
-// Rewrite words 9..20 of record t (E0 and the three differences) from the nodal field,
-// keeping J^-1 and the node ids that share those 16-byte lines.
-__device__ __forceinline__ void refresh_trec_one(int64_t t, const int4* __restrict__ tet, const double* __restrict__ E,
-                                                 float* trec)
+// Rewrite words 9..20 of record t (E0 and the three differences) from the nodal field, keeping
+// J^-1 and the node ids that share those 16-byte lines.  Four lanes share a record, lane q
+// writing its float4 2 + q, so a warp writes 8 records' 64 contiguous bytes each.
+__device__ __forceinline__ void refresh_trec_part(int64_t t, int q, const int4* __restrict__ tet,
+                                                  const double* __restrict__ E, float* trec)
 {
-    int4 tn = tet[t];
+    const int4 tn = __ldg(tet + t);
     const double* e0 = E + 3 * (int64_t)tn.x;
-    const double* e1 = E + 3 * (int64_t)tn.y;
-    const double* e2 = E + 3 * (int64_t)tn.z;
-    const double* e3 = E + 3 * (int64_t)tn.w;
-    float* r = trec + 64 * t;
-    float4* r4 = reinterpret_cast<float4*>(r);
-    float j8 = r[8];
-    float nd0 = r[21], nd1 = r[22], nd2 = r[23];
-    r4[2] = make_float4(j8, (float)e0[0], (float)e0[1], (float)e0[2]);
-    r4[3] = make_float4((float)(e1[0] - e0[0]), (float)(e1[1] - e0[1]), (float)(e1[2] - e0[2]),
-                        (float)(e2[0] - e0[0]));
-    r4[4] = make_float4((float)(e2[1] - e0[1]), (float)(e2[2] - e0[2]), (float)(e3[0] - e0[0]),
-                        (float)(e3[1] - e0[1]));
-    r4[5] = make_float4((float)(e3[2] - e0[2]), nd0, nd1, nd2);
+    float4* r4 = reinterpret_cast<float4*>(trec + 64 * t) + 2 + q;
+    const double a0 = __ldg(e0), a1 = __ldg(e0 + 1), a2 = __ldg(e0 + 2);
+    if (q == 0) {
+        const float j8 = r4->x;
+        *r4 = make_float4(j8, (float)a0, (float)a1, (float)a2);
+    } else if (q == 1) {
+        const double* e1 = E + 3 * (int64_t)tn.y;
+        const double* e2 = E + 3 * (int64_t)tn.z;
+        *r4 = make_float4((float)(__ldg(e1) - a0), (float)(__ldg(e1 + 1) - a1), (float)(__ldg(e1 + 2) - a2),
+                          (float)(__ldg(e2) - a0));
+    } else if (q == 2) {
+        const double* e2 = E + 3 * (int64_t)tn.z;
+        const double* e3 = E + 3 * (int64_t)tn.w;
+        *r4 = make_float4((float)(__ldg(e2 + 1) - a1), (float)(__ldg(e2 + 2) - a2), (float)(__ldg(e3) - a0),
+                          (float)(__ldg(e3 + 1) - a1));
+    } else {
+        const double* e3 = E + 3 * (int64_t)tn.w;
+        const float4 old = *r4;
+        *r4 = make_float4((float)(__ldg(e3 + 2) - a2), old.y, old.z, old.w);
+    }
 }
 
 __device__ __forceinline__ void baryj(const float* j, float rx, float ry, float rz, float l[4])
@@ -564,8 +572,8 @@ __global__ void k_batch_refresh_trec(const FieldJob* __restrict__ jobs, BlockMap
     const int k = m.ctx_of[blockIdx.x];
     const unsigned lb = blockIdx.x - m.first[k], nb = m.first[k + 1] - m.first[k];
     const FieldJob& J = jobs[k];
-    for (int64_t t = lb * (int64_t)blockDim.x + threadIdx.x; t < J.T; t += (int64_t)nb * blockDim.x)
-        refresh_trec_one(t, J.tet, J.E, J.trec);
+    for (int64_t g = lb * (int64_t)blockDim.x + threadIdx.x; g < 4 * J.T; g += (int64_t)nb * blockDim.x)
+        refresh_trec_part(g >> 2, (int)(g & 3), J.tet, J.E, J.trec);
 }
 
 __global__ void k_mcc_mixed(ParticleStore P, SpeciesDev S, PushParams pp, LedgerDev* L)
@@ -618,8 +626,8 @@ __global__ void k_from_mixed(MeshView M, int64_t n, ParticleStore P, double* x, 
 // Refresh the nodal-E words of every tet record from the FP64 nodal field.
 __global__ void k_refresh_trec(int64_t T, const int4* __restrict__ tet, const double* __restrict__ E, float* trec)
 {
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < T; t += (int64_t)gridDim.x * blockDim.x)
-        refresh_trec_one(t, tet, E, trec);
+    for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < 4 * T; g += (int64_t)gridDim.x * blockDim.x)
+        refresh_trec_part(g >> 2, (int)(g & 3), tet, E, trec);
 }
 
 void launch_push_mixed(const MeshView& M, const ParticleStore& P, const SpeciesDev& S, const PushParams& pp,
