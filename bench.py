@@ -9,8 +9,8 @@ Workloads (all synthetic, seeded; the reference publishes no dataset):
                 Te = Ti = 1 eV, 64 particles per cell per species (~268M), dt = 2e-8 s,
                 FP32 cell-relative push, fixed-point deposit, FP32-SpMV PCG under FP64
                 refinement to 1e-10, elastic MCC (sigma 1e-19 m^2, n_n 1e14 m^-3), electrons
-                re-sorted by tet every 2 steps (they cross ~0.7 cells per step), ions every
-                16   [default]
+                re-sorted by tet every step (they cross ~0.7 cells per step), ions every 16
+                [default]
   plain32       32^3 cells, h = 0.05 m, 8^3-cell body, 20 ppc, FP64, Jacobi-PCG to 1e-8
   batched64     64 independent scenarios stepped together (one launch per kernel over all of
                 them, one CUDA-graph launch per step, launch shapes autotuned): box edge
@@ -46,7 +46,7 @@ QE, ME, MP = 1.602176634e-19, 9.1093837015e-31, 1.67262192369e-27
 
 CONFIGS = {
     "precision128": dict(n=128, L=1.6, body=(48, 80), bias=-10.0, ppc=64, dt=2e-8, precision=1, rtol=1e-10,
-                         density=1e10, te=1.0, ti=1.0, sort_interval=2, ion_sort_interval=16),
+                         density=1e10, te=1.0, ti=1.0, sort_interval=1, ion_sort_interval=16),
     "plain32": dict(n=32, L=1.6, body=(12, 20), bias=-10.0, ppc=20, dt=2e-8, precision=0, rtol=1e-8, density=1e10,
                     te=1.0, ti=1.0, sort_interval=8),
     "batched64": dict(scenarios=64, seed=2026, precision=1, rtol=1e-10, sort_interval=4),
