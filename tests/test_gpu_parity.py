@@ -188,6 +188,18 @@ def test_edge_cases(lib):
     assert dom.count(0) == 0
     with pytest.raises(Exception):
         dom.set_particles(5, np.zeros((1, 3)), np.zeros((1, 3)))
+    # a species re-sort interval needs a context interval to be a multiple of
+    with pytest.raises(Exception):
+        dom.set_species_sort_interval(1, 4)
+    with pytest.raises(Exception):
+        dom.set_species_sort_interval(7, 0)
+    dom.set_species_sort_interval(1, 0)
+    dom.close()
+    dom = gpu_domain(mesh, 2e-8, face_bc=(1,) * 6, sort_interval=2)
+    dom.set_species(sp)
+    with pytest.raises(Exception):
+        dom.set_species_sort_interval(1, 3)
+    dom.set_species_sort_interval(1, 6)
     dom.close()
 
 
