@@ -15,7 +15,6 @@
 
 using namespace scdat;
 
-struct SpeciesState;
 struct scdat_ctx;
 // true when species s re-sorts at the context's current step count (a multiple of the
 // context's sort interval)
