@@ -326,7 +326,8 @@ def run_ours(args, cfg):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_kind": peak_kind, "kernel": "push (gather+boris+relocate+deposit+mcc)",
                      "alg_bytes_per_launch": bytes_push, "launch_ms": push_ms},
-        "stage_ms_per_step": {"push": tm["push_ms"] / args.steps, "field": tm["field_ms"] / args.steps},
+        "stage_ms_per_step": {"push": tm["push_ms"] / args.steps, "field": tm["field_ms"] / args.steps,
+                              "resort": tm["sort_ms"] / args.steps},
         "gpu_launches": int(tm["kernel_launches"]),
         "clocks": clk,
         "e2e": {"value": e2e_val, "unit": "particle-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},

@@ -373,6 +373,9 @@ SCDAT_API void* scdat_stream(scdat_ctx* ctx);
 SCDAT_API int scdat_set_timing(scdat_ctx* ctx, int32_t enable);
 SCDAT_API int scdat_get_timing(scdat_ctx* ctx, double* push_ms, int64_t* push_launches, int64_t* push_particles,
                                double* field_ms, int64_t* field_solves, int64_t* kernel_launches);
+/* The same for the re-sorts by tet (key build, radix sort, gather of the store) since
+ * scdat_set_timing(1): summed device milliseconds and the number of species sorted. */
+SCDAT_API int scdat_get_sort_timing(scdat_ctx* ctx, double* sort_ms, int64_t* sorts);
 
 /* LinearSystem::solve(ITERATIVE) (Tools/Solver/src/LinearSystem.cpp:84-87,258-327) without a
  * context: Jacobi-preconditioned CG on a caller-assembled SPD system whose arrays all live in

@@ -87,6 +87,7 @@ EXPORTS = ["scdat_default_params", "scdat_create", "scdat_destroy", "scdat_last_
            "scdat_set_species_sort_interval",
            "scdat_get_fields", "scdat_get_species_charge", "scdat_get_ledger", "scdat_reset_ledger",
            "scdat_get_statistics", "scdat_version", "scdat_stream", "scdat_set_timing", "scdat_get_timing",
+           "scdat_get_sort_timing",
            "scdat_pcg_csr", "scdat_pcg_csr_noalloc", "scdat_set_charge_density", "scdat_set_dt", "scdat_set_seed",
            "scdat_batch_default_tuning", "scdat_batch_create", "scdat_batch_destroy", "scdat_batch_last_error",
            "scdat_batch_step", "scdat_batch_set_tuning", "scdat_batch_get_tuning", "scdat_batch_autotune",
@@ -164,6 +165,7 @@ def load():
     L.scdat_set_timing.argtypes = [vp, C.c_int32]
     L.scdat_get_timing.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_int64), C.POINTER(C.c_int64),
                                    C.POINTER(C.c_double), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+    L.scdat_get_sort_timing.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_int64)]
     L.scdat_pcg_csr.argtypes = [C.c_int32, vp, vp, vp, vp, vp, vp, C.c_double, C.c_int32, vp,
                                 C.POINTER(C.c_int32), C.POINTER(C.c_double)]
     L.scdat_pcg_csr_noalloc.argtypes = L.scdat_pcg_csr.argtypes
@@ -434,8 +436,10 @@ class Domain:
         pl, pp, fs, kl = C.c_int64(), C.c_int64(), C.c_int64(), C.c_int64()
         self._ck(self.L.scdat_get_timing(self.h, C.byref(pm), C.byref(pl), C.byref(pp), C.byref(fm), C.byref(fs),
                                          C.byref(kl)))
+        sm, sn = C.c_double(), C.c_int64()
+        self._ck(self.L.scdat_get_sort_timing(self.h, C.byref(sm), C.byref(sn)))
         return dict(push_ms=pm.value, push_launches=pl.value, push_particles=pp.value, field_ms=fm.value,
-                    field_solves=fs.value, kernel_launches=kl.value)
+                    field_solves=fs.value, kernel_launches=kl.value, sort_ms=sm.value, sorts=sn.value)
 
     def stats(self):
         st = StatsC()

@@ -399,6 +399,14 @@ int harvest_timing(scdat_ctx* ctx)
         cudaEventDestroy(pr.second);
     }
     ctx->ev_field.clear();
+    for (auto& pr : ctx->ev_sort) {
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, pr.first, pr.second));
+        ctx->sort_ms += ms;
+        cudaEventDestroy(pr.first);
+        cudaEventDestroy(pr.second);
+    }
+    ctx->ev_sort.clear();
     return SCDAT_OK;
 }
 
@@ -433,6 +441,12 @@ int do_sort(scdat_ctx* ctx, int s)
     const uint32_t inactive = (uint32_t)ctx->hm.T;  // keys: tet, T (no hint), T+1 (inactive)
     int bits = 1;
     while (((uint64_t)1 << bits) <= (uint64_t)inactive + 1) ++bits;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (ctx->timing) {
+        CK(cudaEventCreate(&e0));
+        CK(cudaEventCreate(&e1));
+        CK(cudaEventRecord(e0, ctx->st));
+    }
     ctx->launches += 2;  // keys + one gather of the whole store (the radix sort itself is CUB's)
     launch_sort_keys(n, S.tet.p, inactive, ctx->kin.p, ctx->vin.p, ctx->nact.p, ctx->st);
     size_t tmp = 0;
@@ -472,6 +486,11 @@ int do_sort(scdat_ctx* ctx, int s)
     S.tet.swap(ctx->scratchi);
     S.id.swap(ctx->scratchu);
     CK(cudaGetLastError());
+    if (ctx->timing) {
+        CK(cudaEventRecord(e1, ctx->st));
+        ctx->ev_sort.emplace_back(e0, e1);
+        ctx->sorts += 1;
+    }
     int64_t act = 0;
     CK(cudaMemcpyAsync(&act, ctx->nact.p, sizeof(act), cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
@@ -667,6 +686,7 @@ SCDAT_API int scdat_destroy(scdat_ctx* ctx)
     if (ctx->st) cudaStreamSynchronize(ctx->st);
     for (auto& pr : ctx->ev_push) { cudaEventDestroy(pr.first); cudaEventDestroy(pr.second); }
     for (auto& pr : ctx->ev_field) { cudaEventDestroy(pr.first); cudaEventDestroy(pr.second); }
+    for (auto& pr : ctx->ev_sort) { cudaEventDestroy(pr.first); cudaEventDestroy(pr.second); }
     cudaStream_t st = ctx->st;
     delete ctx;
     if (st) cudaStreamDestroy(st);
@@ -1423,8 +1443,8 @@ SCDAT_API int scdat_set_timing(scdat_ctx* ctx, int32_t enable)
     int rc = harvest_timing(ctx);
     if (rc) return rc;
     ctx->timing = enable != 0;
-    ctx->push_ms = ctx->field_ms = 0.0;
-    ctx->push_launches = ctx->field_solves = ctx->push_particles = ctx->launches = 0;
+    ctx->push_ms = ctx->field_ms = ctx->sort_ms = 0.0;
+    ctx->push_launches = ctx->field_solves = ctx->push_particles = ctx->launches = ctx->sorts = 0;
     return SCDAT_OK;
 }
 
@@ -1440,6 +1460,16 @@ SCDAT_API int scdat_get_timing(scdat_ctx* ctx, double* push_ms, int64_t* push_la
     if (field_ms) *field_ms = ctx->field_ms;
     if (field_solves) *field_solves = ctx->field_solves;
     if (kernel_launches) *kernel_launches = ctx->launches;
+    return SCDAT_OK;
+}
+
+SCDAT_API int scdat_get_sort_timing(scdat_ctx* ctx, double* sort_ms, int64_t* sorts)
+{
+    if (!ctx) return SCDAT_ERR_ARG;
+    int rc = harvest_timing(ctx);
+    if (rc) return rc;
+    if (sort_ms) *sort_ms = ctx->sort_ms;
+    if (sorts) *sorts = ctx->sorts;
     return SCDAT_OK;
 }
 

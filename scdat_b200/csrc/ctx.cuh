@@ -133,8 +133,9 @@ struct scdat_ctx {
     int grid_push = 148 * 8, grid_nodes = 148 * 4, grid_red = 148 * 8;
     // optional per-kernel timing (CUDA events around the launches on the context stream)
     bool timing = false;
-    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_push, ev_field;
-    double push_ms = 0.0, field_ms = 0.0;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_push, ev_field, ev_sort;
+    double push_ms = 0.0, field_ms = 0.0, sort_ms = 0.0;
+    int64_t sorts = 0;
     int64_t push_launches = 0, field_solves = 0;
     int64_t push_particles = 0;
     int64_t launches = 0;  // kernels of this library launched since scdat_set_timing
