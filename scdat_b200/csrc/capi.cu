@@ -48,6 +48,9 @@ void launch_sort_keys(int64_t n, const int32_t* tet, uint32_t inactive_key, uint
 template <typename T>
 void launch_gather_store(int64_t n, const int64_t* active, const uint32_t* perm, const GatherArrays<T>& in,
                          const GatherArrays<T>& out, cudaStream_t st);
+void launch_gather_mixed(int64_t n, const int64_t* active, const uint32_t* perm, const float4* in_mix,
+                         const int32_t* in_tet, const uint32_t* in_id, float4* out_mix, int32_t* out_tet,
+                         uint32_t* out_id, cudaStream_t st);
 void launch_scatter_values(int64_t n, const int64_t* idx, const double* v, double* dst, cudaStream_t st);
 }  // namespace scdat
 
@@ -91,8 +94,7 @@ ParticleStore store_of(scdat_ctx* ctx, int s)
     ParticleStore P{};
     P.x = S.x.p; P.y = S.y.p; P.z = S.z.p;
     P.vx = S.vx.p; P.vy = S.vy.p; P.vz = S.vz.p;
-    P.xf = S.xf.p; P.yf = S.yf.p; P.zf = S.zf.p;
-    P.vxf = S.vxf.p; P.vyf = S.vyf.p; P.vzf = S.vzf.p;
+    P.mix = S.mix.p;
     P.tet = S.tet.p;
     P.id = S.id.p;
     P.count = ctx->counts.p + s;
@@ -459,17 +461,10 @@ int do_sort(scdat_ctx* ctx, int s)
     if (ctx->scratchi.n < S.tet.n) CK(ctx->scratchi.alloc(S.tet.n));
     if (ctx->scratchu.n < S.id.n) CK(ctx->scratchu.alloc(S.id.n));
     if (ctx->mixed) {
-        DBuf<float>* fa[6] = {&S.xf, &S.yf, &S.zf, &S.vxf, &S.vyf, &S.vzf};
-        GatherArrays<float> in{}, out{};
-        for (int a = 0; a < 6; ++a) {
-            if (ctx->shadow32[a].n < fa[a]->n) CK(ctx->shadow32[a].alloc(fa[a]->n));
-            in.v[a] = fa[a]->p;
-            out.v[a] = ctx->shadow32[a].p;
-        }
-        in.tet = S.tet.p; in.id = S.id.p;
-        out.tet = ctx->scratchi.p; out.id = ctx->scratchu.p;
-        launch_gather_store<float>(n, ctx->nact.p, perm, in, out, ctx->st);
-        for (int a = 0; a < 6; ++a) fa[a]->swap(ctx->shadow32[a]);
+        if (ctx->shadow_mix.n < S.mix.n) CK(ctx->shadow_mix.alloc(S.mix.n));
+        launch_gather_mixed(n, ctx->nact.p, perm, S.mix.p, S.tet.p, S.id.p, ctx->shadow_mix.p, ctx->scratchi.p,
+                            ctx->scratchu.p, ctx->st);
+        S.mix.swap(ctx->shadow_mix);
     } else {
         DBuf<double>* da[6] = {&S.x, &S.y, &S.z, &S.vx, &S.vy, &S.vz};
         GatherArrays<double> in{}, out{};
@@ -728,11 +723,11 @@ static int alloc_species(scdat_ctx* ctx, int s, int64_t n)
     SpeciesState& S = ctx->species[s];
     int64_t cap = std::max<int64_t>(n, 1);
     if (ctx->mixed) {
-        for (DBuf<float>* a : {&S.xf, &S.yf, &S.zf, &S.vxf, &S.vyf, &S.vzf}) CK(a->alloc((size_t)cap));
+        CK(S.mix.alloc(2 * (size_t)cap));
         for (DBuf<double>* a : {&S.x, &S.y, &S.z, &S.vx, &S.vy, &S.vz}) a->release();
     } else {
         for (DBuf<double>* a : {&S.x, &S.y, &S.z, &S.vx, &S.vy, &S.vz}) CK(a->alloc((size_t)cap));
-        for (DBuf<float>* a : {&S.xf, &S.yf, &S.zf, &S.vxf, &S.vyf, &S.vzf}) a->release();
+        S.mix.release();
     }
     CK(S.tet.alloc((size_t)cap));
     CK(S.id.alloc((size_t)cap));
@@ -764,9 +759,9 @@ static int alloc_species(scdat_ctx* ctx, int s, int64_t n)
         CK(ctx->vout.alloc(need));
     }
     for (int a = 0; a < 6; ++a) {
-        if (ctx->mixed && ctx->shadow32[a].n < need) CK(ctx->shadow32[a].alloc(need));
         if (!ctx->mixed && ctx->shadow64[a].n < need) CK(ctx->shadow64[a].alloc(need));
     }
+    if (ctx->mixed && ctx->shadow_mix.n < 2 * need) CK(ctx->shadow_mix.alloc(2 * need));
     if (ctx->scratchi.n < need) CK(ctx->scratchi.alloc(need));
     if (ctx->scratchu.n < need) CK(ctx->scratchu.alloc(need));
     int bits = 1;

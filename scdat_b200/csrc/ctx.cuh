@@ -62,7 +62,7 @@ struct SpeciesState {
     int64_t n = 0;  // host view of the stored count (updated on set/compact)
     int sort_interval = 0;  // 0: the context's params.sort_interval
     DBuf<double> x, y, z, vx, vy, vz;
-    DBuf<float> xf, yf, zf, vxf, vyf, vzf;
+    DBuf<float4> mix;  // mixed form: two float4 per particle (see ParticleStore)
     DBuf<int32_t> tet;
     DBuf<uint32_t> id;
 };
@@ -104,7 +104,7 @@ struct scdat_ctx {
     DBuf<uint32_t> kin, kout, vin, vout;
     DBuf<unsigned char> cub_tmp;
     DBuf<double> shadow64[6];  // re-sort targets, swapped with the store's arrays
-    DBuf<float> shadow32[6];
+    DBuf<float4> shadow_mix;
     DBuf<int32_t> scratchi;
     DBuf<uint32_t> scratchu;
     DBuf<int64_t> nact;

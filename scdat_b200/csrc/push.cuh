@@ -7,14 +7,31 @@
 namespace scdat {
 
 struct ParticleStore {
-    // FP64 form: absolute positions.  Mixed form: xf/yf/zf hold float offsets from the
-    // origin node of the particle's tet and vxf/vyf/vzf float velocities.
+    // FP64 form: absolute positions.  Mixed form: one 32-byte record per particle, two float4:
+    // (x, y, z, vx) with the position as a float offset from the origin node of the particle's
+    // tet, then (vy, vz, unused, unused) -- one sector per particle for the push's loads and
+    // stores and for the re-sort's gather.
     double *x, *y, *z, *vx, *vy, *vz;
-    float *xf, *yf, *zf, *vxf, *vyf, *vzf;
+    float4* mix;
     int32_t* tet;
     uint32_t* id;
     const int64_t* count;  // device-resident particle count of this species
 };
+
+__device__ __forceinline__ void mix_load(const ParticleStore& P, int64_t i, float& x, float& y, float& z, float& vx,
+                                         float& vy, float& vz)
+{
+    const float4 a = P.mix[2 * i], b = P.mix[2 * i + 1];
+    x = a.x; y = a.y; z = a.z; vx = a.w;
+    vy = b.x; vz = b.y;
+}
+
+__device__ __forceinline__ void mix_store(const ParticleStore& P, int64_t i, float x, float y, float z, float vx,
+                                          float vy, float vz)
+{
+    P.mix[2 * i] = make_float4(x, y, z, vx);
+    P.mix[2 * i + 1] = make_float4(vy, vz, 0.0f, 0.0f);
+}
 
 __device__ __forceinline__ bool bary_inside(const double lam[4])
 {

@@ -355,8 +355,7 @@ __device__ __forceinline__ void finish_f(const MeshView& M, const ParticleStore&
             f.vx = (float)dvx; f.vy = (float)dvy; f.vz = (float)dvz;
         }
     }
-    P.xf[i] = f.rx; P.yf[i] = f.ry; P.zf[i] = f.rz;
-    P.vxf[i] = f.vx; P.vyf[i] = f.vy; P.vzf[i] = f.vz;
+    mix_store(P, i, f.rx, f.ry, f.rz, f.vx, f.vy, f.vz);
     P.tet[i] = tet_out;
 }
 
@@ -367,8 +366,7 @@ __device__ __forceinline__ void defer_store_f(const ParticleStore& P, const Defe
     D.it[slot] = f.it;
     D.rem[slot] = f.rem;
     D.vstart[slot] = f.vstart;
-    P.xf[i] = f.rx; P.yf[i] = f.ry; P.zf[i] = f.rz;
-    P.vxf[i] = f.vx; P.vyf[i] = f.vy; P.vzf[i] = f.vz;
+    mix_store(P, i, f.rx, f.ry, f.rz, f.vx, f.vy, f.vz);
     P.tet[i] = f.cur;
 }
 
@@ -383,13 +381,12 @@ __device__ __forceinline__ void push1_warp(const MeshView& M, const ParticleStor
     FlightF f;
     if (i < n) {
         f.cur = P.tet[i];
-        f.vx = P.vxf[i]; f.vy = P.vyf[i]; f.vz = P.vzf[i];
+        mix_load(P, i, f.rx, f.ry, f.rz, f.vx, f.vy, f.vz);
         if (f.cur <= kTetAbsorbed) {
             // updateStatistics sums every particle the container still holds (PICCycle.cpp:941-966)
             double ux = f.vx, uy = f.vy, uz = f.vz;
             c.ke += 0.5 * S.m * (ux * ux + uy * uy + uz * uz);
         } else {
-            f.rx = P.xf[i]; f.ry = P.yf[i]; f.rz = P.zf[i];
             f.vstart = sqrtf(f.vx * f.vx + f.vy * f.vy + f.vz * f.vz);
             f.rem = (float)pp.dt;
             f.it = 0;
@@ -434,8 +431,7 @@ __device__ __forceinline__ void push_more_warp(const MeshView& M, const Particle
     if (e < n) {
         i = Din.idx[e];
         f.cur = P.tet[i];
-        f.rx = P.xf[i]; f.ry = P.yf[i]; f.rz = P.zf[i];
-        f.vx = P.vxf[i]; f.vy = P.vyf[i]; f.vz = P.vzf[i];
+        mix_load(P, i, f.rx, f.ry, f.rz, f.vx, f.vy, f.vz);
         f.it = Din.it[e];
         f.rem = (float)Din.rem[e];
         f.vstart = (float)Din.vstart[e];
@@ -584,9 +580,11 @@ __global__ void k_mcc_mixed(ParticleStore P, SpeciesDev S, PushParams pp, Ledger
     unsigned long long nhit = 0;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         if (P.tet[i] <= kTetAbsorbed) continue;
-        double vx = P.vxf[i], vy = P.vyf[i], vz = P.vzf[i];
+        float rx, ry, rz, ux, uy, uz;
+        mix_load(P, i, rx, ry, rz, ux, uy, uz);
+        double vx = ux, vy = uy, vz = uz;
         if (mcc_elastic(S, pp, P.id[i], vx, vy, vz)) {
-            P.vxf[i] = (float)vx; P.vyf[i] = (float)vy; P.vzf[i] = (float)vz;
+            mix_store(P, i, rx, ry, rz, (float)vx, (float)vy, (float)vz);
             ++nhit;
         }
     }
@@ -601,12 +599,12 @@ __global__ void k_to_mixed(MeshView M, int64_t n, const double* x, const double*
         int t = locate(M, x[i], y[i], z[i], P.tet[i]);
         if (t >= 0) {
             double3 o = origin(M, t);
-            P.xf[i] = (float)(x[i] - o.x); P.yf[i] = (float)(y[i] - o.y); P.zf[i] = (float)(z[i] - o.z);
+            mix_store(P, i, (float)(x[i] - o.x), (float)(y[i] - o.y), (float)(z[i] - o.z), (float)vx[i], (float)vy[i],
+                      (float)vz[i]);
         } else {
-            P.xf[i] = (float)x[i]; P.yf[i] = (float)y[i]; P.zf[i] = (float)z[i];
+            mix_store(P, i, (float)x[i], (float)y[i], (float)z[i], (float)vx[i], (float)vy[i], (float)vz[i]);
         }
         P.tet[i] = t >= 0 ? t : kTetNoHint;
-        P.vxf[i] = (float)vx[i]; P.vyf[i] = (float)vy[i]; P.vzf[i] = (float)vz[i];
     }
 }
 
@@ -620,8 +618,10 @@ __global__ void k_from_mixed(MeshView M, int64_t n, ParticleStore P, double* x, 
             double3 o = origin(M, t);
             ox = o.x; oy = o.y; oz = o.z;
         }
-        x[i] = ox + (double)P.xf[i]; y[i] = oy + (double)P.yf[i]; z[i] = oz + (double)P.zf[i];
-        vx[i] = P.vxf[i]; vy[i] = P.vyf[i]; vz[i] = P.vzf[i];
+        float rx, ry, rz, ux, uy, uz;
+        mix_load(P, i, rx, ry, rz, ux, uy, uz);
+        x[i] = ox + (double)rx; y[i] = oy + (double)ry; z[i] = oz + (double)rz;
+        vx[i] = ux; vy[i] = uy; vz[i] = uz;
     }
 }
 

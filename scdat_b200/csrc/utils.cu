@@ -62,10 +62,36 @@ void launch_gather_store(int64_t n, const int64_t* active, const uint32_t* perm,
     if (grid < 1) grid = 1;
     k_gather_store<T><<<grid, 256, 0, st>>>(active, perm, in, out);
 }
+// The same for the mixed form's 32-byte records (one sector each), tet and id.
+__global__ void k_gather_mixed(const int64_t* __restrict__ active, const uint32_t* __restrict__ perm,
+                               const float4* __restrict__ in_mix, const int32_t* __restrict__ in_tet,
+                               const uint32_t* __restrict__ in_id, float4* __restrict__ out_mix,
+                               int32_t* __restrict__ out_tet, uint32_t* __restrict__ out_id)
+{
+    const int64_t n = *active;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t j = __ldg(perm + i);
+        const float4 a = __ldg(in_mix + 2 * (int64_t)j), b = __ldg(in_mix + 2 * (int64_t)j + 1);
+        const int32_t t = __ldg(in_tet + j);
+        const uint32_t id = __ldg(in_id + j);
+        out_mix[2 * i] = a;
+        out_mix[2 * i + 1] = b;
+        out_tet[i] = t;
+        out_id[i] = id;
+    }
+}
+
+void launch_gather_mixed(int64_t n, const int64_t* active, const uint32_t* perm, const float4* in_mix,
+                         const int32_t* in_tet, const uint32_t* in_id, float4* out_mix, int32_t* out_tet,
+                         uint32_t* out_id, cudaStream_t st)
+{
+    int grid = (int)std::min<int64_t>((n + 255) / 256, 148 * 16);
+    if (grid < 1) grid = 1;
+    k_gather_mixed<<<grid, 256, 0, st>>>(active, perm, in_mix, in_tet, in_id, out_mix, out_tet, out_id);
+}
+
 template void launch_gather_store<double>(int64_t, const int64_t*, const uint32_t*, const GatherArrays<double>&,
                                           const GatherArrays<double>&, cudaStream_t);
-template void launch_gather_store<float>(int64_t, const int64_t*, const uint32_t*, const GatherArrays<float>&,
-                                         const GatherArrays<float>&, cudaStream_t);
 
 __global__ void k_scatter_values(int64_t n, const int64_t* __restrict__ idx, const double* __restrict__ v, double* dst)
 {
@@ -111,10 +137,8 @@ __global__ void k_seed_box(const int32_t* __restrict__ hex_ijk, int64_t ncell, i
         double vx = sigma * r1 * cos(tp * g1), vy = sigma * r1 * sin(tp * g1), vz = sigma * r2 * cos(tp * g3);
         if (mixed) {
             int o = __ldg(&M.tet[tet].x);
-            P.xf[k] = (float)(x - M.xyz[3 * o]);
-            P.yf[k] = (float)(y - M.xyz[3 * o + 1]);
-            P.zf[k] = (float)(z - M.xyz[3 * o + 2]);
-            P.vxf[k] = (float)vx; P.vyf[k] = (float)vy; P.vzf[k] = (float)vz;
+            mix_store(P, k, (float)(x - M.xyz[3 * o]), (float)(y - M.xyz[3 * o + 1]), (float)(z - M.xyz[3 * o + 2]),
+                      (float)vx, (float)vy, (float)vz);
         } else {
             P.x[k] = x; P.y[k] = y; P.z[k] = z;
             P.vx[k] = vx; P.vy[k] = vy; P.vz[k] = vz;
@@ -162,10 +186,8 @@ __global__ void k_seed_tets(const int32_t* __restrict__ tets, int64_t ntet, int3
         const double vx = dx + sigma * r1 * cos(tp * g[1]), vy = dy + sigma * r1 * sin(tp * g[1]),
                      vz = dz + sigma * r2 * cos(tp * g[3]);
         if (mixed) {
-            P.xf[k] = (float)(x - M.xyz[3 * nd[0]]);
-            P.yf[k] = (float)(y - M.xyz[3 * nd[0] + 1]);
-            P.zf[k] = (float)(z - M.xyz[3 * nd[0] + 2]);
-            P.vxf[k] = (float)vx; P.vyf[k] = (float)vy; P.vzf[k] = (float)vz;
+            mix_store(P, k, (float)(x - M.xyz[3 * nd[0]]), (float)(y - M.xyz[3 * nd[0] + 1]),
+                      (float)(z - M.xyz[3 * nd[0] + 2]), (float)vx, (float)vy, (float)vz);
         } else {
             P.x[k] = x; P.y[k] = y; P.z[k] = z;
             P.vx[k] = vx; P.vy[k] = vy; P.vz[k] = vz;
@@ -193,8 +215,10 @@ __global__ void k_layer_moments(ParticleStore P, int64_t n, int mixed, MeshView 
         if (t < 0) continue;
         double z, vx, vy, vz;
         if (mixed) {
-            z = M.xyz[3 * __ldg(&M.tet[t].x) + 2] + (double)P.zf[i];
-            vx = P.vxf[i]; vy = P.vyf[i]; vz = P.vzf[i];
+            float rx, ry, rz, ux, uy, uz;
+            mix_load(P, i, rx, ry, rz, ux, uy, uz);
+            z = M.xyz[3 * __ldg(&M.tet[t].x) + 2] + (double)rz;
+            vx = ux; vy = uy; vz = uz;
         } else {
             z = P.z[i];
             vx = P.vx[i]; vy = P.vy[i]; vz = P.vz[i];
