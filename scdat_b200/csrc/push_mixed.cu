@@ -31,29 +31,6 @@ __device__ __forceinline__ bool inside_f(const float l[4])
 // record layout (64 words): [0..8] J^-1, [9..11] E0, [12..20] E1-E0, E2-E0, E3-E0,
 // [21..24] node ids, [25..28] face neighbours, [29..31] unused | [32..43] origin minus the
 // origin of each face neighbour (FP32), [44..63] unused
-struct TetRec {
-    float j[9];
-    float e0[3];
-    float d[9];
-    int nd[4];
-};
-
-__device__ __forceinline__ TetRec load_rec(const MeshView& M, int t)
-{
-    const float4* g = reinterpret_cast<const float4*>(M.trec + 64 * (int64_t)t);
-    float4 a = __ldg(g), b = __ldg(g + 1), c = __ldg(g + 2), d = __ldg(g + 3), e = __ldg(g + 4), f = __ldg(g + 5),
-           h = __ldg(g + 6);
-    TetRec R;
-    R.j[0] = a.x; R.j[1] = a.y; R.j[2] = a.z; R.j[3] = a.w;
-    R.j[4] = b.x; R.j[5] = b.y; R.j[6] = b.z; R.j[7] = b.w;
-    R.j[8] = c.x; R.e0[0] = c.y; R.e0[1] = c.z; R.e0[2] = c.w;
-    R.d[0] = d.x; R.d[1] = d.y; R.d[2] = d.z; R.d[3] = d.w;
-    R.d[4] = e.x; R.d[5] = e.y; R.d[6] = e.z; R.d[7] = e.w;
-    R.d[8] = f.x;
-    R.nd[0] = __float_as_int(f.y); R.nd[1] = __float_as_int(f.z); R.nd[2] = __float_as_int(f.w);
-    R.nd[3] = __float_as_int(h.x);
-    return R;
-}
 
 // Rewrite words 9..20 of record t (E0 and the three differences) from the nodal field, keeping
 // J^-1 and the node ids that share those 16-byte lines.  Four lanes share a record, lane q
