@@ -287,7 +287,7 @@ def run_ours(args, cfg):
     h_nodes = torch.from_numpy(dir_nodes).pin_memory()
     h_vals = torch.from_numpy(mesh["phi"][dir_nodes].copy()).pin_memory()
     h_phi = torch.empty(dom.N, dtype=torch.float64).pin_memory()
-    e2e_steps = max(1, min(args.steps, 3))
+    e2e_steps = max(1, min(args.steps, 10))
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     e2e_ps = 0
@@ -423,7 +423,7 @@ def run_batched(args, cfg):
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     e2e_ps = 0
-    e2e_steps = max(1, min(args.steps, 3))
+    e2e_steps = max(1, min(args.steps, 10))
     for _ in range(e2e_steps):
         for d, hn, hv in zip(doms, h_nodes, h_vals):
             d.L.scdat_set_node_potentials(d.h, hn.shape[0], hn.data_ptr(), hv.data_ptr())

@@ -48,9 +48,9 @@ void launch_sort_keys(int64_t n, const int32_t* tet, uint32_t inactive_key, uint
 template <typename T>
 void launch_gather_store(int64_t n, const int64_t* active, const uint32_t* perm, const GatherArrays<T>& in,
                          const GatherArrays<T>& out, cudaStream_t st);
-void launch_gather_mixed(int64_t n, const int64_t* active, const uint32_t* perm, const float4* in_mix,
-                         const int32_t* in_tet, const uint32_t* in_id, float4* out_mix, int32_t* out_tet,
-                         uint32_t* out_id, cudaStream_t st);
+void launch_gather_mixed(int64_t n, const int64_t* active, const uint32_t* perm, const uint32_t* sorted_keys,
+                         uint32_t nohint_key, const float4* in_mix, const uint32_t* in_id, float4* out_mix,
+                         int32_t* out_tet, uint32_t* out_id, cudaStream_t st);
 void launch_scatter_values(int64_t n, const int64_t* idx, const double* v, double* dst, cudaStream_t st);
 }  // namespace scdat
 
@@ -462,8 +462,8 @@ int do_sort(scdat_ctx* ctx, int s)
     if (ctx->scratchu.n < S.id.n) CK(ctx->scratchu.alloc(S.id.n));
     if (ctx->mixed) {
         if (ctx->shadow_mix.n < S.mix.n) CK(ctx->shadow_mix.alloc(S.mix.n));
-        launch_gather_mixed(n, ctx->nact.p, perm, S.mix.p, S.tet.p, S.id.p, ctx->shadow_mix.p, ctx->scratchi.p,
-                            ctx->scratchu.p, ctx->st);
+        launch_gather_mixed(n, ctx->nact.p, perm, ctx->kout.p, inactive, S.mix.p, S.id.p, ctx->shadow_mix.p,
+                            ctx->scratchi.p, ctx->scratchu.p, ctx->st);
         S.mix.swap(ctx->shadow_mix);
     } else {
         DBuf<double>* da[6] = {&S.x, &S.y, &S.z, &S.vx, &S.vy, &S.vz};

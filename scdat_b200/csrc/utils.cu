@@ -62,17 +62,21 @@ void launch_gather_store(int64_t n, const int64_t* active, const uint32_t* perm,
     if (grid < 1) grid = 1;
     k_gather_store<T><<<grid, 256, 0, st>>>(active, perm, in, out);
 }
-// The same for the mixed form's 32-byte records (one sector each), tet and id.
+// The same for the mixed form's 32-byte records (one sector each) and ids; the tet of a kept
+// particle is its sorted key (read in order, not gathered): the tet id, or nohint_key for a
+// particle without a hint.
 __global__ void k_gather_mixed(const int64_t* __restrict__ active, const uint32_t* __restrict__ perm,
-                               const float4* __restrict__ in_mix, const int32_t* __restrict__ in_tet,
-                               const uint32_t* __restrict__ in_id, float4* __restrict__ out_mix,
-                               int32_t* __restrict__ out_tet, uint32_t* __restrict__ out_id)
+                               const uint32_t* __restrict__ sorted_keys, uint32_t nohint_key,
+                               const float4* __restrict__ in_mix, const uint32_t* __restrict__ in_id,
+                               float4* __restrict__ out_mix, int32_t* __restrict__ out_tet,
+                               uint32_t* __restrict__ out_id)
 {
     const int64_t n = *active;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         const uint32_t j = __ldg(perm + i);
         const float4 a = __ldg(in_mix + 2 * (int64_t)j), b = __ldg(in_mix + 2 * (int64_t)j + 1);
-        const int32_t t = __ldg(in_tet + j);
+        const uint32_t key = __ldg(sorted_keys + i);
+        const int32_t t = key < nohint_key ? (int32_t)key : kTetNoHint;
         const uint32_t id = __ldg(in_id + j);
         out_mix[2 * i] = a;
         out_mix[2 * i + 1] = b;
@@ -81,13 +85,14 @@ __global__ void k_gather_mixed(const int64_t* __restrict__ active, const uint32_
     }
 }
 
-void launch_gather_mixed(int64_t n, const int64_t* active, const uint32_t* perm, const float4* in_mix,
-                         const int32_t* in_tet, const uint32_t* in_id, float4* out_mix, int32_t* out_tet,
-                         uint32_t* out_id, cudaStream_t st)
+void launch_gather_mixed(int64_t n, const int64_t* active, const uint32_t* perm, const uint32_t* sorted_keys,
+                         uint32_t nohint_key, const float4* in_mix, const uint32_t* in_id, float4* out_mix,
+                         int32_t* out_tet, uint32_t* out_id, cudaStream_t st)
 {
     int grid = (int)std::min<int64_t>((n + 255) / 256, 148 * 16);
     if (grid < 1) grid = 1;
-    k_gather_mixed<<<grid, 256, 0, st>>>(active, perm, in_mix, in_tet, in_id, out_mix, out_tet, out_id);
+    k_gather_mixed<<<grid, 256, 0, st>>>(active, perm, sorted_keys, nohint_key, in_mix, in_id, out_mix, out_tet,
+                                         out_id);
 }
 
 template void launch_gather_store<double>(int64_t, const int64_t*, const uint32_t*, const GatherArrays<double>&,
