@@ -487,66 +487,6 @@ __device__ __forceinline__ unsigned warp_append(bool want, unsigned* cnt)
     return base + (unsigned)__popc(m & ((1u << lane) - 1u));
 }
 
-// The deposit of a pass-1 sub-step that stayed inside its tet: q*w*w[i] into the tet's node i.
-// The sub-step records it here instead of adding it, and warp_stay_deposit adds the warp's
-// records together.
-template <typename W>
-struct StayDep {
-    int t;  // the tet, -1: nothing recorded
-    W w[4];
-};
-
-// Warp-aggregated charge deposit of the lanes' StayDep records; every lane of the warp calls it.
-// Particles are stored sorted by tet, so lanes holding the same tet sit in runs.  Each lane turns
-// its four contributions into the same 128-bit fixed-point values that fx_red adds, split into
-// the three limb words; a segmented shuffle reduction sums each run's limbs as integers (a run
-// holds at most 32 lanes, so the two low limb sums stay below 2^37, and the high word adds
-// modulo 2^64 exactly as the atomics do), and the first lane of the run adds the sums to the
-// run's four nodes.  The accumulators therefore receive the same integers as with one set of
-// atomics per lane: the charge is bitwise unchanged, with up to 32x fewer atomics.  node_of(t, i)
-// gives node i of tet t.
-template <typename W, typename NodeOf>
-__device__ __forceinline__ void warp_stay_deposit(const ChargeAcc& A, const StayDep<W>& sd, double qw, double inv_uq,
-                                                  NodeOf node_of)
-{
-    const unsigned full = 0xffffffffu;
-    const int lane = threadIdx.x & 31;
-    if (!__any_sync(full, sd.t >= 0)) return;
-    const int prev = __shfl_up_sync(full, sd.t, 1);
-    const unsigned heads = __ballot_sync(full, lane == 0 || prev != sd.t);
-    const unsigned after = heads & ~((2u << lane) - 1u);  // run starts above this lane (lane 31: none)
-    const int last = after ? __ffs(after) - 2 : 31;       // last lane of this lane's run
-    const bool head = (heads >> lane) & 1u;
-    const unsigned span = __reduce_max_sync(full, head ? (unsigned)(last - lane + 1) : 1u);
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        unsigned long long a = 0ull, b = 0ull, h = 0ull;
-        if (sd.t >= 0) {
-            const Fx128 v = fx_from_double((qw * (double)sd.w[q]) * inv_uq);
-            a = v.lo & 0xffffffffull;
-            b = v.lo >> 32;
-            h = (unsigned long long)v.hi;
-        }
-        // after the offsets 1 .. o, lane l holds the sum over lanes l .. min(l + 2o - 1, last)
-        for (unsigned o = 1; o < span; o <<= 1) {
-            const unsigned long long a2 = __shfl_down_sync(full, a, o);
-            const unsigned long long b2 = __shfl_down_sync(full, b, o);
-            const unsigned long long h2 = __shfl_down_sync(full, h, o);
-            if (lane + (int)o <= last) {
-                a += a2;
-                b += b2;
-                h += h2;
-            }
-        }
-        if (head && sd.t >= 0) {
-            const int node = node_of(sd.t, q);
-            if (a) atomicAdd(A.l0 + node, a);
-            if (b) atomicAdd(A.l1 + node, b);
-            if (h) atomicAdd(A.h + node, h);
-        }
-    }
-}
-
 constexpr int kCap1 = 1;   // sub-steps every particle gets in pass 1 (1, 2, 4: 45.6, 46.1, 47.0 ms at 128^3)
 constexpr int kCap2 = 16;  // further sub-steps in pass 2; pass 3 runs to the end
 

@@ -90,12 +90,10 @@ struct FlightD {
 };
 
 // Run sub-steps until the step's time is used up, the particle is lost, or `cap` sub-steps
-// ran in this call.  With STAY, the first sub-step that stays inside its tet records its
-// deposit in sd (for warp_stay_deposit) instead of adding it.
-template <bool STAY>
+// ran in this call.
 __device__ __forceinline__ int advance_d(const MeshView& M, const SpeciesDev& S, const PushParams& pp, FlightD& f,
                                          int cap, ChargeAcc A,
-                                         unsigned& nsub, StayDep<double>& sd)
+                                         unsigned& nsub)
 {
     const double qm = S.qm;
     const double qw = S.q * S.w;
@@ -142,19 +140,12 @@ __device__ __forceinline__ int advance_d(const MeshView& M, const SpeciesDev& S,
                     // q*w*lambda(midpoint) for the segment-cloud and Gauss-3 kernels
                     double tx = f.px - sx, ty = f.py - sy, tz = f.pz - sz;
                     bool tiny = sqrt(tx * tx + ty * ty + tz * tz) < 1e-15;
-                    if (STAY && sd.t < 0) {
-                        sd.t = f.cur;
+                    int4 tn = rec_nodes(M, f.cur);
+                    int nd[4] = {tn.x, tn.y, tn.z, tn.w};
 #pragma unroll
-                        for (int q = 0; q < 4; ++q)
-                            sd.w[q] = tiny ? lam[q] : (pp.dep_kernel == 0 ? le[q] : 0.5 * (lam[q] + le[q]));
-                    } else {
-                        int4 tn = rec_nodes(M, f.cur);
-                        int nd[4] = {tn.x, tn.y, tn.z, tn.w};
-#pragma unroll
-                        for (int q = 0; q < 4; ++q) {
-                            double lk = tiny ? lam[q] : (pp.dep_kernel == 0 ? le[q] : 0.5 * (lam[q] + le[q]));
-                            fx_red(A, nd[q], fx_from_double((qw * lk) * pp.inv_uq));
-                        }
+                    for (int q = 0; q < 4; ++q) {
+                        double lk = tiny ? lam[q] : (pp.dep_kernel == 0 ? le[q] : 0.5 * (lam[q] + le[q]));
+                        fx_red(A, nd[q], fx_from_double((qw * lk) * pp.inv_uq));
                     }
                 } else {
                     deposit_traj(M, S, pp, f.cur, sx, sy, sz, f.px, f.py, f.pz, A);
@@ -226,8 +217,6 @@ __global__ void __launch_bounds__(256) k_push_f64(const __grid_constant__ MeshVi
             const int64_t i = base + lane;
             int st = -1;
             FlightD f;
-            StayDep<double> sd;
-            sd.t = -1;
             if (i < n) {
                 int t0 = P.tet[i];
                 f.vx = P.vx[i]; f.vy = P.vy[i]; f.vz = P.vz[i];
@@ -244,19 +233,15 @@ __global__ void __launch_bounds__(256) k_push_f64(const __grid_constant__ MeshVi
                         f.cur = 0;  // result.final_element stays 0 (PICParticleAlgorithms.cpp:543,577)
                         st = kLost;
                     } else {
-                        st = advance_d<true>(M, S, pp, f, kCap1, A, c.nsub, sd);
+                        st = advance_d(M, S, pp, f, kCap1, A, c.nsub);
                     }
                 }
             }
-            if (pp.deposit)
-                warp_stay_deposit(A, sd, S.q * S.w, pp.inv_uq, [&](int t, int q) {
-                    return __ldg(reinterpret_cast<const int*>(M.geom + 16 * (int64_t)t + 14) + q);
-                });
             unsigned slot = warp_append(st == kCapped, D.count);
             if (st == kCapped && slot < D.cap) {
                 defer_store_d(P, D, slot, i, f);
             } else if (st >= 0) {
-                if (st == kCapped) st = advance_d<false>(M, S, pp, f, 0x7fffffff, A, c.nsub, sd);
+                if (st == kCapped) st = advance_d(M, S, pp, f, 0x7fffffff, A, c.nsub);
                 finish_d(M, P, S, pp, L, i, f, st, c);
             }
             warp_chunk_end(c);
@@ -282,7 +267,6 @@ __global__ void __launch_bounds__(256) k_push_f64_more(const __grid_constant__ M
         const int64_t e = base + lane;
         int st = -1;
         FlightD f;
-        StayDep<double> sd;  // unused: passes 2 and 3 add their deposits directly
         int64_t i = 0;
         if (e < n) {
             i = Din.idx[e];
@@ -292,13 +276,13 @@ __global__ void __launch_bounds__(256) k_push_f64_more(const __grid_constant__ M
             f.it = Din.it[e];
             f.rem = Din.rem[e];
             f.vstart = Din.vstart[e];
-            st = advance_d<false>(M, S, pp, f, chain ? cap : 0x7fffffff, A, c.nsub, sd);
+            st = advance_d(M, S, pp, f, chain ? cap : 0x7fffffff, A, c.nsub);
         }
         unsigned slot = chain ? warp_append(st == kCapped, Dout.count) : 0xffffffffu;
         if (st == kCapped && chain && slot < Dout.cap) {
             defer_store_d(P, Dout, slot, i, f);
         } else if (st >= 0) {
-            if (st == kCapped) st = advance_d<false>(M, S, pp, f, 0x7fffffff, A, c.nsub, sd);
+            if (st == kCapped) st = advance_d(M, S, pp, f, 0x7fffffff, A, c.nsub);
             finish_d(M, P, S, pp, L, i, f, st, c);
         }
         warp_chunk_end(c);

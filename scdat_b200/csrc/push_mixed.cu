@@ -210,12 +210,10 @@ struct FlightF {
 };
 
 // Run sub-steps until the step's time is used up, the particle is lost, or `cap` sub-steps
-// ran in this call.  With STAY, the first sub-step that stays inside its tet records its
-// deposit in sd (for warp_stay_deposit) instead of adding it.
-template <bool STAY>
+// ran in this call.
 __device__ __forceinline__ int advance_f(const MeshView& M, const SpeciesDev& S, const PushParams& pp, FlightF& f,
                                          int cap, ChargeAcc A,
-                                         unsigned& nsub, StayDep<float>& sd)
+                                         unsigned& nsub)
 {
     const float qm = (float)S.qm;
     const float floor_ratio = (float)pp.floor_ratio;
@@ -265,18 +263,11 @@ __device__ __forceinline__ int advance_f(const MeshView& M, const SpeciesDev& S,
                 if (in) {
                     float tx = f.rx - sx, ty = f.ry - sy, tz = f.rz - sz;
                     bool tiny = sqrtf(tx * tx + ty * ty + tz * tz) < 1e-15f;
-                    if (STAY && sd.t < 0) {
-                        sd.t = f.cur;
 #pragma unroll
-                        for (int q = 0; q < 4; ++q)
-                            sd.w[q] = tiny ? l[q] : (pp.dep_kernel == 0 ? le[q] : 0.5f * (l[q] + le[q]));
-                    } else {
-#pragma unroll
-                        for (int q = 0; q < 4; ++q) {
-                            float lk = tiny ? l[q] : (pp.dep_kernel == 0 ? le[q] : 0.5f * (l[q] + le[q]));
-                            const int nd = __float_as_int(__ldg(reinterpret_cast<const float*>(rec) + 21 + q));
-                            fx_red(A, nd, fx_from_double((qw * (double)lk) * pp.inv_uq));
-                        }
+                    for (int q = 0; q < 4; ++q) {
+                        float lk = tiny ? l[q] : (pp.dep_kernel == 0 ? le[q] : 0.5f * (l[q] + le[q]));
+                        const int nd = __float_as_int(__ldg(reinterpret_cast<const float*>(rec) + 21 + q));
+                        fx_red(A, nd, fx_from_double((qw * (double)lk) * pp.inv_uq));
                     }
                 } else {
                     deposit_traj_f(M, S, pp, f.cur, sx, sy, sz, f.rx, f.ry, f.rz, A);
@@ -365,8 +356,6 @@ __device__ __forceinline__ void push1_warp(const MeshView& M, const ParticleStor
     const int64_t i = base + (threadIdx.x & 31);
     int st = -1;
     FlightF f;
-    StayDep<float> sd;
-    sd.t = -1;
     if (i < n) {
         f.cur = P.tet[i];
         mix_load(P, i, f.rx, f.ry, f.rz, f.vx, f.vy, f.vz);
@@ -391,18 +380,14 @@ __device__ __forceinline__ void push1_warp(const MeshView& M, const ParticleStor
                     f.cur = t;
                 }
             }
-            if (st != kLost) st = advance_f<true>(M, S, pp, f, kCap1, A, c.nsub, sd);
+            if (st != kLost) st = advance_f(M, S, pp, f, kCap1, A, c.nsub);
         }
     }
-    if (pp.deposit)
-        warp_stay_deposit(A, sd, S.q * S.w, pp.inv_uq, [&](int t, int q) {
-            return __float_as_int(__ldg(M.trec + 64 * (int64_t)t + 21 + q));
-        });
     unsigned slot = warp_append(st == kCapped, D.count);
     if (st == kCapped && slot < D.cap) {
         defer_store_f(P, D, slot, i, f);
     } else if (st >= 0) {
-        if (st == kCapped) st = advance_f<false>(M, S, pp, f, 0x7fffffff, A, c.nsub, sd);
+        if (st == kCapped) st = advance_f(M, S, pp, f, 0x7fffffff, A, c.nsub);
         finish_f(M, P, S, pp, L, i, f, st, c);
     }
     warp_chunk_end(c);
@@ -419,7 +404,6 @@ __device__ __forceinline__ void push_more_warp(const MeshView& M, const Particle
     const int64_t e = base + (threadIdx.x & 31);
     int st = -1;
     FlightF f;
-    StayDep<float> sd;  // unused: passes 2 and 3 add their deposits directly
     int64_t i = 0;
     if (e < n) {
         i = Din.idx[e];
@@ -428,13 +412,13 @@ __device__ __forceinline__ void push_more_warp(const MeshView& M, const Particle
         f.it = Din.it[e];
         f.rem = (float)Din.rem[e];
         f.vstart = (float)Din.vstart[e];
-        st = advance_f<false>(M, S, pp, f, chain ? cap : 0x7fffffff, A, c.nsub, sd);
+        st = advance_f(M, S, pp, f, chain ? cap : 0x7fffffff, A, c.nsub);
     }
     unsigned slot = chain ? warp_append(st == kCapped, Dout.count) : 0xffffffffu;
     if (st == kCapped && chain && slot < Dout.cap) {
         defer_store_f(P, Dout, slot, i, f);
     } else if (st >= 0) {
-        if (st == kCapped) st = advance_f<false>(M, S, pp, f, 0x7fffffff, A, c.nsub, sd);
+        if (st == kCapped) st = advance_f(M, S, pp, f, 0x7fffffff, A, c.nsub);
         finish_f(M, P, S, pp, L, i, f, st, c);
     }
     warp_chunk_end(c);
