@@ -132,6 +132,8 @@ SCDAT_API void scdat_default_params(scdat_params* p);
  * geometry, the locate grid, the node graph and the Dirichlet-reduced matrix. */
 SCDAT_API int scdat_create(const scdat_mesh_desc* mesh, const scdat_params* params, scdat_ctx** out);
 SCDAT_API int scdat_destroy(scdat_ctx* ctx);
+/* One-line reason of the context's last failed call.  With ctx NULL: the reason of the calling
+ * thread's last failed scdat_create (whose context no longer exists), or "null context". */
 SCDAT_API const char* scdat_last_error(const scdat_ctx* ctx);
 
 /* ParticleManager species (ParticleFactory::createElectron/createIon,

@@ -246,7 +246,7 @@ class Domain:
         h = C.c_void_p()
         rc = self.L.scdat_create(C.byref(md), C.byref(prm), C.byref(h))
         if rc != 0:
-            raise ScdatError(rc, "scdat_create failed (bad mesh or CUDA error)")
+            raise ScdatError(rc, "scdat_create: " + self.L.scdat_last_error(None).decode())
         self.h = h
         self.nspecies = 0
 

@@ -500,6 +500,12 @@ int do_sort(scdat_ctx* ctx, int s)
 // ======================================================================================
 // C ABI
 // ======================================================================================
+namespace {
+// reason of the calling thread's last failed scdat_create (its context is gone by then)
+thread_local std::string t_create_err;
+int create_ctx(const scdat_mesh_desc* mesh, const scdat_params* params, scdat_ctx* ctx);
+}  // namespace
+
 extern "C" {
 
 SCDAT_API const char* scdat_version(void) { return "scdat_b200 0.1.0 (sm_100a)"; }
@@ -524,14 +530,38 @@ SCDAT_API void scdat_default_params(scdat_params* p)
     p->seed = 0x5CDA7B200ull;
 }
 
-SCDAT_API const char* scdat_last_error(const scdat_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+SCDAT_API const char* scdat_last_error(const scdat_ctx* ctx)
+{
+    if (ctx) return ctx->err.c_str();
+    return t_create_err.empty() ? "null context" : t_create_err.c_str();
+}
 
 SCDAT_API int scdat_create(const scdat_mesh_desc* mesh, const scdat_params* params, scdat_ctx** out)
 {
-    if (!mesh || !params || !out) return SCDAT_ERR_ARG;
+    if (!mesh || !params || !out) {
+        t_create_err = "scdat_create: null argument";
+        return SCDAT_ERR_ARG;
+    }
     *out = nullptr;
     auto holder = std::make_unique<scdat_ctx>();
-    scdat_ctx* ctx = holder.get();
+    const int rc = create_ctx(mesh, params, holder.get());
+    if (rc != SCDAT_OK) {
+        // the context (its stream and buffers included) is freed here; its reason stays readable
+        t_create_err = holder->err.empty() ? std::string("scdat_create failed") : holder->err;
+        return rc;
+    }
+    t_create_err.clear();
+    *out = holder.release();
+    return SCDAT_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// The body of scdat_create: fills ctx, or returns an error with ctx->err set.
+int create_ctx(const scdat_mesh_desc* mesh, const scdat_params* params, scdat_ctx* ctx)
+{
     ARG(mesh->n_nodes > 0 && mesh->n_tets > 0, "empty mesh");
     ARG(mesh->n_nodes < (int64_t)0x7fffffff && mesh->n_tets < (int64_t)0x7fffffff, "mesh too large for int32 indices");
     ARG(mesh->node_xyz && mesh->tet_nodes && mesh->node_dirichlet, "null mesh array");
@@ -671,20 +701,17 @@ SCDAT_API int scdat_create(const scdat_mesh_desc* mesh, const scdat_params* para
     CK(cudaMemsetAsync(ctx->ke_acc.p, 0, 2 * sizeof(unsigned long long), ctx->st));
     CK(ctx->nact.alloc(1));
     CK(cudaStreamSynchronize(st));
-    *out = holder.release();
     return SCDAT_OK;
 }
+
+}  // namespace
+
+extern "C" {
 
 SCDAT_API int scdat_destroy(scdat_ctx* ctx)
 {
     if (!ctx) return SCDAT_ERR_ARG;
-    if (ctx->st) cudaStreamSynchronize(ctx->st);
-    for (auto& pr : ctx->ev_push) { cudaEventDestroy(pr.first); cudaEventDestroy(pr.second); }
-    for (auto& pr : ctx->ev_field) { cudaEventDestroy(pr.first); cudaEventDestroy(pr.second); }
-    for (auto& pr : ctx->ev_sort) { cudaEventDestroy(pr.first); cudaEventDestroy(pr.second); }
-    cudaStream_t st = ctx->st;
-    delete ctx;
-    if (st) cudaStreamDestroy(st);
+    delete ctx;  // drains the stream, then releases events, stream and buffers
     return SCDAT_OK;
 }
 

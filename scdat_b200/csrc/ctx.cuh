@@ -139,6 +139,23 @@ struct scdat_ctx {
     int64_t push_launches = 0, field_solves = 0;
     int64_t push_particles = 0;
     int64_t launches = 0;  // kernels of this library launched since scdat_set_timing
+
+    // The context owns its stream and timing events, so a context that scdat_create abandons
+    // on an error releases them too.  The stream is drained first; the device buffers are
+    // freed after this body, by their own destructors.
+    scdat_ctx() = default;
+    scdat_ctx(const scdat_ctx&) = delete;
+    scdat_ctx& operator=(const scdat_ctx&) = delete;
+    ~scdat_ctx()
+    {
+        if (st) cudaStreamSynchronize(st);
+        for (auto* evs : {&ev_push, &ev_field, &ev_sort})
+            for (auto& pr : *evs) {
+                cudaEventDestroy(pr.first);
+                cudaEventDestroy(pr.second);
+            }
+        if (st) cudaStreamDestroy(st);
+    }
 };
 
 namespace scdat {

@@ -345,7 +345,8 @@ std::string flatten_mesh(const std::vector<Mesh::NodePtr>& nodes, const std::vec
     return "";
 }
 
-const char* err_of(scdat_ctx* ctx) { return ctx ? scdat_last_error(ctx) : "no device context"; }
+// with no context, the reason of this thread's last failed scdat_create
+const char* err_of(scdat_ctx* ctx) { return scdat_last_error(ctx); }
 
 }  // namespace
 

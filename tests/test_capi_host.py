@@ -56,3 +56,47 @@ def test_null_arguments_rejected():
     assert L.scdat_step(None, 1) == -1
     assert L.scdat_kuhn_box_mesh(0, 1, 1, 0.1, None, None, 0.0, 0.0, None, None, None, None, None, None, None,
                                  None) == -1
+
+
+def test_create_failure_reason_outlives_the_context():
+    """scdat_create frees a context it could not finish; scdat_last_error(NULL) still gives the
+    calling thread's reason.  The mesh and parameter checks run on the host before any CUDA
+    call, so this needs no GPU."""
+    import ctypes as C
+
+    L = capi.load()
+    m = capi.kuhn_box_mesh((2, 2, 2), 0.1)
+    xyz = np.ascontiguousarray(m["xyz"])
+    tet = np.ascontiguousarray(m["tet"]).copy()
+    dirichlet = np.ascontiguousarray(m["dirichlet"])
+    p = capi.Params()
+    L.scdat_default_params(p)
+    p.dt = 1e-9
+    md = capi.MeshDesc(len(xyz), len(tet), xyz.ctypes.data, tet.ctypes.data, None, dirichlet.ctypes.data, None)
+    h = C.c_void_p()
+
+    tet[3, 2] = len(xyz) + 5  # a node index past the end
+    assert L.scdat_create(C.byref(md), C.byref(p), C.byref(h)) == -1
+    assert not h.value
+    assert L.scdat_last_error(None) == b"tet node index out of range"
+
+    tet[3, 2] = 0
+    p.dt = 0.0
+    assert L.scdat_create(C.byref(md), C.byref(p), C.byref(h)) == -1
+    assert L.scdat_last_error(None) == b"dt must be positive"
+
+    md.n_nodes = 0
+    assert L.scdat_create(C.byref(md), C.byref(p), C.byref(h)) == -1
+    assert L.scdat_last_error(None) == b"empty mesh"
+
+    assert L.scdat_create(None, None, None) == -1
+    assert L.scdat_last_error(None) == b"scdat_create: null argument"
+    # the Python wrapper reports the same reason
+    bad = dict(m, tet=tet.copy())
+    bad["tet"][0, 0] = -1
+    try:
+        capi.Domain(bad["xyz"], bad["tet"], bad["dirichlet"], 1e-9)
+    except capi.ScdatError as e:
+        assert "tet node index out of range" in str(e)
+    else:
+        raise AssertionError("a mesh with a negative node index was accepted")
