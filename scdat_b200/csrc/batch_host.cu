@@ -487,10 +487,10 @@ SCDAT_API int scdat_batch_step(scdat_batch* b, int32_t n_steps)
             const int si = c->prm.sort_interval;
             if (si > 0) run = std::min<int64_t>(run, si - (c->steps % si));
         }
-        cudaEvent_t e0, e1;
-        BCK(cudaEventCreate(&e0));
-        BCK(cudaEventCreate(&e1));
-        BCK(cudaEventRecord(e0, b->st));
+        StageEvents ev;
+        BCK(cudaEventCreate(&ev.e0));
+        BCK(cudaEventCreate(&ev.e1));
+        BCK(cudaEventRecord(ev.e0, b->st));
         for (int k = 0; k < run; ++k) {
             if (b->tune.use_graph) {
                 BCK(cudaGraphLaunch(b->exec, b->st));
@@ -499,12 +499,10 @@ SCDAT_API int scdat_batch_step(scdat_batch* b, int32_t n_steps)
                 if (rc) return rc;
             }
         }
-        BCK(cudaEventRecord(e1, b->st));
-        BCK(cudaEventSynchronize(e1));
+        BCK(cudaEventRecord(ev.e1, b->st));
+        BCK(cudaEventSynchronize(ev.e1));
         float ms = 0.f;
-        BCK(cudaEventElapsedTime(&ms, e0, e1));
-        cudaEventDestroy(e0);
-        cudaEventDestroy(e1);
+        BCK(cudaEventElapsedTime(&ms, ev.e0, ev.e1));
         b->last_step_ms = ms / run;
         rc = after_steps(b, run);
         if (rc) return rc;

@@ -187,11 +187,11 @@ int do_push(scdat_ctx* ctx, bool do_mcc)
     CK(cudaMemsetAsync(ctx->ke_acc.p, 0, 2 * sizeof(unsigned long long), ctx->st));
     CK(cudaMemsetAsync(&ctx->led.p->active, 0, sizeof(unsigned long long), ctx->st));
     PushParams pp = push_params(ctx, do_mcc);
-    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    StageEvents ev;
     if (ctx->timing) {
-        CK(cudaEventCreate(&e0));
-        CK(cudaEventCreate(&e1));
-        CK(cudaEventRecord(e0, ctx->st));
+        CK(cudaEventCreate(&ev.e0));
+        CK(cudaEventCreate(&ev.e1));
+        CK(cudaEventRecord(ev.e0, ctx->st));
     }
     for (int s = 0; s < S; ++s) {
         if (ctx->species[s].cap == 0) continue;
@@ -213,8 +213,8 @@ int do_push(scdat_ctx* ctx, bool do_mcc)
     }
     CK(cudaGetLastError());
     if (ctx->timing) {
-        CK(cudaEventRecord(e1, ctx->st));
-        ctx->ev_push.emplace_back(e0, e1);
+        CK(cudaEventRecord(ev.e1, ctx->st));
+        ev.commit(ctx->ev_push);
         ctx->push_launches += 1;
     }
     CK(cudaMemsetAsync(ctx->totq.p, 0, sizeof(unsigned long long) * 2, ctx->st));
@@ -352,11 +352,11 @@ int run_pcg_mixed(scdat_ctx* ctx, double rtol, int max_iter, int& iters, double&
 int do_solve_field(scdat_ctx* ctx)
 {
     const PoissonView& A = ctx->pv;
-    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    StageEvents ev;
     if (ctx->timing) {
-        CK(cudaEventCreate(&e0));
-        CK(cudaEventCreate(&e1));
-        CK(cudaEventRecord(e0, ctx->st));
+        CK(cudaEventCreate(&ev.e0));
+        CK(cudaEventCreate(&ev.e1));
+        CK(cudaEventRecord(ev.e0, ctx->st));
     }
     if (A.R > 0) {
         ctx->launches += 3;
@@ -375,8 +375,8 @@ int do_solve_field(scdat_ctx* ctx)
     }
     int rc = do_lsq(ctx, 0.0);
     if (ctx->timing) {
-        CK(cudaEventRecord(e1, ctx->st));
-        ctx->ev_field.emplace_back(e0, e1);
+        CK(cudaEventRecord(ev.e1, ctx->st));
+        ev.commit(ctx->ev_field);
         ctx->field_solves += 1;
     }
     return rc;
@@ -443,11 +443,11 @@ int do_sort(scdat_ctx* ctx, int s)
     const uint32_t inactive = (uint32_t)ctx->hm.T;  // keys: tet, T (no hint), T+1 (inactive)
     int bits = 1;
     while (((uint64_t)1 << bits) <= (uint64_t)inactive + 1) ++bits;
-    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    StageEvents ev;
     if (ctx->timing) {
-        CK(cudaEventCreate(&e0));
-        CK(cudaEventCreate(&e1));
-        CK(cudaEventRecord(e0, ctx->st));
+        CK(cudaEventCreate(&ev.e0));
+        CK(cudaEventCreate(&ev.e1));
+        CK(cudaEventRecord(ev.e0, ctx->st));
     }
     ctx->launches += 2;  // keys + one gather of the whole store (the radix sort itself is CUB's)
     launch_sort_keys(n, S.tet.p, inactive, ctx->kin.p, ctx->vin.p, ctx->nact.p, ctx->st);
@@ -482,8 +482,8 @@ int do_sort(scdat_ctx* ctx, int s)
     S.id.swap(ctx->scratchu);
     CK(cudaGetLastError());
     if (ctx->timing) {
-        CK(cudaEventRecord(e1, ctx->st));
-        ctx->ev_sort.emplace_back(e0, e1);
+        CK(cudaEventRecord(ev.e1, ctx->st));
+        ev.commit(ctx->ev_sort);
         ctx->sorts += 1;
     }
     int64_t act = 0;

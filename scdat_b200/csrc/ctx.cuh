@@ -67,6 +67,25 @@ struct SpeciesState {
     DBuf<uint32_t> id;
 };
 
+// The start and end events of one timed stage.  An early error return destroys them; commit()
+// hands the recorded pair to a context's list, whose owner destroys it after reading it.
+struct StageEvents {
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    StageEvents() = default;
+    StageEvents(const StageEvents&) = delete;
+    StageEvents& operator=(const StageEvents&) = delete;
+    ~StageEvents()
+    {
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+    }
+    void commit(std::vector<std::pair<cudaEvent_t, cudaEvent_t>>& list)
+    {
+        list.emplace_back(e0, e1);
+        e0 = e1 = nullptr;
+    }
+};
+
 struct scdat_ctx {
     std::string err;
     scdat_params prm{};
