@@ -415,6 +415,9 @@ class Reference:
         L.ref_lsq_field.argtypes = [C.c_void_p, _dp, _dp]
         L.ref_cycle_run.argtypes = [C.c_void_p, C.c_int64, _dp, _dp, _i32p, _dp, _i32p, C.c_int, C.c_double, _i32p,
                                     _dp, C.POINTER(C.c_int64), _i64p, _i32p, _dp, _dp, _dp, _dp, _dp, _dp]
+        L.ref_cycle_mcc_run.argtypes = [C.c_void_p, C.c_int64, _dp, _dp, _i32p, _dp, _i32p, C.c_int, C.c_double,
+                                        _i32p, _dp, C.c_double, C.c_double, C.c_uint, C.POINTER(C.c_int64), _i64p,
+                                        _i32p, _dp, _dp, _dp, _dp, _dp, C.POINTER(C.c_int64)]
         L.ref_mcc_count.argtypes = [C.c_int64, _dp, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
                                     C.c_uint, C.c_int, C.POINTER(C.c_int64)]
         L.ref_mcc_count.restype = C.c_int64
@@ -499,6 +502,31 @@ class Reference:
         assert rc == 0, rc
         return dict(x=x, v=v, id=ids[:Pout.value] - 1, status=status, rho=rho, phi=phi, E=E.reshape(-1, 3),
                     ledger=ledger.reshape(6, 8), stats=stats, seconds=float(secs[0]))
+
+    def cycle_mcc(self, mesh, parts, species, nsteps, dt, face_bc, phi0, n_target, sigma, seed, neighbors=True):
+        """PICCycle steps, each followed by Collision::executeBackgroundMccStep with a constant
+        elastic cross-section for both species (ref_harness.cpp: ref_cycle_mcc_run).  The
+        container drops inactive particles after every MCC step: only active particles return,
+        with their 0-based ids."""
+        h = self.mesh(mesh, neighbors)
+        P = parts["x"].shape[0]
+        x = parts["x"].copy()
+        v = parts["v"].copy()
+        kind = np.array([species[s].kind for s in parts["species"]], np.int32)
+        w = np.array([species[s].w for s in parts["species"]], np.float64)
+        Pout, hits = C.c_int64(), C.c_int64()
+        ids = np.zeros(P, np.int64)
+        status = np.zeros(P, np.int32)
+        rho, phi, E = np.zeros(mesh.N), np.zeros(mesh.N), np.zeros(mesh.N * 3)
+        ledger, stats = np.zeros(6 * 8), np.zeros(5)
+        rc = self.L.ref_cycle_mcc_run(h, P, x.reshape(-1), v.reshape(-1), kind, w, parts["tet"].astype(np.int32),
+                                      nsteps, dt, np.asarray(face_bc, np.int32), np.ascontiguousarray(phi0, np.float64),
+                                      n_target, sigma, seed, C.byref(Pout), ids, status, rho, phi, E, ledger, stats,
+                                      C.byref(hits))
+        assert rc == 0, rc
+        n = Pout.value
+        return dict(x=x[:n], v=v[:n], id=ids[:n] - 1, status=status[:n], rho=rho, phi=phi, E=E.reshape(-1, 3),
+                    ledger=ledger.reshape(6, 8), stats=stats, hits=hits.value)
 
     def mcc_count(self, v, kind, w, sigma, n_target, dt, seed, repeats):
         """(first-draw hits as the handler counts them, particles actually scattered)"""

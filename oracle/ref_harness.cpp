@@ -192,14 +192,22 @@ int ref_poisson(void* h, const double* rho, double* phi, double* E)
     return 0;
 }
 
-// Run nsteps of PICCycle::executeTimeStep (fresh PoissonSolver per step so the system is
-// re-assembled, see PoissonSolver.cpp:387-392) and optionally the background MCC step.
-// face_bc[6]: 0 none, 1 absorbing(1.0), 2 periodic over the x and y box lengths.
-// Particles come back in container order with their ids (1-based insertion order).
-int ref_cycle_run(void* h, int64_t P, double* x, double* v, const int32_t* kind, const double* w,
-                  const int32_t* hint, int nsteps, double dt, const int32_t* face_bc, const double* phi0,
-                  int64_t* P_out, int64_t* id_out, int32_t* status_out, double* rho_out, double* phi_out,
-                  double* E_out, double* ledger_out, double* stats_out, double* seconds_out)
+}  // extern "C"
+
+namespace {
+
+// Constant elastic background collisions for both species (one process per species, as the
+// PIC-MCC driver configures them), run after every executeTimeStep.
+struct MccCfg {
+    double n_target, sigma;
+    unsigned seed;
+    int64_t* hits;  // the handler's collision count (first-draw hits) over the run
+};
+
+int cycle_run(void* h, int64_t P, double* x, double* v, const int32_t* kind, const double* w, const int32_t* hint,
+              int nsteps, double dt, const int32_t* face_bc, const double* phi0, int64_t* P_out, int64_t* id_out,
+              int32_t* status_out, double* rho_out, double* phi_out, double* E_out, double* ledger_out,
+              double* stats_out, double* seconds_out, const MccCfg* mcc)
 {
     auto* rm = static_cast<RefMesh*>(h);
     const auto& nodes = rm->mesh->getNodes();
@@ -232,11 +240,33 @@ int ref_cycle_run(void* h, int64_t P, double* x, double* v, const int32_t* kind,
     cycle.setPotential(phi);
     for (int64_t i = 0; i < P; ++i)
         if (hint[i] >= 0) cycle.addParticleLocation(pm->getParticle(ids[i]), (SP::ElementId)hint[i]);
+    using namespace SCDAT::Collision;
+    std::unique_ptr<MonteCarloCollisionHandler> handler;
+    BackgroundMccRuntimeConfig mcc_cfg;  // keeps the configured processes (no re-initialisation)
+    double volume = 1.0;
+    if (mcc) {
+        handler = std::make_unique<MonteCarloCollisionHandler>(mcc->seed);
+        handler->clearCollisionProcesses();
+        CollisionParameters cp;
+        cp.energy_threshold = 0.0;
+        cp.cross_section_max = mcc->sigma;
+        cp.additional_params["reference_energy"] = 1.0;
+        cp.additional_params["power_index"] = 0.0;  // constant cross-section
+        handler->addCollisionProcess("elastic_electron", CollisionProcessFactory::createElasticProcess(
+                                                             ParticleSpecies::ELECTRON, ParticleSpecies::NEUTRAL,
+                                                             mcc->n_target, cp));
+        handler->addCollisionProcess("elastic_ion", CollisionProcessFactory::createElasticProcess(
+                                                        ParticleSpecies::ION, ParticleSpecies::NEUTRAL,
+                                                        mcc->n_target, cp));
+        volume = (hi.x() - lo.x()) * (hi.y() - lo.y()) * (hi.z() - lo.z());
+    }
     auto t0 = std::chrono::steady_clock::now();
     for (int s = 0; s < nsteps; ++s) {
         cycle.setPoissonSolver(std::make_shared<SCDAT::FieldSolver::PoissonSolver>(rm->mesh));
         if (!cycle.executeTimeStep()) return 2;
+        if (mcc) executeBackgroundMccStep(pm->getContainer(), *handler, dt, volume, mcc_cfg);
     }
+    if (mcc && mcc->hits) *mcc->hits = (int64_t)handler->getStatistics().total_collisions;
     auto t1 = std::chrono::steady_clock::now();
     if (seconds_out) *seconds_out = std::chrono::duration<double>(t1 - t0).count();
     auto& cont = pm->getContainer();
@@ -278,6 +308,38 @@ int ref_cycle_run(void* h, int64_t P, double* x, double* v, const int32_t* kind,
     stats_out[3] = st.active_particles;
     stats_out[4] = st.surface_deposited_charge;
     return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+// Run nsteps of PICCycle::executeTimeStep (fresh PoissonSolver per step so the system is
+// re-assembled, see PoissonSolver.cpp:387-392).  face_bc[6]: 0 none, 1 absorbing(1.0),
+// 2 periodic over the x and y box lengths.  Particles come back in container order with their
+// ids (1-based insertion order).
+int ref_cycle_run(void* h, int64_t P, double* x, double* v, const int32_t* kind, const double* w,
+                  const int32_t* hint, int nsteps, double dt, const int32_t* face_bc, const double* phi0,
+                  int64_t* P_out, int64_t* id_out, int32_t* status_out, double* rho_out, double* phi_out,
+                  double* E_out, double* ledger_out, double* stats_out, double* seconds_out)
+{
+    return cycle_run(h, P, x, v, kind, w, hint, nsteps, dt, face_bc, phi0, P_out, id_out, status_out, rho_out,
+                     phi_out, E_out, ledger_out, stats_out, seconds_out, nullptr);
+}
+
+// The same run with Collision::executeBackgroundMccStep (CollisionPicAdapter.cpp:338-434) after
+// every step: a constant elastic cross-section sigma against neutrals of density n_target for
+// both species, the handler seeded with `seed`.  The container drops inactive particles after
+// each MCC step, so only active particles come back.  *hits: the handler's collision count.
+int ref_cycle_mcc_run(void* h, int64_t P, double* x, double* v, const int32_t* kind, const double* w,
+                      const int32_t* hint, int nsteps, double dt, const int32_t* face_bc, const double* phi0,
+                      double n_target, double sigma, unsigned seed, int64_t* P_out, int64_t* id_out,
+                      int32_t* status_out, double* rho_out, double* phi_out, double* E_out, double* ledger_out,
+                      double* stats_out, int64_t* hits)
+{
+    const MccCfg cfg{n_target, sigma, seed, hits};
+    return cycle_run(h, P, x, v, kind, w, hint, nsteps, dt, face_bc, phi0, P_out, id_out, status_out, rho_out,
+                     phi_out, E_out, ledger_out, stats_out, nullptr, &cfg);
 }
 
 // PICCycle::setPotential -> updateElectricField (LSQ with 1e-18 regularisation).

@@ -172,3 +172,67 @@ def test_mcc_statistics_match_reference(orc, ref):
     assert abs(ref_hits - m1) < 5 * s1, (ref_hits, m1, s1)
     assert abs(ref_scat - m2) < 5 * s2, (ref_scat, m2, s2)
     assert abs(hits - m2) < 5 * s2, (hits, m2, s2)
+
+
+def _oracle_mcc_run(orc, mesh, sp, parts, nsteps, dt, face_bc, n_t, sigma, seed):
+    """The oracle's PIC-MCC run in the reference's order: each step the cycle (push, boundary
+    events, field), then elastic MCC on Philox streams, then the absorbed particles leave the
+    container (Collision::executeBackgroundMccStep, CollisionPicAdapter.cpp:338-434)."""
+    procs = [O.Elastic(n_t, sigma, 1.0, 0.0, 0.0, 1, 0) for _ in sp]
+    cur = {k: v.copy() for k, v in parts.items()}
+    phi, ledger = mesh.phi_bc.copy(), np.zeros((7, 8))
+    for k in range(nsteps):
+        out = oracle_cycle(orc, mesh, sp, cur, 1, dt, face_bc, phi)
+        ledger += out["ledger"]
+        phi = out["phi"]
+        v = out["v"]
+        if n_t > 0:
+            v, _ = orc.mcc(out["v"], cur["species"], out["status"], cur["id"], sp, procs, dt, seed, k, mode=0)
+        act = out["status"] == O.ACTIVE
+        cur = {key: val[act] for key, val in cur.items()}
+        cur.update(x=out["x"][act], v=v[act], tet=out["tet"][act])
+    return cur, ledger
+
+
+def test_full_mcc_run_matches_reference_statistically(orc, ref):
+    """A full PIC-MCC run of the reference (PICCycle steps, each followed by its background MCC
+    step on one mt19937 stream) against the oracle's run on Philox streams, from the same
+    particles.  The streams cannot match, so the runs are compared statistically: per species
+    the mean x-velocity, the mean squared speed and the surviving count, and per face the
+    collected electron and ion counts, each within 5 sigma of the difference (the sampling
+    errors of the two runs added as if independent, which overstates them since the runs
+    share their initial state).  Electrons start with a +x drift of two thermal speeds and
+    collide often, so the drift left after the run measures the collisions: without MCC it
+    lies far outside the band.  The floating potential is not on this reference path (the
+    reference's PICCycle has no surface circuit), so it is not compared here."""
+    mesh = O.kuhn_box((6, 6, 6), 0.05)
+    ppc, nsteps, dt, sigma, n_t = 40, 8, 2e-8, 1e-19, 3e20
+    sp = O.plasma_species(1e10, 1.0, 1.0, 0.05, ppc)
+    parts = O.seed_particles(mesh, sp, ppc, 100)
+    vth = np.sqrt(O.QE / O.ME)
+    parts["v"][parts["species"] == 0, 0] += 2.0 * vth
+    face_bc = (1,) * 6
+    mine, led = _oracle_mcc_run(orc, mesh, sp, parts, nsteps, dt, face_bc, n_t, sigma, 1000)
+    theirs = ref.cycle_mcc(mesh, parts, sp, nsteps, dt, face_bc, mesh.phi_bc, n_t, sigma, 2000)
+    their_species = parts["species"][theirs["id"]]
+
+    def z_means(a, b):
+        return abs(a.mean() - b.mean()) / np.sqrt(a.var() / len(a) + b.var() / len(b))
+
+    for s in (0, 1):
+        a, b = mine["v"][mine["species"] == s], theirs["v"][their_species == s]
+        assert len(a) > 1000 and len(b) > 1000
+        assert z_means(a[:, 0], b[:, 0]) < 5.0, ("mean vx", s)
+        assert z_means((a ** 2).sum(1), (b ** 2).sum(1)) < 5.0, ("mean v^2", s)
+        assert abs(len(a) - len(b)) < 5.0 * np.sqrt(len(a) + len(b)), ("survivors", s)
+    for f in range(6):
+        for col in (4, 5):  # absorbed electron and ion macro-particles on face f
+            c1, c2 = led[f, col], theirs["ledger"][f, col]
+            assert abs(c1 - c2) < 5.0 * np.sqrt(c1 + c2 + 1.0), (f, col, c1, c2)
+    assert theirs["ledger"][1, 4] > 100  # the drift carries electrons to the +x face
+
+    # power: the same run without collisions keeps most of the drift
+    free, _ = _oracle_mcc_run(orc, mesh, sp, parts, nsteps, dt, face_bc, 0.0, sigma, 1000)
+    a = free["v"][free["species"] == 0][:, 0]
+    b = theirs["v"][their_species == 0][:, 0]
+    assert z_means(a, b) > 10.0
