@@ -11,7 +11,7 @@ import pytest
 import oracle as O
 from conftest import rel_err
 from golden.make_golden import CASES, make_inputs
-from pic_helpers import gpu_domain, gpu_load_particles, gpu_state, oracle_cycle
+from pic_helpers import gpu_domain, gpu_load_particles, gpu_state, oracle_cycle, oracle_mcc_run
 
 pytestmark = pytest.mark.gpu
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
@@ -140,6 +140,43 @@ def test_mcc_matches_oracle_streams(lib, orc, mode):
     assert np.array_equal(changed_g, changed_o)
     assert rel_err(st["v"], v) < TOL
     dom.close()
+
+
+def test_full_mcc_run_matches_oracle(lib, orc):
+    """Several full steps with elastic MCC (fused into the push) against the oracle's run in the
+    reference's order (cycle, then MCC, then inactive particles dropped) on the same Philox
+    streams: the same collisions, statuses and ledger counts, and states, fields and ledger
+    charges to 1e-12.  MCC changes velocities only, so running it inside the push, before the
+    field solve, gives the reference order's result."""
+    mesh = O.kuhn_box((4, 4, 4), 0.05)
+    sp = O.plasma_species(1e10, 1.0, 1.0, 0.05, 8)
+    parts = O.seed_particles(mesh, sp, 8, 33)
+    vth = np.sqrt(O.QE / O.ME)
+    parts["v"][parts["species"] == 0, 0] += 2.0 * vth  # drift into the +x face
+    dt, n_t, sigma, seed, nsteps, face_bc = 2e-8, 4e20, 1e-19, 777, 4, (1,) * 6
+    ref = oracle_mcc_run(orc, mesh, sp, parts, nsteps, dt, face_bc, n_t, sigma, seed)
+    dom = gpu_domain(mesh, dt, face_bc=face_bc, pcg_rtol=1e-15, pcg_max_iter=20000, body_tally=False, seed=seed)
+    gpu_load_particles(dom, sp, parts)
+    for s in range(len(sp)):
+        dom.set_elastic(s, n_t, sigma, mode=0)
+    dom.set_potential(mesh.phi_bc)
+    dom.step(nsteps)
+    st = gpu_state(dom, len(sp), len(parts["tet"]))
+    stats = dom.stats()
+    rho, phi, E = dom.fields()
+    led = dom.ledger()
+    dom.close()
+    assert stats["mcc_collisions"] == ref["hits"] and ref["hits"] > 200
+    ids = ref["parts"]["id"]
+    act = np.nonzero(st["status"] == O.ACTIVE)[0]
+    assert np.array_equal(np.sort(act), np.sort(ids))  # the same particles survive
+    assert np.abs(st["x"][ids] - ref["parts"]["x"]).max() <= TOL * np.abs(ref["parts"]["x"]).max()
+    assert rel_err(st["v"][ids], ref["parts"]["v"]) < TOL
+    assert rel_err(rho, ref["rho"]) < TOL
+    assert rel_err(phi, ref["phi"]) < TOL
+    assert rel_err(E, ref["E"]) < TOL
+    assert np.array_equal(led[:6, 4:6], ref["ledger"][:6, 4:6]) and led[1, 4] > 0
+    np.testing.assert_allclose(led[:6, [0, 1, 3]], ref["ledger"][:6, [0, 1, 3]], rtol=TOL, atol=1e-30)
 
 
 def test_picycle_boundary_scenarios(lib):

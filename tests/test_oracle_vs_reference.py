@@ -5,7 +5,7 @@ import pytest
 
 import oracle as O
 from conftest import rel_err
-from pic_helpers import oracle_cycle
+from pic_helpers import oracle_cycle, oracle_mcc_run
 
 
 def _setup(n=(5, 5, 5), body=((2, 3), (2, 3), (2, 3)), bias=-10.0, ppc=3, seed=5):
@@ -174,26 +174,6 @@ def test_mcc_statistics_match_reference(orc, ref):
     assert abs(hits - m2) < 5 * s2, (hits, m2, s2)
 
 
-def _oracle_mcc_run(orc, mesh, sp, parts, nsteps, dt, face_bc, n_t, sigma, seed):
-    """The oracle's PIC-MCC run in the reference's order: each step the cycle (push, boundary
-    events, field), then elastic MCC on Philox streams, then the absorbed particles leave the
-    container (Collision::executeBackgroundMccStep, CollisionPicAdapter.cpp:338-434)."""
-    procs = [O.Elastic(n_t, sigma, 1.0, 0.0, 0.0, 1, 0) for _ in sp]
-    cur = {k: v.copy() for k, v in parts.items()}
-    phi, ledger = mesh.phi_bc.copy(), np.zeros((7, 8))
-    for k in range(nsteps):
-        out = oracle_cycle(orc, mesh, sp, cur, 1, dt, face_bc, phi)
-        ledger += out["ledger"]
-        phi = out["phi"]
-        v = out["v"]
-        if n_t > 0:
-            v, _ = orc.mcc(out["v"], cur["species"], out["status"], cur["id"], sp, procs, dt, seed, k, mode=0)
-        act = out["status"] == O.ACTIVE
-        cur = {key: val[act] for key, val in cur.items()}
-        cur.update(x=out["x"][act], v=v[act], tet=out["tet"][act])
-    return cur, ledger
-
-
 def test_full_mcc_run_matches_reference_statistically(orc, ref):
     """A full PIC-MCC run of the reference (PICCycle steps, each followed by its background MCC
     step on one mt19937 stream) against the oracle's run on Philox streams, from the same
@@ -212,7 +192,8 @@ def test_full_mcc_run_matches_reference_statistically(orc, ref):
     vth = np.sqrt(O.QE / O.ME)
     parts["v"][parts["species"] == 0, 0] += 2.0 * vth
     face_bc = (1,) * 6
-    mine, led = _oracle_mcc_run(orc, mesh, sp, parts, nsteps, dt, face_bc, n_t, sigma, 1000)
+    run = oracle_mcc_run(orc, mesh, sp, parts, nsteps, dt, face_bc, n_t, sigma, 1000)
+    mine, led = run["parts"], run["ledger"]
     theirs = ref.cycle_mcc(mesh, parts, sp, nsteps, dt, face_bc, mesh.phi_bc, n_t, sigma, 2000)
     their_species = parts["species"][theirs["id"]]
 
@@ -232,7 +213,7 @@ def test_full_mcc_run_matches_reference_statistically(orc, ref):
     assert theirs["ledger"][1, 4] > 100  # the drift carries electrons to the +x face
 
     # power: the same run without collisions keeps most of the drift
-    free, _ = _oracle_mcc_run(orc, mesh, sp, parts, nsteps, dt, face_bc, 0.0, sigma, 1000)
+    free = oracle_mcc_run(orc, mesh, sp, parts, nsteps, dt, face_bc, 0.0, sigma, 1000)["parts"]
     a = free["v"][free["species"] == 0][:, 0]
     b = theirs["v"][their_species == 0][:, 0]
     assert z_means(a, b) > 10.0
