@@ -11,6 +11,7 @@ Only tests/, the smoke check and the benchmark's CPU-baseline leg import this mo
 """
 from __future__ import annotations
 
+import contextlib
 import ctypes as C
 import os
 import subprocess
@@ -263,10 +264,21 @@ ACTIVE, ABSORBED, ESCAPED = 0, 1, 2
 
 
 class Oracle:
-    def __init__(self):
+    """fast_locate: replace the reference's linear scan over all tets (the last step of
+    locateParticle) by the oracle's exact stand-in, a bin grid listing every tet that can hold
+    a point in ascending id order (scdat_oracle.c, orc_grid_create), so that meshes of 10^5
+    tets and more finish in seconds.  Both give the same tet for every point (tested)."""
+
+    def __init__(self, fast_locate: bool = False):
         build_oracle()
         L = C.CDLL(ORACLE_SO)
         self.L = L
+        self.fast_locate = fast_locate
+        self._grids = {}
+        L.orc_grid_create.argtypes = [_dp, _i32p, C.c_int64]
+        L.orc_grid_create.restype = C.c_void_p
+        L.orc_grid_destroy.argtypes = [C.c_void_p]
+        L.orc_grid_use.argtypes = [C.c_void_p]
         L.orc_philox4x32_10.argtypes = [_u32p, _u32p, _u32p]
         L.orc_barycentric.argtypes = [_dp, _i32p, C.c_int64, _dp, _dp]
         L.orc_barycentric.restype = C.c_int
@@ -289,6 +301,26 @@ class Oracle:
         L.orc_boris.argtypes = [_dp, _dp, C.c_double, C.c_double, _dp]
         L.orc_boris.restype = None
 
+    @contextlib.contextmanager
+    def _scan(self, mesh):
+        """Select the scan accelerator of `mesh` for the calls inside (fast_locate only)."""
+        if not self.fast_locate:
+            yield
+            return
+        key = id(mesh)
+        if key not in self._grids:
+            self._grids[key] = (mesh, self.L.orc_grid_create(mesh.xyz, mesh.tet, mesh.T))
+        self.L.orc_grid_use(self._grids[key][1])
+        try:
+            yield
+        finally:
+            self.L.orc_grid_use(None)
+
+    def close(self):
+        for _, g in self._grids.values():
+            self.L.orc_grid_destroy(g)
+        self._grids.clear()
+
     # -- RNG
     def philox(self, ctr, key):
         o = np.zeros(4, dtype=np.uint32)
@@ -303,7 +335,8 @@ class Oracle:
 
     def locate(self, mesh, p, hint=-1, neighbors=True):
         nb = _nullable(mesh.nbr, np.int32) if neighbors else None
-        return int(self.L.orc_locate_point(mesh.xyz, mesh.tet, nb, mesh.T, np.asarray(p, np.float64), int(hint)))
+        with self._scan(mesh):
+            return int(self.L.orc_locate_point(mesh.xyz, mesh.tet, nb, mesh.T, np.asarray(p, np.float64), int(hint)))
 
     # -- push
     def push(self, mesh, E, parts, species, dt, nseg=10, kernel=1, deposit=True, neighbors=True,
@@ -321,9 +354,10 @@ class Oracle:
         pp = PushParams(dt, floor_ratio, nseg, kernel, 1 if deposit else 0, 0)
         stats = PushStats()
         nb = _nullable(mesh.nbr, np.int32) if neighbors else None
-        self.L.orc_push(mesh.N, mesh.xyz, mesh.T, mesh.tet, nb, np.ascontiguousarray(E, np.float64).reshape(-1),
-                        P, x.reshape(-1), v.reshape(-1), parts["species"].astype(np.int32), tet, st, lost, sq, sm, sw,
-                        C.byref(pp), rho, C.byref(stats))
+        with self._scan(mesh):
+            self.L.orc_push(mesh.N, mesh.xyz, mesh.T, mesh.tet, nb, np.ascontiguousarray(E, np.float64).reshape(-1),
+                            P, x.reshape(-1), v.reshape(-1), parts["species"].astype(np.int32), tet, st, lost, sq, sm,
+                            sw, C.byref(pp), rho, C.byref(stats))
         return dict(x=x, v=v, tet=tet, lost=lost, status=st, rho=rho, substeps=stats.substeps,
                     nlost=stats.lost)
 
@@ -345,9 +379,10 @@ class Oracle:
         sm = np.array([s.m for s in species])
         sw = np.array([s.w for s in species])
         nb = _nullable(mesh.nbr, np.int32) if neighbors else None
-        self.L.orc_boundary(mesh.T, mesh.xyz, mesh.tet, nb, P, out["x"].reshape(-1), out["v"].reshape(-1),
-                            parts["species"].astype(np.int32), out["tet"], out["status"], out["lost"], sq, sm, sw,
-                            C.byref(b), ledger, sc)
+        with self._scan(mesh):
+            self.L.orc_boundary(mesh.T, mesh.xyz, mesh.tet, nb, P, out["x"].reshape(-1), out["v"].reshape(-1),
+                                parts["species"].astype(np.int32), out["tet"], out["status"], out["lost"], sq, sm, sw,
+                                C.byref(b), ledger, sc)
         out["ledger"] = ledger.reshape(7, 8)
         out["surface_charge"] = float(sc[0])
         return out

@@ -117,6 +117,144 @@ ORC_API int orc_barycentric(const double* xyz, const int32_t* tet4, int64_t t, c
     return orc_bary(xyz, tet4, t, q, lam);
 }
 
+/* Scan accelerator for the linear scan below (an exact stand-in, not a different rule).
+ * Uniform bins over the mesh's bounding box; each bin lists, in ascending id order, every tet
+ * whose bounding box -- widened by 1e-6 of its diagonal, far more than the 1e-8 barycentric
+ * tolerance lets a containing point lie outside the tet -- overlaps the bin.  Every tet that
+ * contains a point p is therefore listed in p's bin, so the first containing tet of that
+ * list is the lowest-id containing tet, which is what the linear scan returns.  A point
+ * outside every widened box is in no tet.  Bin indices of boxes and points come from the same
+ * monotone expression, so a point on a bin face finds the tets listed for its bin.  Used only
+ * while orc_grid_use() has selected a grid built for the same tet array. */
+typedef struct {
+    const int32_t* tet4;
+    int64_t T;
+    double lo[3], hi[3], inv[3];
+    int n[3];
+    int64_t* start; /* [bins+1] */
+    int32_t* ids;
+} orc_grid;
+
+static const orc_grid* g_locate_grid = NULL;
+
+static int grid_axis_bin(const orc_grid* g, int a, double x)
+{
+    int b = (int)floor((x - g->lo[a]) * g->inv[a]);
+    return b < 0 ? 0 : (b >= g->n[a] ? g->n[a] - 1 : b);
+}
+
+static void tet_box(const double* xyz, const int32_t* tn, double lo[3], double hi[3])
+{
+    for (int a = 0; a < 3; ++a) {
+        lo[a] = hi[a] = xyz[3 * tn[0] + a];
+        for (int k = 1; k < 4; ++k) {
+            double v = xyz[3 * tn[k] + a];
+            if (v < lo[a]) lo[a] = v;
+            if (v > hi[a]) hi[a] = v;
+        }
+    }
+    double d = sqrt((hi[0] - lo[0]) * (hi[0] - lo[0]) + (hi[1] - lo[1]) * (hi[1] - lo[1]) +
+                    (hi[2] - lo[2]) * (hi[2] - lo[2]));
+    for (int a = 0; a < 3; ++a) {
+        lo[a] -= 1e-6 * d;
+        hi[a] += 1e-6 * d;
+    }
+}
+
+ORC_API void* orc_grid_create(const double* xyz, const int32_t* tet4, int64_t T)
+{
+    if (T <= 0) return NULL;
+    orc_grid* g = (orc_grid*)calloc(1, sizeof(orc_grid));
+    g->tet4 = tet4;
+    g->T = T;
+    for (int64_t t = 0; t < T; ++t) {
+        double lo[3], hi[3];
+        tet_box(xyz, tet4 + 4 * t, lo, hi);
+        for (int a = 0; a < 3; ++a) {
+            if (t == 0 || lo[a] < g->lo[a]) g->lo[a] = lo[a];
+            if (t == 0 || hi[a] > g->hi[a]) g->hi[a] = hi[a];
+        }
+    }
+    /* about two tets per bin */
+    double ext[3], vol = 1.0;
+    for (int a = 0; a < 3; ++a) {
+        ext[a] = g->hi[a] - g->lo[a];
+        if (ext[a] <= 0.0) ext[a] = 1.0;
+        vol *= ext[a];
+    }
+    double cell = cbrt(vol / ((double)T / 2.0 + 1.0));
+    int64_t bins = 1;
+    for (int a = 0; a < 3; ++a) {
+        int n = (int)ceil(ext[a] / cell);
+        g->n[a] = n < 1 ? 1 : (n > 1024 ? 1024 : n);
+        g->inv[a] = (double)g->n[a] / ext[a];
+        bins *= g->n[a];
+    }
+    g->start = (int64_t*)calloc((size_t)bins + 1, sizeof(int64_t));
+    for (int pass = 0; pass < 2; ++pass) {
+        int64_t* fill = NULL;
+        if (pass == 1) {
+            for (int64_t b = 0; b < bins; ++b) g->start[b + 1] += g->start[b];
+            g->ids = (int32_t*)malloc(sizeof(int32_t) * (size_t)(g->start[bins] > 0 ? g->start[bins] : 1));
+            fill = (int64_t*)malloc(sizeof(int64_t) * (size_t)bins);
+            memcpy(fill, g->start, sizeof(int64_t) * (size_t)bins);
+        }
+        for (int64_t t = 0; t < T; ++t) { /* ascending t: each bin's list is sorted */
+            double lo[3], hi[3];
+            tet_box(xyz, tet4 + 4 * t, lo, hi);
+            int b0[3], b1[3];
+            for (int a = 0; a < 3; ++a) {
+                b0[a] = grid_axis_bin(g, a, lo[a]);
+                b1[a] = grid_axis_bin(g, a, hi[a]);
+            }
+            for (int k = b0[2]; k <= b1[2]; ++k)
+                for (int j = b0[1]; j <= b1[1]; ++j)
+                    for (int i = b0[0]; i <= b1[0]; ++i) {
+                        int64_t b = i + (int64_t)g->n[0] * (j + (int64_t)g->n[1] * k);
+                        if (pass == 0)
+                            g->start[b + 1] += 1;
+                        else
+                            g->ids[fill[b]++] = (int32_t)t;
+                    }
+        }
+        free(fill);
+    }
+    return g;
+}
+
+ORC_API void orc_grid_destroy(void* h)
+{
+    orc_grid* g = (orc_grid*)h;
+    if (!g) return;
+    if (g_locate_grid == g) g_locate_grid = NULL;
+    free(g->start);
+    free(g->ids);
+    free(g);
+}
+
+/* Select the grid the scan uses (NULL: the plain linear scan). */
+ORC_API void orc_grid_use(void* h) { g_locate_grid = (const orc_grid*)h; }
+
+/* The lowest-id tet containing p: the linear scan of locateParticle, or its exact stand-in. */
+static int64_t orc_scan(const double* xyz, const int32_t* tet4, int64_t T, v3 p)
+{
+    double lam[4];
+    const orc_grid* g = g_locate_grid;
+    if (g && g->tet4 == tet4 && g->T == T) {
+        const double c[3] = {p.x, p.y, p.z};
+        for (int a = 0; a < 3; ++a)
+            if (!(c[a] >= g->lo[a] && c[a] <= g->hi[a])) return -1;
+        int64_t b = grid_axis_bin(g, 0, c[0]) +
+                    (int64_t)g->n[0] * (grid_axis_bin(g, 1, c[1]) + (int64_t)g->n[1] * grid_axis_bin(g, 2, c[2]));
+        for (int64_t e = g->start[b]; e < g->start[b + 1]; ++e)
+            if (orc_bary(xyz, tet4, g->ids[e], p, lam)) return g->ids[e];
+        return -1;
+    }
+    for (int64_t t = 0; t < T; ++t)
+        if (orc_bary(xyz, tet4, t, p, lam)) return t;
+    return -1;
+}
+
 /* CrossTetrahedron::locateParticle, PICParticleAlgorithms.cpp:853-891: the hint, then the
  * hint's neighbour list in order (nbr4 row, -1 entries skipped; nbr4 == NULL means the
  * lists are empty, as the reference ships), then the lowest-id tet of a linear scan. */
@@ -133,9 +271,7 @@ static int64_t orc_locate(const double* xyz, const int32_t* tet4, const int32_t*
             }
         }
     }
-    for (int64_t t = 0; t < T; ++t)
-        if (orc_bary(xyz, tet4, t, p, lam)) return t;
-    return -1;
+    return orc_scan(xyz, tet4, T, p);
 }
 
 ORC_API int64_t orc_locate_point(const double* xyz, const int32_t* tet4, const int32_t* nbr4, int64_t T,

@@ -6,6 +6,7 @@ shared library.  ``load()`` raises when libscdat_b200.so is missing -- there is 
 from __future__ import annotations
 
 import ctypes as C
+import weakref
 import os
 
 import numpy as np
@@ -249,6 +250,7 @@ class Domain:
             raise ScdatError(rc, "scdat_create: " + self.L.scdat_last_error(None).decode())
         self.h = h
         self.nspecies = 0
+        self._batches = weakref.WeakSet()  # Batches holding this Domain
 
     def _ck(self, rc):
         if rc != 0:
@@ -256,8 +258,13 @@ class Domain:
         return rc
 
     def close(self):
+        # A Batch's graph points into this Domain's buffers, and the library refuses to destroy a
+        # context a batch still holds: close those batches first.  This also holds when the
+        # garbage collector finalises a cycle holding both in an arbitrary order.
+        for b in list(getattr(self, "_batches", ())):
+            b.close()
         if getattr(self, "h", None):
-            self.L.scdat_destroy(self.h)
+            self._ck(self.L.scdat_destroy(self.h))
             self.h = None
 
     def __del__(self):
@@ -265,6 +272,10 @@ class Domain:
             self.close()
         except Exception:
             pass
+
+    def rows(self):
+        """Interior (non-Dirichlet) nodes: the rows of the reduced Poisson system."""
+        return int(np.count_nonzero(self.dirichlet == 0))
 
     def set_species(self, species):
         arr = (SpeciesC * len(species))(*[SpeciesC(s.q, s.m, s.w, 1 if s.q < 0 else 0, 0) for s in species])
@@ -464,6 +475,8 @@ class Batch:
                 self.L.scdat_batch_destroy(h)
             self.h = None
             raise ScdatError(rc, msg)
+        for d in self.domains:
+            d._batches.add(self)
         t = self.tuning()
         t.use_graph = 1 if use_graph else 0
         if push_blocks_per_sm:
@@ -513,6 +526,8 @@ class Batch:
         if getattr(self, "h", None):
             self.L.scdat_batch_destroy(self.h)
             self.h = None
+            for d in getattr(self, "domains", ()):
+                d._batches.discard(self)
 
     def __del__(self):
         try:

@@ -112,7 +112,7 @@ __global__ void k_batch_inner_setup(const FieldJob* __restrict__ jobs, int njobs
         PcgScalars* o = jobs[k].sco;
         if (o->done) continue;
         const double bb = o->bb > 0.0 ? o->bb : 1.0;
-        if (o->rr <= o->rtol * o->rtol * bb || o->iter >= o->max_iter || o->outer >= 12) {
+        if (o->rr <= o->rtol * o->rtol * bb || o->iter >= o->max_iter || o->outer >= kMaxRefinePasses) {
             o->done = 1;
             continue;
         }

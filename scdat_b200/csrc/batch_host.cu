@@ -74,12 +74,17 @@ struct scdat_batch {
     int64_t steps = 0;
     double last_step_ms = 0.0;
 
+    // Drains the batch's streams before anything is released (work still in flight writes into
+    // the contexts' buffers), then lets the contexts go.
     ~scdat_batch()
     {
+        for (cudaStream_t s : {st, st2, st3})
+            if (s) cudaStreamSynchronize(s);
         release_graph();
         if (any_host) cudaFreeHost(any_host);
         for (cudaStream_t s : {st, st2, st3})
             if (s) cudaStreamDestroy(s);
+        for (scdat_ctx* c : ctx) --c->batch_refs;
     }
     void release_graph()
     {
@@ -370,6 +375,7 @@ SCDAT_API int scdat_batch_create(int32_t n, scdat_ctx* const* ctxs, scdat_batch*
             return SCDAT_ERR_STATE;
         }
         b->ctx.push_back(c);
+        ++c->batch_refs;
         njobs += (int)c->species.size();
     }
     if (njobs > kMaxBatchJobs) {

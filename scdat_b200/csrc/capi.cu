@@ -305,7 +305,9 @@ int run_pcg_mixed(scdat_ctx* ctx, double rtol, int max_iter, int& iters, double&
     iters = 0;
     relres = 0.0;
     PcgScalars h{};
-    for (int outer = 0; outer < 12; ++outer) {
+    // every pass ends with the FP64 residual of the corrected x, so relres always describes the
+    // returned solution, also when the pass cap ends the loop
+    for (int outer = 0;; ++outer) {
         ++ctx->launches;
         launch_residual64(A, ctx->b.p, ctx->x.p, ctx->r.p, ctx->rf.p, ctx->sc.p, ctx->part.p, ctx->grid_red, ctx->st);
         CK(cudaGetLastError());
@@ -313,7 +315,7 @@ int run_pcg_mixed(scdat_ctx* ctx, double rtol, int max_iter, int& iters, double&
         if (rc) return rc;
         double bb = h.bb > 0.0 ? h.bb : 1.0;
         relres = std::sqrt(h.rr / bb);
-        if (h.rr <= rtol * rtol * bb || iters >= max_iter) break;
+        if (h.rr <= rtol * rtol * bb || iters >= max_iter || outer == kMaxRefinePasses) break;
         // inner FP32 solve A e = r from e = 0, to the tolerance this pass needs
         ctx->launches += 2;
         launch_zero_f32(R, ctx->xf.p, ctx->grid_red, ctx->st);
@@ -711,6 +713,10 @@ extern "C" {
 SCDAT_API int scdat_destroy(scdat_ctx* ctx)
 {
     if (!ctx) return SCDAT_ERR_ARG;
+    if (ctx->batch_refs > 0) {
+        ctx->err = "context is held by a batch: destroy the batch first";
+        return SCDAT_ERR_STATE;
+    }
     delete ctx;  // drains the stream, then releases events, stream and buffers
     return SCDAT_OK;
 }
@@ -1275,8 +1281,10 @@ SCDAT_API int scdat_solve_field(scdat_ctx* ctx)
     int rc = do_solve_field(ctx);
     if (rc) return rc;
     CK(cudaStreamSynchronize(ctx->st));
-    if (ctx->last_pcg_iter >= ctx->prm.pcg_max_iter && ctx->last_pcg_rel > ctx->prm.pcg_rtol) {
-        ctx->err = "field solve reached its iteration cap";
+    if (!(ctx->last_pcg_rel <= ctx->prm.pcg_rtol)) {
+        ctx->err = ctx->last_pcg_iter >= ctx->prm.pcg_max_iter
+                       ? "field solve reached its iteration cap"
+                       : "field solve stopped above its tolerance (refinement pass cap, CG breakdown or non-finite residual)";
         return SCDAT_ERR_NOT_CONVERGED;
     }
     return SCDAT_OK;

@@ -158,6 +158,10 @@ struct scdat_ctx {
     int64_t push_launches = 0, field_solves = 0;
     int64_t push_particles = 0;
     int64_t launches = 0;  // kernels of this library launched since scdat_set_timing
+    // batches that hold this context (scdat_batch_create / scdat_batch_destroy); a batch's
+    // captured graph and job tables point into the context's buffers, so scdat_destroy refuses
+    // while it is non-zero
+    int batch_refs = 0;
 
     // The context owns its stream and timing events, so a context that scdat_create abandons
     // on an error releases them too.  The stream is drained first; the device buffers are

@@ -36,6 +36,10 @@ struct PcgScalars {
 // rtol in this pass with a factor-4 margin, but no tighter than 1e-5 (what an FP32 Jacobi-PCG
 // reliably reaches) and no looser than 1e-1.  The host-driven and the graph-driven loops both
 // call it, so they take the same passes.
+// Refinement passes of the mixed solve (FP32 inner solve + FP64 correction) before it stops;
+// the FP64 residual of the last corrected x is still computed and reported.
+constexpr int kMaxRefinePasses = 12;
+
 __host__ __device__ inline double inner_rtol(double rr, double bb, double rtol)
 {
     const double need = 0.25 * rtol * sqrt(bb / rr);

@@ -109,5 +109,9 @@ extern "C" SCDAT_API int scdat_pcg_csr(int32_t R, const int32_t* row_ptr, const 
     if (e != cudaSuccess) return SCDAT_ERR_CUDA;
     if (iterations) *iterations = it;
     if (relres) *relres = rel;
-    return (it >= max_iter && rel > rtol) ? SCDAT_ERR_NOT_CONVERGED : SCDAT_OK;
+    // converged only when the residual test holds: an iteration cap, a CG breakdown (p.Ap <= 0,
+    // e.g. an indefinite matrix) or a non-finite residual (a zero diagonal entry) all report
+    // NOT_CONVERGED, as LinearSystem::conjugateGradient returns false on |pAp| < 1e-30
+    // (LinearSystem.cpp:258-327)
+    return (rel <= rtol) ? SCDAT_OK : SCDAT_ERR_NOT_CONVERGED;
 }

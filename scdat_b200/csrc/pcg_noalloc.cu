@@ -71,5 +71,6 @@ extern "C" SCDAT_API int scdat_pcg_csr_noalloc(int32_t R, const int32_t* row_ptr
     if (e != cudaSuccess) return SCDAT_ERR_CUDA;
     if (iterations) *iterations = it;
     if (relres) *relres = rel;
-    return (it >= max_iter && rel > rtol) ? SCDAT_ERR_NOT_CONVERGED : SCDAT_OK;
+    // same status rule as scdat_pcg_csr: anything short of the residual test is NOT_CONVERGED
+    return (rel <= rtol) ? SCDAT_OK : SCDAT_ERR_NOT_CONVERGED;
 }

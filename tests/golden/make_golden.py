@@ -3,7 +3,8 @@
 Run in a checkout where the reference tree is present and oracle/_ref was built
 (`make -C oracle ref`):
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py            # the small cases
+    python tests/golden/make_golden.py config0    # config0_ref.npz, the 32^3 configuration
 
 Every fixture is produced by the reference's own classes (CrossTetrahedron, PoissonSolver,
 PICCycle) through oracle/ref_harness.cpp on identical, seeded mesh and particle state.
@@ -35,9 +36,58 @@ def make_inputs(case):
     return mesh, sp, parts, dt, nsteps, face_bc
 
 
+# The first benchmark configuration at its full size: 32^3 hex cells of 0.05 m x 6 tets, the
+# 8^3-cell body (cells 12..19 per axis) at -10 V, outer faces at 0 V, electrons and H+ at
+# 1e10 m^-3 and 1 eV, 20 particles per cell per species, dt = 2e-8 s.
+CONFIG0 = dict(n=(32, 32, 32), h=0.05, body=((12, 20), (12, 20), (12, 20)), bias=-10.0, ppc=20, seed=2024, dt=2e-8)
+# every CONFIG0_STRIDE-th particle of the seeded population goes through the reference push
+CONFIG0_STRIDE = 315
+
+
+def make_config0_inputs():
+    c = CONFIG0
+    mesh = O.kuhn_box(c["n"], c["h"], body=c["body"], bias=c["bias"])
+    sp = O.plasma_species(1e10, 1.0, 1.0, c["h"], c["ppc"])
+    parts = O.seed_particles(mesh, sp, c["ppc"], c["seed"])
+    return mesh, sp, parts, c["dt"]
+
+
+def config0_laplace(o, mesh):
+    """Laplace potential of the configuration by the oracle's CG to 1e-14 (the reference's dense
+    PoissonSolver needs ~10 GB at this size); deterministic, so the GPU tests recompute it."""
+    A = o.assemble(mesh)
+    phi, _, _ = o.poisson(mesh, A, np.zeros(mesh.N), mesh.phi_bc, rtol=1e-14)
+    return A, phi
+
+
+def subsample(parts, stride):
+    return {k: (v[::stride].copy() if isinstance(v, np.ndarray) and v.shape[:1] == parts["tet"].shape else v)
+            for k, v in parts.items()}
+
+
+def make_config0(o, r):
+    mesh, sp, parts, dt = make_config0_inputs()
+    _, phi = config0_laplace(o, mesh)
+    E = r.lsq(mesh, phi)  # PICCycle::setPotential's LSQ field, by the reference
+    sub = subsample(parts, CONFIG0_STRIDE)
+    push = r.push(mesh, E, sub, sp, dt)  # CrossTetrahedron with neighbour lists filled
+    nz = np.nonzero(push["rho"])[0]
+    np.savez_compressed(
+        os.path.join(HERE, "config0_ref.npz"),
+        phi_sum=np.sum(phi), phi_abs_sum=np.sum(np.abs(phi)), E_abs_sum=np.sum(np.abs(E)),
+        push_x=push["x"], push_v=push["v"], push_tet=push["tet"], push_lost=push["lost"],
+        push_substeps=push["substeps"], rho_nodes=nz.astype(np.int32), rho_vals=push["rho"][nz],
+    )
+    print("config0", mesh.N, mesh.T, parts["x"].shape[0], sub["x"].shape[0])
+
+
 def main():
     o = O.Oracle()
     r = O.Reference()
+    if len(sys.argv) > 1 and sys.argv[1] == "config0":
+        make_config0(O.Oracle(fast_locate=True), r)
+        r.close()
+        return
     for case in CASES:
         mesh, sp, parts, dt, nsteps, face_bc = make_inputs(case)
         A = o.assemble(mesh)

@@ -136,3 +136,39 @@ def test_batch_rejects_fp64_contexts(lib):
     with pytest.raises(capi.ScdatError):
         capi.Batch([dom])
     dom.close()
+
+
+def test_batch_lifetime(lib):
+    """A batch's graph and job tables point into its contexts' buffers.  The library refuses to
+    destroy a context while a batch holds it; Domain.close closes such a batch first (also when
+    the garbage collector finalises both in either order); and a batch destroyed before its
+    contexts leaves nothing behind: a new context afterwards steps bitwise as in a process that
+    never had a batch."""
+    from scdat_b200 import capi
+
+    dom, sp, parts = _scenario(0)
+    dom.step(2)
+    ref = _state(dom, sp, parts)
+    dom.close()
+
+    dom, sp, parts = _scenario(1)
+    b = capi.Batch([dom])
+    b.step(2)
+    assert lib.scdat_destroy(dom.h) == -3  # SCDAT_ERR_STATE: held by a batch
+    assert b"batch" in lib.scdat_last_error(dom.h)
+    dom.close()  # closes the batch, then the context
+    assert b.h is None and dom.h is None
+
+    dom, sp, parts = _scenario(1)
+    b = capi.Batch([dom])
+    b.step(1)
+    b.close()  # batch first, then the context
+    assert lib.scdat_destroy(dom.h) == 0
+    dom.h = None
+
+    dom, sp, parts = _scenario(0)
+    dom.step(2)
+    got = _state(dom, sp, parts)
+    dom.close()
+    for key in ("rho", "phi", "E", "ledger", "x", "v", "tet", "status"):
+        assert np.array_equal(np.nan_to_num(got[key]), np.nan_to_num(ref[key])), key
