@@ -456,6 +456,10 @@ class Reference:
         L.ref_mcc_count.argtypes = [C.c_int64, _dp, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
                                     C.c_uint, C.c_int, C.POINTER(C.c_int64)]
         L.ref_mcc_count.restype = C.c_int64
+        L.ref_circuit_advance.argtypes = [C.c_int, _dp, _dp, _dp, _dp, _dp, C.c_double, _dp]
+        L.ref_circuit_advance.restype = C.c_int
+        L.ref_whipple_yield.argtypes = [C.c_double, C.c_double, C.c_int, _dp, _dp]
+        L.ref_whipple_yield.restype = None
         self._meshes = {}
 
     def mesh(self, mesh: BoxMesh, neighbors=True):
@@ -562,6 +566,20 @@ class Reference:
         n = Pout.value
         return dict(x=x[:n], v=v[:n], id=ids[:n] - 1, status=status[:n], rho=rho, phi=phi, E=E.reshape(-1, 3),
                     ledger=ledger.reshape(6, 8), stats=stats, hits=hits.value)
+
+    def circuit_advance(self, C_f, G_s, V0, I_a, didv, dt):
+        """SurfaceCircuitCoupling::advanceImplicit over independent nodes: the new potentials."""
+        a = [np.ascontiguousarray(v, np.float64) for v in (C_f, G_s, V0, I_a, didv)]
+        out = np.zeros(len(a[0]))
+        assert self.L.ref_circuit_advance(len(out), *a, float(dt), out) == 0
+        return out
+
+    def whipple_yield(self, peak_yield, peak_energy_ev, e_ev):
+        """evaluateLegacySecondaryElectronYield(Whipple) of a material with these peaks."""
+        e = np.ascontiguousarray(e_ev, np.float64)
+        out = np.zeros(len(e))
+        self.L.ref_whipple_yield(float(peak_yield), float(peak_energy_ev), len(e), e, out)
+        return out
 
     def mcc_count(self, v, kind, w, sigma, n_target, dt, seed, repeats):
         """(first-draw hits as the handler counts them, particles actually scattered)"""

@@ -8,11 +8,16 @@
 //   PICCycle::setPotential (nodal LSQ field)    Tools/PICcore/include/PICCycle.h:105-120
 //   PICCycle::executeTimeStep                   Tools/PICcore/src/PICCycle.cpp:311-416
 //   Collision::executeBackgroundMccStep         Tools/Interactions/Collisions/include/CollisionPicAdapter.h:64-75
+//   SurfaceCircuitCoupling::advanceImplicit     Tools/Coupling/src/SurfaceCircuitCoupling.cpp:866-1126
+//   evaluateLegacySecondaryElectronYield        Tools/Material/src/SurfaceMaterialModel.cpp:620-636
 // Only the parity tests and the CPU reference arm of the benchmark load it.
 #include "PICcore/include/PICCycle.h"
 #include "Mesh/include/MeshParsing.h"
 #include "Particle/include/ParticleManager.h"
 #include "Interactions/Collisions/include/CollisionPicAdapter.h"
+#include "Coupling/include/SurfaceCircuitCoupling.h"
+#include "Material/include/MaterialProperty.h"
+#include "Material/include/SurfaceMaterialModel.h"
 
 #include <chrono>
 #include <cstdint>
@@ -394,6 +399,41 @@ int64_t ref_mcc_count(int64_t P, const double* v, int kind, double w, double sig
     total = (int64_t)handler.getStatistics().total_collisions;
     if (scattered) *scattered = changed;
     return total;
+}
+
+// One implicit advance of n independent circuit nodes (capacitance C, shunt conductance G to
+// ground, potential V0, linearised plasma current I and dI/dV) by the reference's
+// SurfaceCircuitCoupling; the new potentials go to V.
+int ref_circuit_advance(int n, const double* C, const double* G, const double* V0, const double* I,
+                        const double* dIdV, double dt, double* V)
+{
+    SCDAT::Coupling::SurfaceCircuitCoupling circuit;
+    SCDAT::Coupling::SurfaceCircuitLinearization lin;
+    for (int k = 0; k < n; ++k) {
+        SCDAT::Coupling::SurfaceCircuitNode node;
+        node.potential_v = V0[k];
+        node.capacitance_f = C[k];
+        node.shunt_conductance_s = G[k];
+        circuit.addNode(node);
+        lin.plasma_current_a.push_back(I[k]);
+        lin.plasma_didv_a_per_v.push_back(dIdV[k]);
+    }
+    const auto r = circuit.advanceImplicit(dt, lin);
+    if (!r.converged || (int)r.node_potentials_v.size() != n) return 1;
+    for (int k = 0; k < n; ++k) V[k] = r.node_potentials_v[k];
+    return 0;
+}
+
+// The reference's Whipple secondary-electron yield of a material with the given peak yield and
+// peak energy, at each incident energy.
+void ref_whipple_yield(double peak_yield, double peak_energy_ev, int n, const double* e_ev, double* out)
+{
+    SCDAT::Material::MaterialProperty mat;
+    mat.setSecondaryElectronYield(peak_yield);
+    mat.setScalarProperty("secondary_yield_peak_energy_ev", peak_energy_ev);
+    for (int k = 0; k < n; ++k)
+        out[k] = SCDAT::Material::evaluateLegacySecondaryElectronYield(
+            mat, SCDAT::Material::LegacySecondaryYieldModel::Whipple, e_ev[k]);
 }
 
 }  // extern "C"

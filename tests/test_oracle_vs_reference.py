@@ -217,3 +217,42 @@ def test_full_mcc_run_matches_reference_statistically(orc, ref):
     a = free["v"][free["species"] == 0][:, 0]
     b = theirs["v"][their_species == 0][:, 0]
     assert z_means(a, b) > 10.0
+
+
+def test_surface_circuit_matches_reference(ref):
+    """The oracle's face-potential update (the device's rule) against the reference's
+    SurfaceCircuitCoupling::advanceImplicit on random independent nodes: capacitances of
+    dielectric patches, shunt conductances, plasma currents and their linearisation."""
+    rng = np.random.default_rng(17)
+    mesh = O.kuhn_box((4, 4, 4), 0.05, body=((1, 3), (1, 3), (1, 3)), bias=0.0)
+    for trial in range(200):
+        sc = O.SurfaceCircuit(mesh, (0.05, 0.05, 0.05), (0.15, 0.15, 0.15), eps_r=rng.uniform(1, 10),
+                              thickness=10 ** rng.uniform(-5, -2))
+        sc.C = sc.C * rng.uniform(0.5, 2.0, 6)
+        sc.G = np.where(rng.random(6) < 0.5, 0.0, 10 ** rng.uniform(-12, -6, 6))
+        sc.didv = np.where(rng.random(6) < 0.3, 0.0, -(10 ** rng.uniform(-12, -6, 6)))
+        sc.V = rng.uniform(-1000.0, 100.0, 6)
+        dt = 10 ** rng.uniform(-10, -7)
+        dq = rng.normal(0.0, 1e-12, 6)
+        V0, C0, G0, D0 = sc.V.copy(), sc.C.copy(), sc.G.copy(), sc.didv.copy()
+        sc.advance(dq, dt)
+        theirs = ref.circuit_advance(C0, G0, V0, dq / dt, D0, dt)
+        np.testing.assert_allclose(sc.V, theirs, rtol=1e-12, atol=1e-12 * np.abs(V0).max())
+
+
+def test_whipple_yield_matches_reference(ref):
+    """The oracle's (and the device's) Whipple secondary yield against the reference's
+    evaluateLegacySecondaryElectronYield, over incident energies from 0 to 20 keV and several
+    peak yields and peak energies (including a peak energy below the reference's 1 eV floor)."""
+    e = np.concatenate([[0.0, 1e-6, 0.5], np.geomspace(1e-3, 1.0, 40), np.linspace(1.0, 2e4, 400)])
+    for peak_yield in (0.0, 0.7, 2.0, 3.5):
+        for peak_e in (0.3, 50.0, 300.0, 800.0):
+            mine = O.see_yield(2, peak_yield, peak_e, e)
+            theirs = ref.whipple_yield(peak_yield, peak_e, e)
+            # q = 2.28 (E/Emax)^1.35; the numerator q - 1 + exp(-q) ~ q^2/2 cancels for small q,
+            # so an ulp of exp or pow grows by ~2/q^2 there: the bar is 1e-12 or that condition
+            # number times a few ulps, whichever is larger
+            q = 2.28 * (e / max(1.0, peak_e)) ** 1.35
+            bar = np.maximum(1e-12, 1e-15 / np.maximum(q * q / 2.0, 1e-300))
+            assert np.all(np.abs(mine - theirs) <= bar * np.abs(theirs)), (peak_yield, peak_e)
+            assert np.all(bar[e >= 0.1 * max(1.0, peak_e)] < 1e-12 * 1.5)  # the plain bar above 0.1 Emax
