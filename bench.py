@@ -46,7 +46,7 @@ QE, ME, MP = 1.602176634e-19, 9.1093837015e-31, 1.67262192369e-27
 
 CONFIGS = {
     "precision128": dict(n=128, L=1.6, body=(48, 80), bias=-10.0, ppc=64, dt=2e-8, precision=1, rtol=1e-10,
-                         density=1e10, te=1.0, ti=1.0, sort_interval=1, ion_sort_interval=16),
+                         density=1e10, te=1.0, ti=1.0, sort_interval=1, ion_sort_interval=16, precond="multigrid"),
     "plain32": dict(n=32, L=1.6, body=(12, 20), bias=-10.0, ppc=20, dt=2e-8, precision=0, rtol=1e-8, density=1e10,
                     te=1.0, ti=1.0, sort_interval=8),
     "batched64": dict(scenarios=64, seed=2026, precision=1, rtol=1e-10, sort_interval=4),
@@ -150,11 +150,18 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def build_domain(cfg, precision, capi, solve=True):
+def build_domain(cfg, precision, capi, solve=True, mesh_cache=None):
+    """A freshly seeded context of the workload (mesh arrays reused from mesh_cache)."""
     n = cfg["n"]
     h = cfg["L"] / n
     body = ((cfg["body"][0], cfg["body"][1]),) * 3 if cfg["body"] else None
-    m = capi.kuhn_box_mesh((n, n, n), h, body=body, bias=cfg["bias"], wall=0.0)
+    key = (n, cfg["L"], cfg["body"], cfg["bias"])
+    if mesh_cache is not None and key in mesh_cache:
+        m = mesh_cache[key]
+    else:
+        m = capi.kuhn_box_mesh((n, n, n), h, body=body, bias=cfg["bias"], wall=0.0)
+        if mesh_cache is not None:
+            mesh_cache[key] = m
     dom = capi.Domain(m["xyz"], m["tet"], m["dirichlet"], cfg["dt"], precision=precision, face_bc=(1,) * 6,
                       pcg_rtol=cfg["rtol"], pcg_max_iter=20000, sort_interval=cfg["sort_interval"])
 
@@ -170,6 +177,8 @@ def build_domain(cfg, precision, capi, solve=True):
         dom.set_species_sort_interval(1, cfg["ion_sort_interval"])
     for s in range(2):
         dom.set_elastic(s, 1e14, 1e-19, mode=1)
+    if cfg.get("precond") == "multigrid":
+        dom.set_preconditioner(capi.PRECOND_MULTIGRID)
     dom.set_potential(m["phi"])
     if solve:
         dom.solve_field(allow_not_converged=True)
@@ -187,7 +196,71 @@ def alg_bytes_push(dom, precision, particles):
     return particles * b_p + dom.T * t_b + dom.N * n_b
 
 
+# DRAM bytes per stored particle of one step's push launches (all passes, both species), from
+# an ncu capture of the push scaled per particle; None: not measured for the form.
+PUSH_DRAM_BYTES_PER_PARTICLE = {1: 339.2, 0: None}
+
+
+def cg_iteration_bytes(dom, precision):
+    """Algorithmic bytes of one (inner) CG iteration of the field solve.  Jacobi: R rows x (15
+    nonzeros x (value + column) + 7 vectors x 8 B).  Multigrid: the CG's own direction, mat-vec
+    and update (3 + 3 + 6 vectors, the matrix once) plus one V-cycle, each level's arrays
+    counted once per pass: a first sweep (3 vectors), three sweeps and a residual (matrix + 5
+    vectors each), the restriction and prolongation (their weights and columns, the vectors they
+    read and write), and on the coarsest level the dense inverse once."""
+    V = 4 if precision == 1 else 8
+    levels = dom.solver_levels()
+    R0, nnz0, _ = levels[0]
+    if len(levels) == 1:
+        return R0 * (15 * V + 4 * 15 + 7 * 8)
+
+    def csr_pass(R, nnz, vecs):
+        return 4 * (R + 1) + nnz * (4 + V) + vecs * V * R
+
+    b = 3 * V * R0 + csr_pass(R0, nnz0, 3) + 6 * V * R0
+    for l in range(len(levels) - 1):
+        R, nnz, t = levels[l]
+        Rc = levels[l + 1][0]
+        b += 3 * V * R + 4 * csr_pass(R, nnz, 5)
+        b += 8 * t + 4 * (Rc + 1) + V * (R + Rc)          # restriction
+        b += 8 * t + 4 * (R + 1) + V * (Rc + 2 * R)       # prolongation
+    Rc, nc, _ = levels[-1]
+    b += V * nc + 2 * V * Rc
+    return b
+
+
+def step_bytes(dom, precision, particles, pcg_iters):
+    """Algorithmic bytes of one step by the per-step formula: particle state read and written
+    (FP64 104 B, mixed 56 B), per-tet connectivity and geometry (112 B), per-node field, charge
+    limbs and potential (48 B), and the (inner) CG iterations of the field solve."""
+    b_p = 56 if precision == 1 else 104
+    per_iter = cg_iteration_bytes(dom, precision)
+    return particles * b_p + dom.T * 112 + dom.N * 48 + pcg_iters * per_iter, per_iter
+
+
+def _timed_steps(torch, stream, step, steps, counter):
+    """Times `steps` calls of step() with CUDA events on `stream`; counter() after each step
+    gives its active particles.  Returns (ms, particle-steps, active particles per step)."""
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    ps, act = 0, []
+    for _ in range(steps):
+        step()
+        a = counter()
+        ps += a
+        act.append(int(a))
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    return ev0.elapsed_time(ev1), ps, act
+
+
 def run_ours(args, cfg):
+    """Every form starts from its own freshly seeded context (the same seed, mesh and plasma),
+    runs W untimed steps and then the same K timed steps, so the forms are compared on the
+    same step indices and populations: the stepped context (the headline), the same workload as
+    a one-scenario CUDA-graph batch, the plain FP64 form, and the end-to-end loop through the C
+    ABI with host buffers."""
     import torch
 
     from scdat_b200 import build, capi
@@ -203,7 +276,9 @@ def run_ours(args, cfg):
 
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
     prec = cfg["precision"]
-    dom, mesh = build_domain(cfg, prec, capi)
+    mesh_cache = {}
+    # ---- the headline: stepped context (scdat_step per step) ----
+    dom, mesh = build_domain(cfg, prec, capi, mesh_cache=mesh_cache)
     stream = torch.cuda.ExternalStream(dom.stream())
     for _ in range(args.warmup):
         dom.step(1)
@@ -213,25 +288,18 @@ def run_ours(args, cfg):
     clocks = ClockSampler(local)
     clocks.start()
     dom.set_timing(True)
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    ev0.record(stream)
-    psteps = 0
     pcg_iters = []
-    for _ in range(args.steps):
-        dom.step(1)
+
+    def count_headline():
         st = dom.stats()
-        psteps += st["active_particles"]
         pcg_iters.append(st["last_pcg_iterations"])
-    ev1.record(stream)
-    torch.cuda.synchronize()
-    ms = ev0.elapsed_time(ev1)
+        return st["active_particles"]
+
+    ms, psteps, active = _timed_steps(torch, stream, lambda: dom.step(1), args.steps, count_headline)
     tm = dom.timing()
     clk = clocks.stop()
-    # the potential after warmup + steps steps, for the error against the FP64 form
     phi_at = (args.warmup + args.steps, dom.fields()[1].copy())
-    t_local = ms / 1e3
-    t_max, total_psteps = reduce_over_ranks(dist, t_local, psteps)
+    t_max, total_psteps = reduce_over_ranks(dist, ms / 1e3, psteps)
     value = total_psteps / t_max
     # roofline of the dominant kernel (the push), timed with events on the library stream
     push_ms = tm["push_ms"] / max(tm["push_launches"], 1)
@@ -240,26 +308,28 @@ def run_ours(args, cfg):
     peak, peak_kind = load_peaks()
     achieved = bytes_push / (push_ms / 1e3) / 1e9
     traffic = None
-    # DRAM bytes of one step's push launches from an ncu capture of this workload
-    # (profiles/push_dram_precision128.md, line "dram_bytes_per_particle_<form>: <value>"),
-    # scaled to this run's particles
-    tr_file = os.path.join(ROOT, "profiles", f"push_dram_{args.config}.md")
-    if os.path.exists(tr_file) and not args.n and not args.ppc:
-        import re
-
-        key = "mixed" if prec == 1 else "fp64"
-        m = re.search(rf"dram_bytes_per_particle_{key}:\s*([0-9.eE+]+)", open(tr_file).read())
-        if m:
-            traffic = float(m.group(1)) * parts_per_launch
-    # The same workload as a one-scenario batch: the whole step (three push launches, charge,
-    # the refinement and PCG loops, field) is one CUDA-graph launch with device-side loop
-    # control, bitwise the same results as the stepped context above.  Reported beside the
-    # headline, which is the stepped context (scdat_step, the drop-in entry point).
+    if PUSH_DRAM_BYTES_PER_PARTICLE.get(prec) is not None:
+        traffic = PUSH_DRAM_BYTES_PER_PARTICLE[prec] * parts_per_launch
+    # the per-step formula over the whole step, and the field stage alone
+    it_mean = float(np.mean(pcg_iters)) if pcg_iters else 0.0
+    b_step, b_iter = step_bytes(dom, prec, psteps / max(args.steps, 1), it_mean)
+    step_ms = t_max * 1e3 / args.steps
+    field_ms = tm["field_ms"] / args.steps
+    roof_step = {"alg_bytes": b_step, "achieved": b_step / (step_ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                 "frac": b_step / (step_ms / 1e3) / 1e9 / peak, "peak_kind": peak_kind,
+                 "formula": "P*b_p + T*112 + N*48 + I_pcg*(bytes of one CG iteration)", "cg_iteration_bytes": b_iter}
+    roof_field = {"alg_bytes": it_mean * b_iter, "achieved": it_mean * b_iter / (field_ms / 1e3) / 1e9,
+                  "peak": peak, "unit": "GB/s", "frac": it_mean * b_iter / (field_ms / 1e3) / 1e9 / peak,
+                  "peak_kind": peak_kind, "kernel": "field stage (inner CG iterations, refinement, LSQ)",
+                  "pcg_iterations_per_step_mean": it_mean, "levels": dom.solver_levels()}
+    stored = int(sum(dom.count(s) for s in range(dom.nspecies)))
+    dom.close()
+    # ---- the same workload as a one-scenario batch (one CUDA-graph launch per step) ----
     graph = None
-    runner = dom
-    if prec == 1:
-        batch = capi.Batch([dom])
-        for _ in range(2):
+    if prec == 1 and args.graph_form:
+        gdom, _ = build_domain(cfg, prec, capi, mesh_cache=mesh_cache)
+        batch = capi.Batch([gdom])
+        for _ in range(args.warmup):
             batch.step(1)
         gstream = torch.cuda.ExternalStream(batch.stream())
         torch.cuda.synchronize()
@@ -268,44 +338,74 @@ def run_ours(args, cfg):
         l0 = batch.kernel_launches()
         clocks = ClockSampler(local)
         clocks.start()
-        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        g0.record(gstream)
-        gps = 0
-        for _ in range(args.steps):
-            batch.step(1)
-            gps += dom.stats()["active_particles"]
-        g1.record(gstream)
-        torch.cuda.synchronize()
-        gms = g0.elapsed_time(g1)
+        gms, gps, gact = _timed_steps(torch, gstream, lambda: batch.step(1), args.steps,
+                                      lambda: gdom.stats()["active_particles"])
         gclk = clocks.stop()
-        g_local = gms / 1e3
-        g_max, g_total = reduce_over_ranks(dist, g_local, gps)
+        g_max, g_total = reduce_over_ranks(dist, gms / 1e3, gps)
         graph = {"value": g_total / g_max, "unit": "particle-steps/s", "ms_per_step": g_max * 1e3 / args.steps,
-                 "gpu_launches": int(batch.kernel_launches() - l0), "clocks": gclk,
-                 "form": "one CUDA-graph launch per step (one-scenario batch), steps after the stepped run"}
-    # end-to-end through the C ABI with host buffers: per step, Dirichlet potentials in from
-    # pinned host memory, then the ledger, statistics and the nodal potential back
+                 "gpu_launches": int(batch.kernel_launches() - l0), "clocks": gclk, "active_per_step": gact,
+                 "ratio_vs_stepped": (g_total / g_max) / value,
+                 "form": "one CUDA-graph launch per step (one-scenario batch, Jacobi-PCG), fresh seeded context, "
+                         "same steps"}
+        batch.close()
+        gdom.close()
+    # ---- the plain FP64 form (the 1x of the mixed form's speed-up) ----
+    fp64 = None
+    if prec == 1 and args.fp64_compare:
+        fdom, _ = build_domain(cfg, 0, capi, mesh_cache=mesh_cache)
+        fstream = torch.cuda.ExternalStream(fdom.stream())
+        for _ in range(args.warmup):
+            fdom.step(1)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        fdom.set_timing(True)
+        fms, fps, fact = _timed_steps(torch, fstream, lambda: fdom.step(1), args.steps,
+                                      lambda: fdom.stats()["active_particles"])
+        ftm = fdom.timing()
+        f_max, f_total = reduce_over_ranks(dist, fms / 1e3, fps)
+        p64 = fdom.fields()[1]
+        err = float(np.abs(phi_at[1] - p64).max() / max(np.abs(p64).max(), 1e-300))
+        fp64 = {"value": f_total / f_max, "unit": "particle-steps/s", "steps": args.steps,
+                "ms_per_step": f_max * 1e3 / args.steps, "active_per_step": fact,
+                "stage_ms_per_step": {"push": ftm["push_ms"] / args.steps, "field": ftm["field_ms"] / args.steps,
+                                      "resort": ftm["sort_ms"] / args.steps},
+                "ratio": value / (f_total / f_max),
+                "phi_rel_err_vs_fp64": {"value": err, "after_steps": phi_at[0],
+                                        "note": "both forms from the same seeded state over the same steps; "
+                                                "relative to max |phi|"}}
+        fdom.close()
+    # ---- end to end through the C ABI with host buffers: per step, Dirichlet potentials in
+    # from pinned host memory, then the ledger, statistics and the nodal potential back ----
+    edom, _ = build_domain(cfg, prec, capi, mesh_cache=mesh_cache)
     dir_nodes = np.nonzero(mesh["dirichlet"])[0].astype(np.int64)
     h_nodes = torch.from_numpy(dir_nodes).pin_memory()
     h_vals = torch.from_numpy(mesh["phi"][dir_nodes].copy()).pin_memory()
-    h_phi = torch.empty(dom.N, dtype=torch.float64).pin_memory()
-    e2e_steps = max(1, min(args.steps, 10))
+    h_phi = torch.empty(edom.N, dtype=torch.float64).pin_memory()
+    for _ in range(args.warmup):
+        edom.step(1)
     torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
     t0 = time.perf_counter()
     e2e_ps = 0
-    for _ in range(e2e_steps):
-        dom.L.scdat_set_node_potentials(dom.h, len(dir_nodes), h_nodes.data_ptr(), h_vals.data_ptr())
-        runner.step(1)
-        led = dom.ledger()
-        st = dom.stats()
-        dom.L.scdat_get_fields(dom.h, None, h_phi.data_ptr(), None)
+    parts_s = np.zeros(3)  # host seconds: potentials in, step, results back
+    for _ in range(args.steps):
+        ta = time.perf_counter()
+        edom.L.scdat_set_node_potentials(edom.h, len(dir_nodes), h_nodes.data_ptr(), h_vals.data_ptr())
+        tb = time.perf_counter()
+        edom.step(1)
+        tc = time.perf_counter()
+        edom.ledger()
+        st = edom.stats()
+        edom.L.scdat_get_fields(edom.h, None, h_phi.data_ptr(), None)
+        parts_s += (tb - ta, tc - tb, time.perf_counter() - tc)
         e2e_ps += st["active_particles"]
-    t1 = time.perf_counter()
-    e2e_val = e2e_ps / (t1 - t0)
+    e_max, e_total = reduce_over_ranks(dist, time.perf_counter() - t0, e2e_ps)
+    e2e_val = e_total / e_max
     h2d = len(dir_nodes) * 16
-    d2h = dom.N * 8 + 7 * 8 * 8 + 120
-    if prec == 1:
-        batch.close()
+    d2h = edom.N * 8 + 7 * 8 * 8 + 120
+    edom.close()
     out = {
         "metric": "PIC particle-steps/s on 1 B200 (mixed/batched vs plain FP64 at equal error)",
         "value": value,
@@ -313,7 +413,7 @@ def run_ours(args, cfg):
         "n_gpus": world,
         "steps": args.steps,
         "warmup": args.warmup,
-        "ms_per_step": t_max * 1e3 / args.steps,
+        "ms_per_step": step_ms,
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
@@ -321,26 +421,32 @@ def run_ours(args, cfg):
         "data": "synthetic (seeded Kuhn-box plasma, no dataset)",
         "step_form": "scdat_step per step (stepped context)",
         "config": {"workload": args.config, "cells": cfg["n"] ** 3, "tets": dom.T, "nodes": dom.N,
-                   "particles": int(sum(dom.count(s) for s in range(dom.nspecies))), "ppc_per_species": cfg["ppc"],
+                   "particles": stored, "ppc_per_species": cfg["ppc"],
                    "precision": "mixed" if prec == 1 else "fp64", "pcg_rtol": cfg["rtol"],
-                   "pcg_iterations_per_step": pcg_iters, "l2": "inputs larger than L2 (particle state > 126 MB)",
-                   "parallelism": f"replicas x{world}"},
+                   "preconditioner": cfg.get("precond", "jacobi"),
+                   "pcg_iterations_per_step": pcg_iters, "active_per_step": active,
+                   "l2": "inputs larger than L2 (particle state > 126 MB)", "parallelism": f"replicas x{world}"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_kind": peak_kind, "kernel": "push (gather+boris+relocate+deposit+mcc)",
                      "alg_bytes_per_launch": bytes_push, "launch_ms": push_ms},
-        "stage_ms_per_step": {"push": tm["push_ms"] / args.steps, "field": tm["field_ms"] / args.steps,
+        "roofline_step": roof_step,
+        "roofline_field": roof_field,
+        "stage_ms_per_step": {"push": tm["push_ms"] / args.steps, "field": field_ms,
                               "resort": tm["sort_ms"] / args.steps},
         "gpu_launches": int(tm["kernel_launches"]),
         "clocks": clk,
-        "e2e": {"value": e2e_val, "unit": "particle-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "e2e": {"value": e2e_val, "unit": "particle-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "host_ms_per_step": {"potentials_in": parts_s[0] * 1e3 / args.steps,
+                                     "step": parts_s[1] * 1e3 / args.steps,
+                                     "results_out": parts_s[2] * 1e3 / args.steps},
+                "form": "fresh seeded context, W untimed steps, the same K steps timed with the host clock"},
     }
     if graph is not None:
         out["graph_form"] = graph
-    dom.close()
+    if fp64 is not None:
+        out["fp64_form"] = fp64
     if rank == 0 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(cfg, args)
-    if rank == 0 and args.fp64_compare and prec == 1:
-        out["fp64_form"] = fp64_compare(cfg, args, phi_at)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -571,45 +677,6 @@ def run_surface(args, cfg):
         print(json.dumps(out))
 
 
-def fp64_compare(cfg, args, phi_at=None):
-    """The plain FP64 form on the same workload (the 1x of the mixed-form speed-up).  With
-    phi_at = (steps, phi) from the measured form, the FP64 run continues, untimed, to that
-    step count from the same seeded state and reports the measured form's potential error
-    against it (relative to max |phi|)."""
-    import torch
-
-    from scdat_b200 import capi
-
-    c = dict(cfg)
-    dom, _ = build_domain(c, 0, capi)
-    stream = torch.cuda.ExternalStream(dom.stream())
-    for _ in range(max(1, args.warmup)):
-        dom.step(1)
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    ev0.record(stream)
-    ps = 0
-    k = max(1, min(args.steps, 3))
-    for _ in range(k):
-        dom.step(1)
-        ps += dom.stats()["active_particles"]
-    ev1.record(stream)
-    torch.cuda.synchronize()
-    ms = ev0.elapsed_time(ev1)
-    out = {"value": ps / (ms / 1e3), "unit": "particle-steps/s", "steps": k, "ms_per_step": ms / k}
-    if phi_at is not None:
-        done = max(1, args.warmup) + k
-        if phi_at[0] >= done:
-            dom.step(phi_at[0] - done)
-            p64 = dom.fields()[1]
-            err = float(np.abs(phi_at[1] - p64).max() / max(np.abs(p64).max(), 1e-300))
-            out["phi_rel_err_vs_fp64"] = {"value": err, "after_steps": phi_at[0],
-                                          "note": "both forms from the same seeded state; particle "
-                                                  "trajectories of the two forms drift apart over the steps"}
-    dom.close()
-    return out
-
-
 def reference_sample(cfg):
     """The reference particle path on a bounded sample of the workload: a 16^3-cell box of the
     same cell size, plasma and particles per cell, a 4^3-cell body at the same bias."""
@@ -747,6 +814,9 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU baseline: seconds of reference push timed")
     ap.add_argument("--no-fp64-compare", dest="fp64_compare", action="store_false")
     ap.add_argument("--scenarios", type=int, default=0, help="batched64: number of scenarios (default 64)")
+    ap.add_argument("--precond", choices=["jacobi", "multigrid"], default=None,
+                    help="override the workload's field-solve preconditioner")
+    ap.add_argument("--no-graph-form", dest="graph_form", action="store_false")
     args = ap.parse_args()
     cfg = dict(CONFIGS[args.config])
     if args.config in ("batched64", "surface256"):
@@ -763,6 +833,8 @@ def main():
         cfg["n"] = args.n
     if args.ppc:
         cfg["ppc"] = args.ppc
+    if args.precond:
+        cfg["precond"] = args.precond
     if args.impl == "reference":
         run_reference(args, cfg)
     else:

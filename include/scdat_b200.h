@@ -35,6 +35,9 @@ typedef enum {
 
 typedef enum { SCDAT_PREC_FP64 = 0, SCDAT_PREC_MIXED = 1 } scdat_precision;
 
+/* Preconditioner of the field solve's CG (scdat_set_field_preconditioner). */
+typedef enum { SCDAT_PRECOND_JACOBI = 0, SCDAT_PRECOND_MULTIGRID = 1 } scdat_preconditioner;
+
 /* TrajectoryChargeDepositionKernel, Tools/Particle/include/PICParticleAlgorithms.h:32-37 */
 typedef enum { SCDAT_DEP_NEAREST = 0, SCDAT_DEP_LINEAR = 1, SCDAT_DEP_GAUSS3 = 2 } scdat_deposit_kernel;
 
@@ -262,6 +265,35 @@ SCDAT_API int scdat_compact(scdat_ctx* ctx);
  * many steps, so sorting it at the electrons' rate costs time and buys nothing.  interval must
  * be a positive multiple of params.sort_interval, or 0 to follow it. */
 SCDAT_API int scdat_set_species_sort_interval(scdat_ctx* ctx, int32_t species, int32_t interval);
+
+/* Pass-1 form of one species' push in the precision form (no reference counterpart; the
+ * reference pushes particle by particle).  WALKING: pass 1 gives every particle one sub-step
+ * with the full relocation walk.  STAY_FIRST: pass 1 carries no walk code and completes only
+ * sub-steps that end in the particle's own tet; the others go to the walking passes, which
+ * redo that sub-step with the same arithmetic, so both forms give bitwise the same result.
+ * STAY_FIRST is faster for a species that rarely leaves its tet (ions beside electrons of the
+ * same temperature).  AUTO (default) probes STAY_FIRST every 32 pushes and keeps it while it
+ * defers under a fifth of the species.  The plain FP64 form ignores the setting. */
+typedef enum { SCDAT_PUSH_AUTO = 0, SCDAT_PUSH_WALKING = 1, SCDAT_PUSH_STAY_FIRST = 2 } scdat_push_mode;
+SCDAT_API int scdat_set_species_push_mode(scdat_ctx* ctx, int32_t species, int32_t mode);
+
+/* Preconditioner of the field solve (the reference's CG is Jacobi-preconditioned,
+ * Tools/Solver/include/ConjugateGradientCommon.h:74-161, which stays the default).
+ * SCDAT_PRECOND_MULTIGRID builds, on the first call, a lattice multigrid hierarchy for meshes
+ * whose nodes lie on a regular lattice (e.g. scdat_kuhn_box_mesh): trilinear prolongation,
+ * Galerkin coarse operators P^T A P, damped-Jacobi smoothing (two sweeps before and after), a
+ * dense inverse on the coarsest level (at most 1024 rows), one V-cycle per CG iteration.  It
+ * preconditions the FP64 CG of the plain form and the FP32 inner CG of the precision form;
+ * the convergence test (||r|| <= rtol ||b||, in FP64 for the precision form) is unchanged, so
+ * only the iteration count differs.  Returns SCDAT_ERR_ARG (scdat_last_error says why) when
+ * the mesh has no such hierarchy.  The batched step keeps Jacobi-PCG. */
+SCDAT_API int scdat_set_field_preconditioner(scdat_ctx* ctx, int32_t kind);
+/* Sizes of the field solver's levels (for bandwidth accounting): *levels (1 for Jacobi), and
+ * for each of the first max_levels: rows, off-diagonal nonzeros of the operator (the dense
+ * coarsest level reports rows^2) and nonzeros of the prolongation to the next level (0 on the
+ * last).  Any output array may be NULL. */
+SCDAT_API int scdat_get_field_solver_levels(scdat_ctx* ctx, int32_t max_levels, int32_t* levels, int64_t* rows,
+                                            int64_t* nnz, int64_t* transfer_nnz);
 
 /* PICCycle::getChargeDensity/getPotential/getElectricField (PICCycle.h:79-90); any pointer
  * may be NULL.  rho is nodal charge [C]; E is [n_nodes*3]. */

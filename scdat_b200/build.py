@@ -24,10 +24,18 @@ HOST_DIR = os.path.join(HERE, "host")
 HOST_LIB = os.path.join(HERE, "libscdat_host.so")
 
 SOURCES = ["capi.cu", "push_f64.cu", "push_mixed.cu", "field.cu", "utils.cu", "pcg_csr.cu", "pcg_noalloc.cu",
-           "batch_field.cu", "batch_host.cu", "surface.cu", "adjoint.cu", "mesh_setup.cpp"]
+           "batch_field.cu", "batch_host.cu", "surface.cu", "adjoint.cu", "mg.cu", "mesh_setup.cpp",
+           "mg_setup.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
          "--expt-relaxed-constexpr", f"-I{os.path.join(ROOT, 'include')}"]
+
+
+# The precision form's push runs a particle's sub-steps in whichever of its pass kernels reaches
+# them (the pass split depends on the pass-1 form and the list capacities), and its results are
+# bitwise independent of that split only if every kernel evaluates the same IEEE operations:
+# so no multiply-add contraction in that file (explicit fmaf calls are kept).
+PER_FILE_FLAGS = {"push_mixed.cu": ["--fmad=false"]}
 
 
 def _headers_mtime() -> float:
@@ -42,7 +50,7 @@ def _compile(src: str, force: bool, verbose_ptxas: bool) -> str:
     if not force and os.path.exists(obj):
         if os.path.getmtime(obj) >= max(os.path.getmtime(srcp), _headers_mtime()):
             return obj
-    cmd = [NVCC, *ARCH, *FLAGS, "-c", srcp, "-o", obj]
+    cmd = [NVCC, *ARCH, *FLAGS, *PER_FILE_FLAGS.get(src, []), "-c", srcp, "-o", obj]
     if src.endswith(".cpp"):
         cmd = [NVCC, "-x", "c++", *FLAGS, "-c", srcp, "-o", obj]
     if verbose_ptxas and src.endswith(".cu"):

@@ -15,6 +15,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libscdat_b200.so")
 
 PREC_FP64, PREC_MIXED = 0, 1
+PRECOND_JACOBI, PRECOND_MULTIGRID = 0, 1
+PUSH_AUTO, PUSH_WALKING, PUSH_STAY_FIRST = 0, 1, 2
 DEP_NEAREST, DEP_LINEAR, DEP_GAUSS3 = 0, 1, 2
 BC_NONE, BC_ABSORB, BC_PERIODIC = 0, 1, 2
 ACTIVE, ABSORBED, ESCAPED = 0, 1, 2
@@ -85,7 +87,8 @@ EXPORTS = ["scdat_default_params", "scdat_create", "scdat_destroy", "scdat_last_
            "scdat_set_particles", "scdat_seed_box_particles", "scdat_kuhn_box_mesh", "scdat_get_particle_count",
            "scdat_get_particles", "scdat_set_potential", "scdat_set_node_potentials", "scdat_set_electric_field",
            "scdat_set_elastic_mcc", "scdat_step", "scdat_push", "scdat_solve_field", "scdat_collide", "scdat_compact",
-           "scdat_set_species_sort_interval",
+           "scdat_set_species_sort_interval", "scdat_set_field_preconditioner", "scdat_set_species_push_mode",
+           "scdat_get_field_solver_levels",
            "scdat_get_fields", "scdat_get_species_charge", "scdat_get_ledger", "scdat_reset_ledger",
            "scdat_get_statistics", "scdat_version", "scdat_stream", "scdat_set_timing", "scdat_get_timing",
            "scdat_get_sort_timing",
@@ -157,6 +160,9 @@ def load():
         getattr(L, f).argtypes = [vp]
     L.scdat_step.argtypes = [vp, C.c_int32]
     L.scdat_set_species_sort_interval.argtypes = [vp, C.c_int32, C.c_int32]
+    L.scdat_set_field_preconditioner.argtypes = [vp, C.c_int32]
+    L.scdat_set_species_push_mode.argtypes = [vp, C.c_int32, C.c_int32]
+    L.scdat_get_field_solver_levels.argtypes = [vp, C.c_int32, vp, vp, vp, vp]
     L.scdat_get_fields.argtypes = [vp, vp, vp, vp]
     L.scdat_get_species_charge.argtypes = [vp, C.c_int32, vp]
     L.scdat_get_ledger.argtypes = [vp, vp]
@@ -412,6 +418,26 @@ class Domain:
     def set_species_sort_interval(self, species, interval):
         """scdat_set_species_sort_interval: re-sort this species every `interval` steps."""
         self._ck(self.L.scdat_set_species_sort_interval(self.h, int(species), int(interval)))
+
+    def set_push_mode(self, species, mode):
+        """scdat_set_species_push_mode: PUSH_AUTO, PUSH_WALKING or PUSH_STAY_FIRST."""
+        self._ck(self.L.scdat_set_species_push_mode(self.h, int(species), int(mode)))
+
+    def solver_levels(self):
+        """scdat_get_field_solver_levels: [(rows, operator nonzeros, prolongation nonzeros)]."""
+        nl = C.c_int32()
+        self._ck(self.L.scdat_get_field_solver_levels(self.h, 0, C.byref(nl), None, None, None))
+        r, z, t = (np.zeros(nl.value, np.int64) for _ in range(3))
+        self._ck(self.L.scdat_get_field_solver_levels(self.h, nl.value, C.byref(nl), _p(r), _p(z), _p(t)))
+        return [(int(a), int(b), int(c)) for a, b, c in zip(r, z, t)]
+
+    def set_preconditioner(self, kind):
+        """scdat_set_field_preconditioner: PRECOND_JACOBI (default) or PRECOND_MULTIGRID."""
+        self._ck(self.L.scdat_set_field_preconditioner(self.h, int(kind)))
+
+    def rows(self):
+        """Interior (non-Dirichlet) nodes: the rows of the reduced Poisson system."""
+        return int(np.count_nonzero(self.dirichlet == 0))
 
     def step(self, n=1):
         self._ck(self.L.scdat_step(self.h, n))

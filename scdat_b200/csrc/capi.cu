@@ -7,6 +7,7 @@
 // which is the order of PICCycle::executeTimeStep (PICCycle.cpp:311-416) followed by the
 // background MCC step of the reference driver (Main/main_PICcore.cpp:487-515).
 #include "ctx.cuh"
+#include "mg_setup.h"
 
 #include <cub/device/device_radix_sort.cuh>
 
@@ -26,7 +27,7 @@ void launch_mcc_f64(const ParticleStore& P, const SpeciesDev& S, const PushParam
                     cudaStream_t st);
 void launch_push_mixed(const MeshView& M, const ParticleStore& P, const SpeciesDev& S, const PushParams& pp,
                        const DeferList& D1, const DeferList& D2, ChargeAcc A, LedgerDev* L,
-                       unsigned long long* ke_acc, unsigned* ctr, int grid, cudaStream_t st);
+                       unsigned long long* ke_acc, unsigned* ctr, int grid, bool stay_first, cudaStream_t st);
 void launch_mcc_mixed(const ParticleStore& P, const SpeciesDev& S, const PushParams& pp, LedgerDev* L, int grid,
                       cudaStream_t st);
 void launch_refresh_erec(int64_t T, const int4* tet, const double* E, double* erec, cudaStream_t st);
@@ -169,10 +170,42 @@ int check_flags(scdat_ctx* ctx)
         ctx->err = "device flag: invalid tet index seen";
         return SCDAT_ERR_DEVICE_FLAG;
     }
+    if (f & kFlagDeferOverflow) {
+        ctx->err = "device flag: deferred-particle list overflow";
+        return SCDAT_ERR_DEVICE_FLAG;
+    }
     return SCDAT_OK;
 }
 
 // ---- the stages ----------------------------------------------------------------------
+// Pass-1 form of species s for this push (mixed form).  A stay-first pass 1 pays off for a
+// species of which few particles leave their tet or need more than one sub-step in a step
+// (ions beside electrons of the same temperature); for the others its deferrals cost more than
+// the walk code it drops.  Automatic choice: a stay-first probe on the first push and every
+// kStayProbe-th, then stay-first while the last probe deferred under kStayMaxFrac of the
+// species.  Both forms give bitwise the same result.
+constexpr int kStayProbe = 32;
+constexpr double kStayMaxFrac = 0.2;
+
+bool stay_first_now(scdat_ctx* ctx, int s)
+{
+    SpeciesState& S = ctx->species[s];
+    if (S.stay_pending) {  // the last stay-first push's deferral count has arrived
+        S.stay_frac = S.stay_n > 0 ? (double)ctx->h_deferred[s] / (double)S.stay_n : 1.0;
+        S.stay_pending = false;
+    }
+    bool stay;
+    if (S.push_mode == SCDAT_PUSH_WALKING)
+        stay = false;
+    else if (S.push_mode == SCDAT_PUSH_STAY_FIRST)
+        stay = true;
+    else
+        stay = S.stay_frac < 0.0 || S.pushes % kStayProbe == 0 || S.stay_frac < kStayMaxFrac;
+    ++S.pushes;
+    if (stay) S.stay_n = S.n;
+    return stay;
+}
+
 int do_push(scdat_ctx* ctx, bool do_mcc)
 {
     const int S = (int)ctx->species.size();
@@ -200,14 +233,22 @@ int do_push(scdat_ctx* ctx, bool do_mcc)
         SpeciesDev sd = species_dev(ctx, s);
         // defer-list counts [0, 1] and the three passes' work counters [2, 5)
         CK(cudaMemsetAsync(ctx->dcount.p, 0, 5 * sizeof(unsigned), ctx->st));
-        DeferList d1{ctx->dcount.p, ctx->dcap, ctx->d1idx.p, ctx->d1it.p, ctx->d1rem.p, ctx->d1vs.p};
+        DeferList d1{ctx->dcount.p, ctx->d1cap, ctx->d1idx.p, ctx->d1it.p, ctx->d1rem.p, ctx->d1vs.p};
         DeferList d2{ctx->dcount.p + 1, ctx->dcap, ctx->d2idx.p, ctx->d2it.p, ctx->d2rem.p, ctx->d2vs.p};
         ctx->launches += 3;
         ChargeAcc acc{ctx->acc_l0.p + s * N, ctx->acc_l1.p + s * N, ctx->acc_h.p + s * N};
-        if (ctx->mixed)
+        if (ctx->mixed) {
+            const bool stay = stay_first_now(ctx, s);
             launch_push_mixed(ctx->mv, P, sd, pp, d1, d2, acc, ctx->led.p, ctx->ke_acc.p, ctx->dcount.p + 2,
-                              ctx->grid_push, ctx->st);
-        else
+                              ctx->grid_push, stay, ctx->st);
+            if (stay) {
+                // pass 1's deferred count, read by the next push's choice (the field solve in
+                // between synchronises the stream)
+                CK(cudaMemcpyAsync(ctx->h_deferred + s, ctx->dcount.p, sizeof(unsigned), cudaMemcpyDeviceToHost,
+                                   ctx->st));
+                ctx->species[s].stay_pending = true;
+            }
+        } else
             launch_push_f64(ctx->mv, P, sd, pp, d1, d2, acc, ctx->led.p, ctx->ke_acc.p, ctx->dcount.p + 2,
                             ctx->grid_push, ctx->st);
     }
@@ -264,10 +305,45 @@ int read_scalars(scdat_ctx* ctx, PcgScalars& h)
     return SCDAT_OK;
 }
 
+// Multigrid-preconditioned CG on the Dirichlet-reduced system in V's precision, from x: b, x and
+// the CG vectors r, z, p, q are R-vectors of the caller.  Blocks until the solve ends.
+template <typename V>
+int run_mgpcg(scdat_ctx* ctx, const V* b, V* x, V* r, V* z, V* p, V* q, double rtol, int max_iter, PcgScalars& h)
+{
+    const PoissonView& A = ctx->pv;
+    int rc = pcg_scalars_init(ctx, rtol, max_iter, 0.0);
+    if (rc) return rc;
+    launch_mgpcg_init<V>(A, b, x, r, ctx->sc.p, ctx->part.p, ctx->grid_red, ctx->st);
+    launch_vcycle<V>(ctx->mg_plan, r, z, ctx->sc.p, ctx->part.p, ctx->st);
+    const int per_cycle = 7 * ((int)ctx->mg_plan.lv.size() - 1) + 1;
+    ctx->launches += 1 + per_cycle;
+    const int batch = 2;  // iterations queued between convergence reads (kernels after convergence return at once)
+    for (int k = 0; k < max_iter; k += batch) {
+        for (int j = 0; j < batch; ++j) {
+            ctx->launches += 3 + per_cycle;
+            launch_mgpcg_iter<V>(A, ctx->mg_plan, x, r, z, p, q, ctx->sc.p, ctx->part.p, ctx->grid_red, ctx->st);
+        }
+        CK(cudaGetLastError());
+        rc = read_scalars(ctx, h);
+        if (rc) return rc;
+        if (h.done) break;
+    }
+    if (max_iter <= 0) return read_scalars(ctx, h);
+    return SCDAT_OK;
+}
+
 int run_pcg64(scdat_ctx* ctx, const double* bvec, double* xvec, double rtol, int max_iter, int& iters,
               double& relres)
 {
     const PoissonView& A = ctx->pv;
+    if (ctx->precond == SCDAT_PRECOND_MULTIGRID) {
+        PcgScalars h{};
+        int rc = run_mgpcg<double>(ctx, bvec, xvec, ctx->r.p, ctx->z.p, ctx->p.p, ctx->q.p, rtol, max_iter, h);
+        if (rc) return rc;
+        iters = h.iter;
+        relres = std::sqrt(h.rr / (h.bb > 0.0 ? h.bb : 1.0));
+        return SCDAT_OK;
+    }
     int rc = pcg_scalars_init(ctx, rtol, max_iter, 0.0);
     if (rc) return rc;
     ++ctx->launches;
@@ -317,8 +393,20 @@ int run_pcg_mixed(scdat_ctx* ctx, double rtol, int max_iter, int& iters, double&
         relres = std::sqrt(h.rr / bb);
         if (h.rr <= rtol * rtol * bb || iters >= max_iter || outer == kMaxRefinePasses) break;
         // inner FP32 solve A e = r from e = 0, to the tolerance this pass needs
-        ctx->launches += 2;
+        ctx->launches += 1;
         launch_zero_f32(R, ctx->xf.p, ctx->grid_red, ctx->st);
+        if (ctx->precond == SCDAT_PRECOND_MULTIGRID) {
+            PcgScalars hi{};
+            rc = run_mgpcg<float>(ctx, ctx->rf.p, ctx->xf.p, ctx->qf.p, ctx->zf.p, ctx->pf.p, ctx->pnf.p,
+                                  inner_rtol(h.rr, bb, rtol), std::max(1, max_iter - iters), hi);
+            if (rc) return rc;
+            iters += hi.iter;
+            ++ctx->launches;
+            launch_add_correction(R, ctx->x.p, ctx->xf.p, ctx->grid_red, ctx->st);
+            CK(cudaGetLastError());
+            continue;
+        }
+        ctx->launches += 1;
         rc = pcg_scalars_init(ctx, inner_rtol(h.rr, bb, rtol), std::max(1, max_iter - iters), 0.0);
         if (rc) return rc;
         launch_pcg_init32(A, ctx->rf.p, ctx->xf.p, ctx->qf.p, ctx->zf.p, ctx->sc.p, ctx->part.p, ctx->grid_red,
@@ -348,6 +436,107 @@ int run_pcg_mixed(scdat_ctx* ctx, double rtol, int max_iter, int& iters, double&
         launch_add_correction(R, ctx->x.p, ctx->xf.p, ctx->grid_red, ctx->st);
         CK(cudaGetLastError());
     }
+    return SCDAT_OK;
+}
+
+// Builds the lattice multigrid hierarchy of the context's mesh on the host and uploads it.
+int setup_multigrid(scdat_ctx* ctx)
+{
+    HostMg hmg;
+    std::string why = build_multigrid(ctx->hm, ctx->hps, hmg);
+    if (!why.empty()) {
+        ctx->err = "multigrid preconditioner unavailable: " + why;
+        return SCDAT_ERR_ARG;
+    }
+    cudaStream_t st = ctx->st;
+    const size_t vb = ctx->mixed ? sizeof(float) : sizeof(double);
+    ctx->mgl.clear();
+    MgPlan plan;
+    plan.grid_max = ctx->grid_red;
+    const int L = (int)hmg.lv.size();
+    for (int l = 0; l < L; ++l) {
+        const HostMgLevel& H = hmg.lv[l];
+        auto D = std::make_unique<MgDevLevel>();
+        MgLevelDev v{};
+        v.R = H.R;
+        v.omega = (float)H.omega;
+        if (l == 0) {
+            v.row_ptr = ctx->pv.row_ptr;
+            v.col = ctx->pv.col;
+            v.val = ctx->pv.val;
+            v.valf = ctx->pv.valf;
+            v.diag = ctx->pv.diag;
+            v.diagf = ctx->pv.diagf;
+            v.dinv = ctx->pv.dinv;
+            v.dinvf = ctx->pv.dinvf;
+        } else {
+            std::vector<float> valf(H.val.begin(), H.val.end()), diagf(H.diag.begin(), H.diag.end());
+            std::vector<double> dinv(H.R);
+            std::vector<float> dinvf(H.R);
+            for (int r = 0; r < H.R; ++r) {
+                dinv[r] = 1.0 / H.diag[r];
+                dinvf[r] = (float)dinv[r];
+            }
+            if (valf.empty()) valf.push_back(0.0f);
+            std::vector<double> val = H.val;
+            std::vector<int32_t> col = H.col;
+            if (val.empty()) {
+                val.push_back(0.0);
+                col.push_back(0);
+            }
+            CK(D->row_ptr.upload(H.row_ptr.data(), H.row_ptr.size(), st));
+            CK(D->col.upload(col.data(), col.size(), st));
+            CK(D->val.upload(val.data(), val.size(), st));
+            CK(D->valf.upload(valf.data(), valf.size(), st));
+            CK(D->diag.upload(H.diag.data(), H.diag.size(), st));
+            CK(D->diagf.upload(diagf.data(), diagf.size(), st));
+            CK(D->dinv.upload(dinv.data(), dinv.size(), st));
+            CK(D->dinvf.upload(dinvf.data(), dinvf.size(), st));
+            CK(cudaStreamSynchronize(st));  // the host vectors above go out of scope
+            v.row_ptr = D->row_ptr.p;
+            v.col = D->col.p;
+            v.val = D->val.p;
+            v.valf = D->valf.p;
+            v.diag = D->diag.p;
+            v.diagf = D->diagf.p;
+            v.dinv = D->dinv.p;
+            v.dinvf = D->dinvf.p;
+        }
+        if (l + 1 < L) {
+            CK(D->p_ptr.upload(H.p_ptr.data(), H.p_ptr.size(), st));
+            CK(D->p_col.upload(H.p_col.data(), H.p_col.size(), st));
+            CK(D->p_w.upload(H.p_w.data(), H.p_w.size(), st));
+            CK(D->r_ptr.upload(H.r_ptr.data(), H.r_ptr.size(), st));
+            CK(D->r_col.upload(H.r_col.data(), H.r_col.size(), st));
+            CK(D->r_w.upload(H.r_w.data(), H.r_w.size(), st));
+            v.p_ptr = D->p_ptr.p;
+            v.p_col = D->p_col.p;
+            v.p_w = D->p_w.p;
+            v.r_ptr = D->r_ptr.p;
+            v.r_col = D->r_col.p;
+            v.r_w = D->r_w.p;
+        }
+        // work vectors, each padded to 256 bytes
+        const size_t vbytes = ((size_t)std::max(H.R, 1) * vb + 255) & ~(size_t)255;
+        CK(D->work.alloc(5 * vbytes));
+        MgWork w{};
+        unsigned char* base = D->work.p;
+        w.b = base;
+        w.xa = base + vbytes;
+        w.xb = base + 2 * vbytes;
+        w.res = base + 3 * vbytes;
+        w.xo = base + 4 * vbytes;
+        plan.lv.push_back(v);
+        plan.w.push_back(w);
+        ctx->mgl.push_back(std::move(D));
+    }
+    std::vector<float> cf(hmg.coarse_inv.begin(), hmg.coarse_inv.end());
+    CK(ctx->mg_cinv.upload(hmg.coarse_inv.data(), hmg.coarse_inv.size(), st));
+    CK(ctx->mg_cinvf.upload(cf.data(), cf.size(), st));
+    CK(cudaStreamSynchronize(st));
+    plan.cinv = ctx->mg_cinv.p;
+    plan.cinvf = ctx->mg_cinvf.p;
+    ctx->mg_plan = plan;
     return SCDAT_OK;
 }
 
@@ -743,6 +932,8 @@ SCDAT_API int scdat_set_species(scdat_ctx* ctx, int32_t n_species, const scdat_s
     CK(ctx->acc_l1.alloc((size_t)(n_species * N)));
     CK(ctx->acc_h.alloc((size_t)(n_species * N)));
     CK(ctx->counts.alloc((size_t)n_species));
+    CK(cudaMallocHost((void**)&ctx->h_deferred, sizeof(unsigned) * n_species));
+    std::memset(ctx->h_deferred, 0, sizeof(unsigned) * n_species);
     CK(cudaMemsetAsync(ctx->counts.p, 0, sizeof(int64_t) * n_species, ctx->st));
     CK(cudaMemsetAsync(ctx->acc_l0.p, 0, sizeof(unsigned long long) * n_species * N, ctx->st));
     CK(cudaMemsetAsync(ctx->acc_l1.p, 0, sizeof(unsigned long long) * n_species * N, ctx->st));
@@ -767,18 +958,23 @@ static int alloc_species(scdat_ctx* ctx, int s, int64_t n)
     S.cap = cap;
     S.n = n;
     CK(cudaMemcpyAsync(ctx->counts.p + s, &S.n, sizeof(int64_t), cudaMemcpyHostToDevice, ctx->st));
-    // deferred lists of the multi-pass push: a quarter of the largest species (a full list
-    // only means the overflow finishes in the earlier pass)
+    // deferred lists of the multi-pass push: pass 1's list covers the largest species (a
+    // stay-first pass 1 may defer every particle), pass 2's a quarter of it (a full list only
+    // means the overflow finishes in pass 2)
+    unsigned want1 = (unsigned)std::min<int64_t>(cap + 4096, 0x7fffffff);
     unsigned want = (unsigned)std::min<int64_t>(cap / 4 + 4096, 0x7fffffff);
+    if (!ctx->dcount.p) CK(ctx->dcount.alloc(5));
+    if (want1 > ctx->d1cap) {
+        CK(ctx->d1idx.alloc(want1));
+        CK(ctx->d1it.alloc(want1));
+        CK(ctx->d1rem.alloc(want1));
+        CK(ctx->d1vs.alloc(want1));
+        ctx->d1cap = want1;
+    }
     if (want > ctx->dcap) {
-        CK(ctx->dcount.alloc(5));
-        CK(ctx->d1idx.alloc(want));
         CK(ctx->d2idx.alloc(want));
-        CK(ctx->d1it.alloc(want));
         CK(ctx->d2it.alloc(want));
-        CK(ctx->d1rem.alloc(want));
         CK(ctx->d2rem.alloc(want));
-        CK(ctx->d1vs.alloc(want));
         CK(ctx->d2vs.alloc(want));
         ctx->dcap = want;
     }
@@ -1118,11 +1314,12 @@ SCDAT_API int scdat_set_node_potentials(scdat_ctx* ctx, int64_t n, const int64_t
     ARG(n >= 0 && (n == 0 || (nodes && values)), "bad node arrays");
     if (n == 0) return SCDAT_OK;
     for (int64_t i = 0; i < n; ++i) ARG(nodes[i] >= 0 && nodes[i] < ctx->hm.N, "node index out of range");
-    DBuf<int64_t> di;
-    DBuf<double> dv;
-    CK(di.upload(nodes, (size_t)n, ctx->st));
-    CK(dv.upload(values, (size_t)n, ctx->st));
-    launch_scatter_values(n, di.p, dv.p, ctx->phi.p, ctx->st);
+    // staging buffers kept by the context (grown on demand), so a per-step call allocates nothing
+    if (ctx->stage_nodes.n < (size_t)n) CK(ctx->stage_nodes.alloc((size_t)n));
+    if (ctx->stage_vals.n < (size_t)n) CK(ctx->stage_vals.alloc((size_t)n));
+    CK(cudaMemcpyAsync(ctx->stage_nodes.p, nodes, sizeof(int64_t) * n, cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(ctx->stage_vals.p, values, sizeof(double) * n, cudaMemcpyHostToDevice, ctx->st));
+    launch_scatter_values(n, ctx->stage_nodes.p, ctx->stage_vals.p, ctx->phi.p, ctx->st);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(ctx->st));
     return SCDAT_OK;
@@ -1314,6 +1511,51 @@ SCDAT_API int scdat_set_species_sort_interval(scdat_ctx* ctx, int32_t species, i
     ARG(interval == 0 || (interval > 0 && si > 0 && interval % si == 0),
         "species sort interval must be 0 or a positive multiple of params.sort_interval");
     ctx->species[species].sort_interval = interval;
+    return SCDAT_OK;
+}
+
+SCDAT_API int scdat_set_species_push_mode(scdat_ctx* ctx, int32_t species, int32_t mode)
+{
+    if (!ctx) return SCDAT_ERR_ARG;
+    ARG(species >= 0 && species < (int)ctx->species.size(), "species out of range");
+    ARG(mode == SCDAT_PUSH_AUTO || mode == SCDAT_PUSH_WALKING || mode == SCDAT_PUSH_STAY_FIRST, "unknown push mode");
+    ctx->species[species].push_mode = mode;
+    return SCDAT_OK;
+}
+
+SCDAT_API int scdat_get_field_solver_levels(scdat_ctx* ctx, int32_t max_levels, int32_t* levels, int64_t* rows,
+                                            int64_t* nnz, int64_t* transfer_nnz)
+{
+    if (!ctx || !levels) return SCDAT_ERR_ARG;
+    ARG(max_levels >= 0, "negative level capacity");
+    const bool mg = ctx->precond == SCDAT_PRECOND_MULTIGRID;
+    const int L = mg ? (int)ctx->mg_plan.lv.size() : 1;
+    *levels = L;
+    for (int l = 0; l < std::min(L, (int)max_levels); ++l) {
+        const int64_t r = mg ? ctx->mg_plan.lv[l].R : ctx->pv.R;
+        int64_t z = 0, t = 0;
+        if (l == 0)
+            z = (int64_t)ctx->hps.col.size();
+        else
+            z = (int64_t)ctx->mgl[l]->col.n;
+        if (mg && l + 1 < L) t = (int64_t)ctx->mgl[l]->p_col.n;
+        if (mg && l + 1 == L) z = r * r;  // the coarsest level is solved by a dense inverse
+        if (rows) rows[l] = r;
+        if (nnz) nnz[l] = z;
+        if (transfer_nnz) transfer_nnz[l] = t;
+    }
+    return SCDAT_OK;
+}
+
+SCDAT_API int scdat_set_field_preconditioner(scdat_ctx* ctx, int32_t kind)
+{
+    if (!ctx) return SCDAT_ERR_ARG;
+    ARG(kind == SCDAT_PRECOND_JACOBI || kind == SCDAT_PRECOND_MULTIGRID, "unknown preconditioner");
+    if (kind == SCDAT_PRECOND_MULTIGRID && ctx->mgl.empty()) {
+        int rc = setup_multigrid(ctx);
+        if (rc) return rc;
+    }
+    ctx->precond = kind;
     return SCDAT_OK;
 }
 

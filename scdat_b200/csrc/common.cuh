@@ -180,6 +180,7 @@ struct LedgerDev {
 enum DeviceFlag : unsigned long long {
     kFlagBadTet = 1ull << 0,
     kFlagPcgNotConverged = 1ull << 1,
+    kFlagDeferOverflow = 1ull << 2,  // a stay-first pass 1 found its deferred list full
 };
 
 struct SpeciesDev {

@@ -6,9 +6,11 @@
 #include "common.cuh"
 #include "field.cuh"
 #include "mesh_setup.h"
+#include "mg.cuh"
 #include "push.cuh"
 #include "surface.cuh"
 
+#include <memory>
 #include <string>
 #include <utility>
 #include <vector>
@@ -61,6 +63,14 @@ struct SpeciesState {
     int64_t cap = 0;
     int64_t n = 0;  // host view of the stored count (updated on set/compact)
     int sort_interval = 0;  // 0: the context's params.sort_interval
+    // pass-1 form of the mixed push (scdat_set_species_push_mode) and the automatic choice's
+    // state: pushes so far, the deferred fraction of the last stay-first push (-1: none yet),
+    // the particle count of that push, and whether its count is still to be read
+    int push_mode = 0;
+    int64_t pushes = 0;
+    double stay_frac = -1.0;
+    int64_t stay_n = 0;
+    bool stay_pending = false;
     DBuf<double> x, y, z, vx, vy, vz;
     DBuf<float4> mix;  // mixed form: two float4 per particle (see ParticleStore)
     DBuf<int32_t> tet;
@@ -84,6 +94,15 @@ struct StageEvents {
         list.emplace_back(e0, e1);
         e0 = e1 = nullptr;
     }
+};
+
+// One multigrid level on the device (level 0 shares the context's Poisson arrays and only
+// holds its transfers and work vectors).
+struct MgDevLevel {
+    DBuf<int32_t> row_ptr, col, p_ptr, p_col, r_ptr, r_col;
+    DBuf<double> val, diag, dinv;
+    DBuf<float> valf, diagf, dinvf, p_w, r_w;
+    DBuf<unsigned char> work;  // b, xa, xb, res, xo in the context's precision
 };
 
 struct scdat_ctx {
@@ -110,6 +129,13 @@ struct scdat_ctx {
     DBuf<float> xf, rf, zf, pf, pnf, qf;
     DBuf<PcgScalars> sc;
     DBuf<double> part;
+    // lattice multigrid preconditioner (scdat_set_field_preconditioner): per-level operators,
+    // transfers and work vectors, the coarsest dense inverse, and the launch plan over them
+    int precond = 0;
+    std::vector<std::unique_ptr<MgDevLevel>> mgl;
+    DBuf<double> mg_cinv;
+    DBuf<float> mg_cinvf;
+    MgPlan mg_plan;
     // fields
     DBuf<double> rho, phi, E, tmp_rho;
     DBuf<float> Ef;
@@ -128,12 +154,15 @@ struct scdat_ctx {
     DBuf<uint32_t> scratchu;
     DBuf<int64_t> nact;
     DBuf<int64_t> idx64;
+    DBuf<int64_t> stage_nodes;  // scdat_set_node_potentials staging
+    DBuf<double> stage_vals;
     // deferred-particle lists of the multi-pass push
     DBuf<unsigned> dcount;
     DBuf<uint32_t> d1idx, d2idx;
     DBuf<int> d1it, d2it;
     DBuf<double> d1rem, d2rem, d1vs, d2vs;
-    unsigned dcap = 0;
+    unsigned dcap = 0, d1cap = 0;
+    unsigned* h_deferred = nullptr;  // pinned: pass-1 deferred count of each species' last stay-first push
     // surface circuit of the body faces (scdat_set_surface_circuit)
     bool surface = false;
     int see_model = 0;
@@ -172,6 +201,7 @@ struct scdat_ctx {
     ~scdat_ctx()
     {
         if (st) cudaStreamSynchronize(st);
+        if (h_deferred) cudaFreeHost(h_deferred);
         for (auto* evs : {&ev_push, &ev_field, &ev_sort})
             for (auto& pr : *evs) {
                 cudaEventDestroy(pr.first);

@@ -393,6 +393,106 @@ __device__ __forceinline__ void push1_warp(const MeshView& M, const ParticleStor
     warp_chunk_end(c);
 }
 
+// Pass 1's one sub-step for a species that rarely leaves its tet, with no walk code: the
+// sub-step is computed exactly as advance_f computes it and committed (deposit, position,
+// velocity, time) only when the particle ends inside its tet.  A particle that would leave
+// its tet, or whose start point is outside it, keeps its state untouched and goes to the
+// walking passes, which then run the same sub-step with the same arithmetic; so the result is
+// bitwise the walking pass 1's.  kDone: step finished; kCapped: continue in pass 2.
+__device__ __forceinline__ int advance_stay_f(const MeshView& M, const SpeciesDev& S, const PushParams& pp,
+                                              FlightF& f, ChargeAcc A, unsigned& nsub)
+{
+    if (!(f.rem > 1e-20f && f.it < kMaxSubsteps)) return f.it >= kMaxSubsteps ? kLost : kDone;
+    const float qm = (float)S.qm;
+    const float4* rec = reinterpret_cast<const float4*>(M.trec + 64 * (int64_t)f.cur);
+    float l[4];
+    {
+        float J[9];
+        load_j(M, f.cur, J);
+        baryj(J, f.rx, f.ry, f.rz, l);
+    }
+    if (!inside_f(l)) return kCapped;
+    const float4 c = __ldg(rec + 2), d = __ldg(rec + 3), e = __ldg(rec + 4), g = __ldg(rec + 5);
+    const float Ex = fmaf(l[1], d.x, fmaf(l[2], d.w, fmaf(l[3], e.z, c.y)));
+    const float Ey = fmaf(l[1], d.y, fmaf(l[2], e.x, fmaf(l[3], e.w, c.z)));
+    const float Ez = fmaf(l[1], d.z, fmaf(l[2], e.y, fmaf(l[3], g.x, c.w)));
+    float adt = f.rem;
+    const float Em = sqrtf(Ex * Ex + Ey * Ey + Ez * Ez);
+    if (Em > 1e-10f) {
+        const float acc = Em * fabsf(qm);
+        if (acc > 1e-10f && f.vstart > 1.0f) adt = fminf(adt, 0.1f * f.vstart / acc);
+    }
+    adt = fmaxf(adt, f.rem * (float)pp.floor_ratio);
+    adt = fminf(adt, f.rem);
+    float vx = f.vx, vy = f.vy, vz = f.vz;
+    if (fabsf(qm) > 1e-20f) {
+        const float h = 2.0f * (qm * (0.5f * adt));
+        vx = fmaf(h, Ex, vx);
+        vy = fmaf(h, Ey, vy);
+        vz = fmaf(h, Ez, vz);
+    }
+    const float rx = fmaf(vx, adt, f.rx), ry = fmaf(vy, adt, f.ry), rz = fmaf(vz, adt, f.rz);
+    float le[4];
+    {
+        float J[9];
+        load_j(M, f.cur, J);
+        baryj(J, rx, ry, rz, le);
+    }
+    if (!inside_f(le)) return kCapped;
+    ++f.it;
+    if (pp.deposit) {
+        const double qw = S.q * S.w;
+        const float tx = rx - f.rx, ty = ry - f.ry, tz = rz - f.rz;
+        const bool tiny = sqrtf(tx * tx + ty * ty + tz * tz) < 1e-15f;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const float lk = tiny ? l[q] : (pp.dep_kernel == 0 ? le[q] : 0.5f * (l[q] + le[q]));
+            const int nd = __float_as_int(__ldg(reinterpret_cast<const float*>(rec) + 21 + q));
+            fx_red(A, nd, fx_from_double((qw * (double)lk) * pp.inv_uq));
+        }
+    }
+    f.rx = rx; f.ry = ry; f.rz = rz;
+    f.vx = vx; f.vy = vy; f.vz = vz;
+    f.rem -= adt;
+    ++nsub;
+    return (f.rem > 1e-20f && f.it < kMaxSubsteps) ? kCapped : (f.it >= kMaxSubsteps ? kLost : kDone);
+}
+
+// Stay-first pass 1 for the 32 particles [base, base + 32): one sub-step for those that stay in
+// their tet; everything else (leaving the tet, more time left, no location hint) goes to D,
+// whose capacity covers the whole species, so nothing overflows.
+__device__ __forceinline__ void push1_stay_warp(const MeshView& M, const ParticleStore& P, const SpeciesDev& S,
+                                                const PushParams& pp, const DeferList& D, ChargeAcc A, LedgerDev* L,
+                                                int64_t base, int64_t n, PushStats& c)
+{
+    const int64_t i = base + (threadIdx.x & 31);
+    int st = -1;
+    FlightF f;
+    if (i < n) {
+        f.cur = P.tet[i];
+        mix_load(P, i, f.rx, f.ry, f.rz, f.vx, f.vy, f.vz);
+        if (f.cur <= kTetAbsorbed) {
+            double ux = f.vx, uy = f.vy, uz = f.vz;
+            c.ke += 0.5 * S.m * (ux * ux + uy * uy + uz * uz);
+        } else {
+            f.vstart = sqrtf(f.vx * f.vx + f.vy * f.vy + f.vz * f.vz);
+            f.rem = (float)pp.dt;
+            f.it = 0;
+            st = f.cur < 0 ? kCapped : advance_stay_f(M, S, pp, f, A, c.nsub);
+        }
+    }
+    const unsigned slot = warp_append(st == kCapped, D.count);
+    if (st == kCapped) {
+        if (slot < D.cap)
+            defer_store_f(P, D, slot, i, f);
+        else
+            atomicOr(&L->flags, (unsigned long long)kFlagDeferOverflow);
+    } else if (st >= 0) {
+        finish_f(M, P, S, pp, L, i, f, st, c);
+    }
+    warp_chunk_end(c);
+}
+
 // Passes 2 and 3 for entries [base, base + 32) of list Din (up to `cap` sub-steps, then
 // append to Dout; with Dout.count == nullptr the particles run to the end).
 __device__ __forceinline__ void push_more_warp(const MeshView& M, const ParticleStore& P, const SpeciesDev& S,
@@ -412,7 +512,20 @@ __device__ __forceinline__ void push_more_warp(const MeshView& M, const Particle
         f.it = Din.it[e];
         f.rem = (float)Din.rem[e];
         f.vstart = (float)Din.vstart[e];
-        st = advance_f(M, S, pp, f, chain ? cap : 0x7fffffff, A, c.nsub);
+        st = kDone;
+        if (f.cur < 0) {
+            // no location hint (only a stay-first pass 1 defers these): locate the absolute position
+            const double px = f.rx, py = f.ry, pz = f.rz;
+            const int t = locate_far(M, px, py, pz, -1);
+            if (t < 0) {
+                st = kLost;
+            } else {
+                const double3 o = origin(M, t);
+                f.rx = (float)(px - o.x); f.ry = (float)(py - o.y); f.rz = (float)(pz - o.z);
+                f.cur = t;
+            }
+        }
+        if (st != kLost) st = advance_f(M, S, pp, f, chain ? cap : 0x7fffffff, A, c.nsub);
     }
     unsigned slot = chain ? warp_append(st == kCapped, Dout.count) : 0xffffffffu;
     if (st == kCapped && chain && slot < Dout.cap) {
@@ -441,6 +554,27 @@ __global__ void __launch_bounds__(256, 6) k_push_mixed(const __grid_constant__ M
         if (b0 >= n) break;
         for (int64_t base = b0; base < b0 + 32 * kRun && base < n; base += 32)
             push1_warp(M, P, S, pp, D, A, L, base, n, c);
+    }
+    warp_stats_flush(L, ke_acc);
+}
+
+// Stay-first pass 1 (same work distribution as k_push_mixed); no walk code, so it needs far
+// fewer registers: 6 blocks of 256 per SM at 40 registers spill 64 bytes a thread, against 456
+// for the walking pass 1.
+__global__ void __launch_bounds__(256, 6) k_push_mixed_stay(const __grid_constant__ MeshView M, ParticleStore P,
+                                                         const __grid_constant__ SpeciesDev S,
+                                                         const __grid_constant__ PushParams pp, DeferList D,
+                                                         ChargeAcc A, LedgerDev* L, unsigned long long* ke_acc,
+                                                         unsigned* ctr)
+{
+    const int64_t n = *P.count;
+    PushStats c{0.0, 0u, 0u};
+    warp_stats_begin();
+    for (;;) {
+        const int64_t b0 = (int64_t)next_chunk(ctr) * (32 * kRun);
+        if (b0 >= n) break;
+        for (int64_t base = b0; base < b0 + 32 * kRun && base < n; base += 32)
+            push1_stay_warp(M, P, S, pp, D, A, L, base, n, c);
     }
     warp_stats_flush(L, ke_acc);
 }
@@ -611,9 +745,12 @@ __global__ void k_refresh_trec(int64_t T, const int4* __restrict__ tet, const do
 
 void launch_push_mixed(const MeshView& M, const ParticleStore& P, const SpeciesDev& S, const PushParams& pp,
                        const DeferList& D1, const DeferList& D2, ChargeAcc A, LedgerDev* L,
-                       unsigned long long* ke_acc, unsigned* ctr, int grid, cudaStream_t st)
+                       unsigned long long* ke_acc, unsigned* ctr, int grid, bool stay_first, cudaStream_t st)
 {
-    k_push_mixed<<<grid, 256, 0, st>>>(M, P, S, pp, D1, A, L, ke_acc, ctr);
+    if (stay_first)
+        k_push_mixed_stay<<<grid, 256, 0, st>>>(M, P, S, pp, D1, A, L, ke_acc, ctr);
+    else
+        k_push_mixed<<<grid, 256, 0, st>>>(M, P, S, pp, D1, A, L, ke_acc, ctr);
     k_push_mixed_more<<<grid, 256, 0, st>>>(M, P, S, pp, D1, D2, kCap2, A, L, ke_acc, ctr + 1);
     DeferList none{};
     k_push_mixed_more<<<grid, 256, 0, st>>>(M, P, S, pp, D2, none, 0, A, L, ke_acc, ctr + 2);

@@ -297,3 +297,38 @@ def test_mixed_precision_error_bounded(lib):
     assert (s0["status"] != s1["status"]).mean() < 0.005
     assert both.sum() > 0.9 * (s0["status"] == O.ACTIVE).sum()
     assert np.abs(s1["x"][both] - s0["x"][both]).max() < 1e-6
+
+
+def test_stay_first_push_is_bitwise_the_walking_push(lib):
+    """The precision form's stay-first pass 1 (no walk code; particles leaving their tet go to
+    the walking passes, which redo that sub-step) against the walking pass 1, for both species,
+    over steps with re-sorts, MCC and particles lost at the faces: charge, potential, field,
+    particles, ledger and statistics bitwise equal; the automatic choice likewise."""
+    from scdat_b200 import capi
+
+    mesh = O.kuhn_box((10, 9, 8), 0.05, body=((4, 6), (3, 6), (3, 5)), bias=-30.0)
+    sp = O.plasma_species(1e10, 2.0, 1.0, 0.05, 6)
+    parts = O.seed_particles(mesh, sp, 6, 123)
+    out = []
+    for mode in (capi.PUSH_WALKING, capi.PUSH_STAY_FIRST, capi.PUSH_AUTO):
+        dom = gpu_domain(mesh, 3e-8, face_bc=(2, 2, 1, 1, 1, 1), precision=1, sort_interval=2, seed=9)
+        gpu_load_particles(dom, sp, parts)
+        for s in range(len(sp)):
+            dom.set_push_mode(s, mode)
+            dom.set_elastic(s, 3e19, 1e-19)
+        dom.set_potential(mesh.phi_bc)
+        dom.solve_field()
+        dom.step(6)
+        rho, phi, E = dom.fields()
+        st = gpu_state(dom, len(sp), len(parts["tet"]))
+        out.append((rho, phi, E, st, dom.ledger(), dom.stats()))
+        dom.close()
+    ref = out[0]
+    assert ref[4][:6, 4:6].sum() > 0 and ref[5]["mcc_collisions"] > 0
+    for k in (1, 2):
+        for j in (0, 1, 2, 4):
+            assert np.array_equal(out[k][j], ref[j]), (k, j)
+        for key in ("x", "v", "tet", "status"):
+            assert np.array_equal(np.nan_to_num(out[k][3][key]), np.nan_to_num(ref[3][key])), (k, key)
+        for key in ("active_particles", "total_charge", "total_energy", "substeps", "lost_events", "mcc_collisions"):
+            assert out[k][5][key] == ref[5][key], (k, key)
