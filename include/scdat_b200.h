@@ -431,7 +431,9 @@ SCDAT_API int scdat_pcg_csr(int32_t R, const int32_t* row_ptr, const int32_t* co
  * The first call on each device looks up the array's device address (cudaGetSymbolAddress,
  * with that device current); make that first call before any stream capture.  All calls
  * share the one array, so calls that overlap on the GPU (other streams, other threads) race:
- * serialise them.  Arguments, results and blocking behaviour are those of scdat_pcg_csr. */
+ * serialise them.  The looked-up address is kept for the life of the process: do not reset the
+ * device (cudaDeviceReset) or otherwise recreate its primary context after the first call.
+ * Arguments, results and blocking behaviour are those of scdat_pcg_csr. */
 SCDAT_API int scdat_pcg_csr_noalloc(int32_t R, const int32_t* row_ptr, const int32_t* col, const double* val,
                                     const double* diag, const double* b, double* x, double rtol, int32_t max_iter,
                                     void* stream, int32_t* iterations, double* relres);

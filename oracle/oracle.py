@@ -460,6 +460,10 @@ class Reference:
         L.ref_circuit_advance.restype = C.c_int
         L.ref_whipple_yield.argtypes = [C.c_double, C.c_double, C.c_int, _dp, _dp]
         L.ref_whipple_yield.restype = None
+        L.ref_parse_cross_section_set.argtypes = [C.c_char_p]
+        L.ref_parse_cross_section_set.restype = C.c_int
+        L.ref_estimate_densities.argtypes = [C.c_int64, _i32p, _dp, _dp, _u8p, C.c_double, _dp, _dp]
+        L.ref_estimate_densities.restype = None
         self._meshes = {}
 
     def mesh(self, mesh: BoxMesh, neighbors=True):
@@ -579,6 +583,20 @@ class Reference:
         e = np.ascontiguousarray(e_ev, np.float64)
         out = np.zeros(len(e))
         self.L.ref_whipple_yield(float(peak_yield), float(peak_energy_ev), len(e), e, out)
+        return out
+
+    def parse_cross_section_set(self, text):
+        """Collision::parseCollisionCrossSectionSetId: -1 unknown, else the set's index."""
+        return int(self.L.ref_parse_cross_section_set(text.encode()))
+
+    def estimate_densities(self, types, charges, weights, active, volume, floors):
+        """Collision::estimateCollisionBackgroundDensities: (neutral, ion, electron) densities."""
+        out = np.zeros(3)
+        self.L.ref_estimate_densities(len(types), np.ascontiguousarray(types, np.int32),
+                                      np.ascontiguousarray(charges, np.float64),
+                                      np.ascontiguousarray(weights, np.float64),
+                                      np.ascontiguousarray(active, np.uint8), float(volume),
+                                      np.ascontiguousarray(floors, np.float64), out)
         return out
 
     def mcc_count(self, v, kind, w, sigma, n_target, dt, seed, repeats):

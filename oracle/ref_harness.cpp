@@ -436,4 +436,33 @@ void ref_whipple_yield(double peak_yield, double peak_energy_ev, int n, const do
             mat, SCDAT::Material::LegacySecondaryYieldModel::Whipple, e_ev[k]);
 }
 
+// Collision::parseCollisionCrossSectionSetId: -1 for an unknown name, else the set's index.
+int ref_parse_cross_section_set(const char* text)
+{
+    const auto id = SCDAT::Collision::parseCollisionCrossSectionSetId(text ? text : "");
+    return id ? (int)*id : -1;
+}
+
+// Collision::estimateCollisionBackgroundDensities over n particles (type code, charge, weight,
+// active flag) in `volume`, with the floors (neutral, ion, electron); out = the same three.
+void ref_estimate_densities(int64_t n, const int32_t* type, const double* charge, const double* weight,
+                            const uint8_t* active, double volume, const double* floor3, double* out3)
+{
+    SP::ParticleContainer box((std::size_t)std::max<int64_t>(n, 1));
+    for (int64_t i = 0; i < n; ++i) {
+        SP::Particle p((std::size_t)i + 1, (SP::ParticleType)type[i], Point3D(0, 0, 0), Vector3D(0, 0, 0), 1.0,
+                       charge[i], weight[i]);
+        if (!active[i]) p.setStatus(SP::ParticleStatus::ABSORBED);
+        box.addParticle(p);
+    }
+    SCDAT::Collision::CollisionBackgroundDensities fl{};
+    fl.neutral_density_m3 = floor3[0];
+    fl.ion_density_m3 = floor3[1];
+    fl.electron_density_m3 = floor3[2];
+    const auto d = SCDAT::Collision::estimateCollisionBackgroundDensities(box, volume, fl);
+    out3[0] = d.neutral_density_m3;
+    out3[1] = d.ion_density_m3;
+    out3[2] = d.electron_density_m3;
+}
+
 }  // extern "C"

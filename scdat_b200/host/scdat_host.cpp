@@ -2,6 +2,10 @@
 // device through the C ABI.  No numerical step of the path runs here; see scdat_host.hpp.
 #include "scdat_host.hpp"
 
+#include <cmath>
+
+#include <cctype>
+
 #include "scdat_b200.h"
 
 #include <algorithm>
@@ -1071,32 +1075,60 @@ void MonteCarloCollisionHandler::clearProcesses()
     unsupported_.clear();
 }
 
-// estimateCollisionBackgroundDensities (CollisionPicAdapter.cpp:212-261): the floors, raised by
-// the particle densities counted in the container (sum of weights / volume).
+// estimateCollisionBackgroundDensities (CollisionPicAdapter.cpp:212-261): the floors (a
+// non-finite or negative floor counts as 0, sanitizeDensity at :58-65), raised by the weight
+// densities of the container's active particles by class: electron-like (ELECTRON, or any
+// negative charge), ion-like (PROTON, ION, or any positive charge) and neutral (the rest), as
+// isElectronLike / isIonLike (:23-56) classify the types this layer knows.
+namespace {
+double sanitize_density(double d) { return std::isfinite(d) ? std::max(0.0, d) : 0.0; }
+
+std::string lower_case(std::string t)
+{
+    std::transform(t.begin(), t.end(), t.begin(), [](unsigned char c) { return (char)std::tolower(c); });
+    return t;
+}
+}  // namespace
+
 CollisionBackgroundDensities estimateCollisionBackgroundDensities(const Particle::ParticleContainer& container,
                                                                   double volume_m3,
                                                                   const CollisionBackgroundDensities& floor)
 {
-    CollisionBackgroundDensities d = floor;
-    if (!(volume_m3 > 0.0)) return d;
-    double ne = 0.0, ni = 0.0;
+    CollisionBackgroundDensities d{};
+    d.neutral_density_m3 = sanitize_density(floor.neutral_density_m3);
+    d.ion_density_m3 = sanitize_density(floor.ion_density_m3);
+    d.electron_density_m3 = sanitize_density(floor.electron_density_m3);
+    if (!(volume_m3 > 0.0) || !std::isfinite(volume_m3)) return d;
+    double ne = 0.0, ni = 0.0, nn = 0.0;
     for (const auto& p : container) {
         if (!p.isActive()) continue;
-        if (p.getType() == Particle::ParticleType::ELECTRON)
-            ne += p.getWeight();
-        else if (p.getCharge() > 0.0)
-            ni += p.getWeight();
+        const double w = std::max(0.0, p.getWeight());
+        const auto t = p.getType();
+        if (t == Particle::ParticleType::ELECTRON || p.getCharge() < 0.0)
+            ne += w;
+        else if (t == Particle::ParticleType::PROTON || t == Particle::ParticleType::ION || p.getCharge() > 0.0)
+            ni += w;
+        else
+            nn += w;
     }
-    d.electron_density_m3 = std::max(d.electron_density_m3, ne / volume_m3);
-    d.ion_density_m3 = std::max(d.ion_density_m3, ni / volume_m3);
+    const double inv = 1.0 / volume_m3;
+    d.electron_density_m3 = std::max(d.electron_density_m3, ne * inv);
+    d.ion_density_m3 = std::max(d.ion_density_m3, ni * inv);
+    d.neutral_density_m3 = std::max(d.neutral_density_m3, nn * inv);
     return d;
 }
 
+// parseCollisionCrossSectionSetId (CollisionPicAdapter.cpp:263-282): case-insensitive, with the
+// reference's aliases of each set.
 std::optional<CollisionCrossSectionSetId> parseCollisionCrossSectionSetId(const std::string& text)
 {
-    if (text == "background_mcc_v1") return CollisionCrossSectionSetId::BackgroundMccV1;
-    if (text == "surface_pic_v1") return CollisionCrossSectionSetId::SurfacePicV1;
-    if (text == "vacuum_arc_pic_v1") return CollisionCrossSectionSetId::VacuumArcPicV1;
+    const std::string n = lower_case(text);
+    if (n == "background_mcc_v1" || n == "backgroundmccv1" || n == "default" || n == "background")
+        return CollisionCrossSectionSetId::BackgroundMccV1;
+    if (n == "surface_pic_v1" || n == "surfacepicv1" || n == "surface_pic" || n == "surfacepic")
+        return CollisionCrossSectionSetId::SurfacePicV1;
+    if (n == "vacuum_arc_pic_v1" || n == "vacuumarcpicv1" || n == "arcpic_background_v1" || n == "arcpic")
+        return CollisionCrossSectionSetId::VacuumArcPicV1;
     return std::nullopt;
 }
 

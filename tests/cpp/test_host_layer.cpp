@@ -415,8 +415,47 @@ int parity(const char* in_path, const char* out_path)
 
 }  // namespace
 
+// Host-side collision helpers on inputs from the test (no GPU): "parse <name>" prints the set
+// index (-1: unknown); "densities <in> <out>" reads n, then n x (type, charge, weight, active),
+// the volume and the three floors, and writes the three densities.
+int collision_helpers(int argc, char** argv)
+{
+    if (argc == 3 && std::strcmp(argv[1], "parse") == 0) {
+        const auto id = SCDAT::Collision::parseCollisionCrossSectionSetId(argv[2]);
+        std::printf("%d\n", id ? (int)*id : -1);
+        return 0;
+    }
+    std::ifstream in(argv[2], std::ios::binary);
+    int64_t n = 0;
+    in.read(reinterpret_cast<char*>(&n), sizeof(n));
+    SCDAT::Particle::ParticleContainer box;
+    for (int64_t i = 0; i < n; ++i) {
+        double rec[4];
+        in.read(reinterpret_cast<char*>(rec), sizeof(rec));
+        SCDAT::Particle::Particle p((SCDAT::Particle::ParticleId)(i + 1), (SCDAT::Particle::ParticleType)(int)rec[0],
+                                    SCDAT::Geometry::Point3D(0, 0, 0), SCDAT::Geometry::Vector3D(0, 0, 0), 1.0, rec[1],
+                                    rec[2]);
+        if (rec[3] == 0.0) p.setStatus(SCDAT::Particle::ParticleStatus::ABSORBED);
+        box.addParticle(p);
+    }
+    double vf[4];
+    in.read(reinterpret_cast<char*>(vf), sizeof(vf));
+    if (!in) return 2;
+    SCDAT::Collision::CollisionBackgroundDensities fl{};
+    fl.neutral_density_m3 = vf[1];
+    fl.ion_density_m3 = vf[2];
+    fl.electron_density_m3 = vf[3];
+    const auto d = SCDAT::Collision::estimateCollisionBackgroundDensities(box, vf[0], fl);
+    std::ofstream out(argv[3], std::ios::binary);
+    const double o[3] = {d.neutral_density_m3, d.ion_density_m3, d.electron_density_m3};
+    out.write(reinterpret_cast<const char*>(o), sizeof(o));
+    return out ? 0 : 3;
+}
+
 int main(int argc, char** argv)
 {
+    if ((argc == 3 && std::strcmp(argv[1], "parse") == 0) || (argc == 4 && std::strcmp(argv[1], "densities") == 0))
+        return collision_helpers(argc, argv);
     if (argc == 4 && std::strcmp(argv[1], "parity") == 0) {
         try {
             return parity(argv[2], argv[3]);

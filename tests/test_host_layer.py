@@ -106,3 +106,38 @@ def test_picycle_host_layer_matches_oracle(lib, orc, tmp_path):
     assert np.array_equal(led[:, 4:6], ref["ledger"][:6, 4:6])
     np.testing.assert_allclose(led[:, [0, 1, 3]], ref["ledger"][:6, [0, 1, 3]], rtol=TOL, atol=1e-30)
     np.testing.assert_allclose(sc, ref["surface_charge"], rtol=TOL, atol=1e-30)
+
+
+def test_collision_helpers_match_reference(ref, tmp_path):
+    """The host layer's parseCollisionCrossSectionSetId and estimateCollisionBackgroundDensities
+    against the reference's own (CollisionPicAdapter.cpp:212-282) on CPU: case folding and
+    aliases of the set names; floors sanitised (non-finite or negative -> 0) and raised by the
+    electron-like, ion-like and neutral weight densities of the active particles."""
+    exe = _build_exe()
+    for name in ("background_mcc_v1", "Background", "DEFAULT", "BackgroundMccV1", "surfacePIC", "surface_pic",
+                 "Surface_Pic_V1", "ArcPic", "vacuumarcpicv1", "arcpic_background_v1", "VACUUM_ARC_PIC_V1", "nonsense",
+                 "", "background_mcc_v2"):
+        r = subprocess.run([exe, "parse", name], capture_output=True, text=True, timeout=30)
+        assert r.returncode == 0
+        assert int(r.stdout) == ref.parse_cross_section_set(name), name
+    rng = np.random.default_rng(4)
+    types = (1, 20, 52, 0)  # electron, proton, ion, unknown (classified by the sign of its charge)
+    for trial in range(12):
+        n = int(rng.integers(0, 60))
+        t = rng.choice(types, n)
+        q = np.where(rng.random(n) < 0.3, 0.0, rng.choice([-1.0, 1.0], n) * 1.602176634e-19)
+        w = np.where(rng.random(n) < 0.1, -1.0, rng.uniform(0.0, 1e6, n))
+        act = (rng.random(n) < 0.8).astype(np.uint8)
+        vol = [1e-6, 0.0, -1.0, np.inf, 2.5e-3][trial % 5]
+        floors = np.array([[1e14, 0.0, 3e12], [np.nan, -5.0, np.inf], [0.0, 1e9, 1e9]][trial % 3])
+        case = tmp_path / f"case{trial}.bin"
+        with open(case, "wb") as f:
+            np.array([n], np.int64).tofile(f)
+            np.stack([t.astype(float), q, w, act.astype(float)], axis=1).astype(np.float64).tofile(f)
+            np.array([vol, *floors], np.float64).tofile(f)
+        out = tmp_path / f"out{trial}.bin"
+        r = subprocess.run([exe, "densities", str(case), str(out)], capture_output=True, text=True, timeout=30)
+        assert r.returncode == 0, r.stdout + r.stderr
+        mine = np.fromfile(out, np.float64)
+        theirs = ref.estimate_densities(t, q, w, act, vol, floors)
+        np.testing.assert_array_equal(mine, theirs)
