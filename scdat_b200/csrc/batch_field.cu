@@ -32,8 +32,10 @@ __global__ void k_batch_zero(const FieldJob* __restrict__ jobs, const PushJob* _
     unsigned long long* h = J.h;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nl; i += (int64_t)gridDim.x * blockDim.x) {
         l0[i] = 0ull;
-        l1[i] = 0ull;
-        h[i] = 0ull;
+        if (l1) {  // limb layout (the precision form uses l0 alone)
+            l1[i] = 0ull;
+            h[i] = 0ull;
+        }
     }
     if (blockIdx.x == 0) {
         if (threadIdx.x == 0) {

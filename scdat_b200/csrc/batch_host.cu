@@ -121,7 +121,7 @@ int upload_jobs(scdat_batch* b)
         J.P = store_of(c, s);
         J.S = species_dev(c, s);
         J.pp = push_params(c, true);
-        J.A = ChargeAcc{c->acc_l0.p + s * N, c->acc_l1.p + s * N, c->acc_h.p + s * N};
+        J.A = ChargeAcc{c->acc_l0.p + s * N, nullptr, nullptr};  // batched contexts are all mixed: one word
         J.L = c->led.p;
         J.ke_acc = c->ke_acc.p;
         DeferBufs& d = *b->defer[j];
@@ -138,8 +138,8 @@ int upload_jobs(scdat_batch* b)
         F.T = c->hm.T;
         F.S = (int)c->species.size();
         F.l0 = c->acc_l0.p;
-        F.l1 = c->acc_l1.p;
-        F.h = c->acc_h.p;
+        F.l1 = nullptr;
+        F.h = nullptr;
         F.ke_acc = c->ke_acc.p;
         F.led_active = &c->led.p->active;
         F.lsq_bad = &c->led.p->lsq_bad;

@@ -215,8 +215,10 @@ int do_push(scdat_ctx* ctx, bool do_mcc)
     }
     const int64_t N = ctx->hm.N;
     CK(cudaMemsetAsync(ctx->acc_l0.p, 0, sizeof(unsigned long long) * S * N, ctx->st));
-    CK(cudaMemsetAsync(ctx->acc_l1.p, 0, sizeof(unsigned long long) * S * N, ctx->st));
-    CK(cudaMemsetAsync(ctx->acc_h.p, 0, sizeof(unsigned long long) * S * N, ctx->st));
+    if (!ctx->mixed) {  // the precision form accumulates one word per node (fx_red_word)
+        CK(cudaMemsetAsync(ctx->acc_l1.p, 0, sizeof(unsigned long long) * S * N, ctx->st));
+        CK(cudaMemsetAsync(ctx->acc_h.p, 0, sizeof(unsigned long long) * S * N, ctx->st));
+    }
     CK(cudaMemsetAsync(ctx->ke_acc.p, 0, 2 * sizeof(unsigned long long), ctx->st));
     CK(cudaMemsetAsync(&ctx->led.p->active, 0, sizeof(unsigned long long), ctx->st));
     PushParams pp = push_params(ctx, do_mcc);
@@ -236,7 +238,8 @@ int do_push(scdat_ctx* ctx, bool do_mcc)
         DeferList d1{ctx->dcount.p, ctx->d1cap, ctx->d1idx.p, ctx->d1it.p, ctx->d1rem.p, ctx->d1vs.p};
         DeferList d2{ctx->dcount.p + 1, ctx->dcap, ctx->d2idx.p, ctx->d2it.p, ctx->d2rem.p, ctx->d2vs.p};
         ctx->launches += 3;
-        ChargeAcc acc{ctx->acc_l0.p + s * N, ctx->acc_l1.p + s * N, ctx->acc_h.p + s * N};
+        ChargeAcc acc = ctx->mixed ? ChargeAcc{ctx->acc_l0.p + s * N, nullptr, nullptr}
+                                   : ChargeAcc{ctx->acc_l0.p + s * N, ctx->acc_l1.p + s * N, ctx->acc_h.p + s * N};
         if (ctx->mixed) {
             const bool stay = stay_first_now(ctx, s);
             launch_push_mixed(ctx->mv, P, sd, pp, d1, d2, acc, ctx->led.p, ctx->ke_acc.p, ctx->dcount.p + 2,
@@ -260,7 +263,8 @@ int do_push(scdat_ctx* ctx, bool do_mcc)
     }
     CK(cudaMemsetAsync(ctx->totq.p, 0, sizeof(unsigned long long) * 2, ctx->st));
     ++ctx->launches;
-    launch_finalize_rho(N, S, ctx->acc_l0.p, ctx->acc_l1.p, ctx->acc_h.p, ctx->uq, ctx->rho.p, ctx->totq.p,
+    launch_finalize_rho(N, S, ctx->acc_l0.p, ctx->mixed ? nullptr : ctx->acc_l1.p, ctx->mixed ? nullptr : ctx->acc_h.p,
+                        ctx->uq, ctx->rho.p, ctx->totq.p,
                         ctx->totq.p + 1, ctx->grid_nodes, ctx->st);
     CK(cudaGetLastError());
     return SCDAT_OK;
@@ -1610,7 +1614,8 @@ SCDAT_API int scdat_get_species_charge(scdat_ctx* ctx, int32_t species, double* 
     if (!ctx) return SCDAT_ERR_ARG;
     ARG(species >= 0 && species < (int)ctx->species.size() && rho_s, "bad species index");
     const int64_t N = ctx->hm.N;
-    launch_species_rho(N, ctx->acc_l0.p + species * N, ctx->acc_l1.p + species * N, ctx->acc_h.p + species * N,
+    launch_species_rho(N, ctx->acc_l0.p + species * N, ctx->mixed ? nullptr : ctx->acc_l1.p + species * N,
+                       ctx->mixed ? nullptr : ctx->acc_h.p + species * N,
                        ctx->uq, ctx->tmp_rho.p, ctx->grid_nodes, ctx->st);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(rho_s, ctx->tmp_rho.p, sizeof(double) * N, cudaMemcpyDeviceToHost, ctx->st));

@@ -66,10 +66,11 @@ struct GatherArrays {
 };
 
 
-// Node charge accumulators: each 128-bit contribution is split into 32-bit limbs that go
-// into three 64-bit words with return-free atomic adds (no thread waits on an atomic), and
-// the limbs are recombined exactly when the charge is read.  2^32 contributions per node
-// and step fit before a limb could wrap.
+// Node charge accumulators of the FP64 form: each 128-bit contribution is split into 32-bit
+// limbs that go into three 64-bit words with return-free atomic adds (no thread waits on an
+// atomic), and the limbs are recombined exactly when the charge is read.  2^32 contributions
+// per node and step fit before a limb could wrap.  The precision form uses l0 alone, as one
+// word per node (fx_red_word), with l1 = h = nullptr.
 struct ChargeAcc {
     unsigned long long* l0;  // bits 0..31 of each contribution
     unsigned long long* l1;  // bits 32..63
@@ -84,12 +85,41 @@ __device__ __forceinline__ void fx_red(const ChargeAcc& A, int node, const Fx128
     if (v.hi) atomicAdd(A.h + node, (unsigned long long)v.hi);
 }
 
+// The precision form's accumulators: one signed 64-bit word per node in units of 2^-36 of
+// the charge unit.  Its contributions carry FP32 barycentric weights (24-bit mantissas), so
+// this resolution loses nothing they hold, and each contribution is one return-free atomic
+// (against three limb atomics).  A node's sum stays exact up to 2^27 unit charges per step.
+constexpr double kWordScale = 68719476736.0;  // 2^36
+
+__device__ __forceinline__ void fx_red_word(const ChargeAcc& A, int node, double v)
+{
+    const long long w = __double2ll_rn(v * kWordScale);
+    if (w) atomicAdd(A.l0 + node, (unsigned long long)w);
+}
+
+// the word as a 128-bit value in units of 2^-64
+__host__ __device__ inline Fx128 fx_from_word(unsigned long long w)
+{
+    const long long s = (long long)w;
+    return Fx128{w << 28, s >> 36};
+}
+
+// A limb triple, or with l1 == nullptr a single word (the precision form's layout).
+__host__ __device__ inline Fx128 fx_from_acc(const unsigned long long* l0, const unsigned long long* l1,
+                                             const unsigned long long* h, int64_t i);
+
 __host__ __device__ inline Fx128 fx_from_limbs(unsigned long long l0, unsigned long long l1, unsigned long long h)
 {
     Fx128 r{l0, (long long)h};
     Fx128 m{l1 << 32, (long long)(l1 >> 32)};
     fx_add(r, m);
     return r;
+}
+
+__host__ __device__ inline Fx128 fx_from_acc(const unsigned long long* l0, const unsigned long long* l1,
+                                             const unsigned long long* h, int64_t i)
+{
+    return l1 ? fx_from_limbs(l0[i], l1[i], h[i]) : fx_from_word(l0[i]);
 }
 
 // ------------------------------------------------------------------------------------

@@ -86,7 +86,7 @@ __device__ __forceinline__ void k_finalize_rho_body(int64_t N, int S, const unsi
     Fx128 tot{0ull, 0ll};
     for (int64_t n = g.b * (int64_t)blockDim.x + threadIdx.x; n < N; n += (int64_t)g.n * blockDim.x) {
         Fx128 a{0ull, 0ll};
-        for (int s = 0; s < S; ++s) fx_add(a, fx_from_limbs(l0[s * N + n], l1[s * N + n], h[s * N + n]));
+        for (int s = 0; s < S; ++s) fx_add(a, fx_from_acc(l0, l1, h, s * N + n));
         rho[n] = fx_to_double(a.lo, a.hi, unit);
         fx_add(tot, a);
     }
@@ -105,7 +105,7 @@ __device__ __forceinline__ void k_species_rho_body(int64_t N, const unsigned lon
                               double unit, double* __restrict__ out, Grid g)
 {
     for (int64_t n = g.b * (int64_t)blockDim.x + threadIdx.x; n < N; n += (int64_t)g.n * blockDim.x) {
-        Fx128 a = fx_from_limbs(l0[n], l1[n], h[n]);
+        Fx128 a = fx_from_acc(l0, l1, h, n);
         out[n] = fx_to_double(a.lo, a.hi, unit);
     }
 }

@@ -117,9 +117,10 @@ __device__ __forceinline__ int walk64(const MeshView& M, double px, double py, d
             return t;
         }
         int f = 0;
-#pragma unroll
-        for (int i = 1; i < 4; ++i)
-            if (lam[i] < lam[f]) f = i;
+        double lm = lam[0];
+        if (lam[1] < lm) { lm = lam[1]; f = 1; }
+        if (lam[2] < lm) { lm = lam[2]; f = 2; }
+        if (lam[3] < lm) f = 3;
         int4 nb = rec_nbr(M, t);
         int nt = f == 0 ? nb.x : (f == 1 ? nb.y : (f == 2 ? nb.z : nb.w));
         if (nt < 0) return -1;
@@ -292,9 +293,13 @@ static __device__ __noinline__ int resolve_lost(const MeshView& M, const Species
                 const double d[6] = {fabs(px - pp.blo[0]), fabs(pp.bhi[0] - px), fabs(py - pp.blo[1]),
                                      fabs(pp.bhi[1] - py), fabs(pz - pp.blo[2]), fabs(pp.bhi[2] - pz)};
                 int k = 0;
+                double dk = d[0];
 #pragma unroll
                 for (int f = 1; f < 6; ++f)
-                    if (d[f] < d[k]) k = f;
+                    if (d[f] < dk) {
+                        dk = d[f];
+                        k = f;
+                    }
                 fx_atomic_add(&L->patch_q[k][0], &L->patch_q[k][1], fx_from_double(S.q * S.w * pp.inv_uq));
                 atomicAdd(&L->patch_n[k], 1ull);
                 // secondaries leave the face: it gains delta |q| w, the ledger records their charge

@@ -8,7 +8,7 @@
 // a face neighbour is re-based in FP32 from the FP64 node difference; anything farther (walk,
 // grid lookup, boundary events) reconstructs the FP64 absolute position and uses the FP64
 // locate.  Deposit weights are FP32 barycentrics promoted to FP64 before the exact
-// fixed-point accumulation.
+// fixed-point accumulation (one 64-bit word per node, fx_red_word).
 //
 // Sub-steps run in passes so that warps stay converged: pass 1 gives every particle at most
 // kCap1 sub-steps and appends the unfinished ones to a list; pass 2 gives those up to kCap2
@@ -115,10 +115,12 @@ static __device__ __noinline__ Reloc relocate_f(const MeshView& M, int cur, floa
     load_j(M, t, j);
     baryj(j, qx, qy, qz, l);
     for (int k = 0; k < kWalkSteps; ++k) {
+        // the most violated face (lowest barycentric, the first on ties), without indexing l
         int f = 0;
-#pragma unroll
-        for (int i = 1; i < 4; ++i)
-            if (l[i] < l[f]) f = i;
+        float lm = l[0];
+        if (l[1] < lm) { lm = l[1]; f = 1; }
+        if (l[2] < lm) { lm = l[2]; f = 2; }
+        if (l[3] < lm) f = 3;
         const float* rec = M.trec + 64 * (int64_t)t;
         int nt = __float_as_int(__ldg(rec + 25 + f));
         if (nt < 0) break;
@@ -199,7 +201,7 @@ __device__ __forceinline__ void deposit_traj_f(const MeshView& M, const SpeciesD
     const int* nd = reinterpret_cast<const int*>(M.trec + 64 * (int64_t)t + 21);
     for (int k = 0; k < 4; ++k) {
         int node = __ldg(nd + k);
-        fx_red(A, node, fx_from_double((cw * (double)sum[k]) * pp.inv_uq));
+        fx_red_word(A, node, (cw * (double)sum[k]) * pp.inv_uq);
     }
 }
 
@@ -267,7 +269,7 @@ __device__ __forceinline__ int advance_f(const MeshView& M, const SpeciesDev& S,
                     for (int q = 0; q < 4; ++q) {
                         float lk = tiny ? l[q] : (pp.dep_kernel == 0 ? le[q] : 0.5f * (l[q] + le[q]));
                         const int nd = __float_as_int(__ldg(reinterpret_cast<const float*>(rec) + 21 + q));
-                        fx_red(A, nd, fx_from_double((qw * (double)lk) * pp.inv_uq));
+                        fx_red_word(A, nd, (qw * (double)lk) * pp.inv_uq);
                     }
                 } else {
                     deposit_traj_f(M, S, pp, f.cur, sx, sy, sz, f.rx, f.ry, f.rz, A);
@@ -448,7 +450,7 @@ __device__ __forceinline__ int advance_stay_f(const MeshView& M, const SpeciesDe
         for (int q = 0; q < 4; ++q) {
             const float lk = tiny ? l[q] : (pp.dep_kernel == 0 ? le[q] : 0.5f * (l[q] + le[q]));
             const int nd = __float_as_int(__ldg(reinterpret_cast<const float*>(rec) + 21 + q));
-            fx_red(A, nd, fx_from_double((qw * (double)lk) * pp.inv_uq));
+            fx_red_word(A, nd, (qw * (double)lk) * pp.inv_uq);
         }
     }
     f.rx = rx; f.ry = ry; f.rz = rz;
