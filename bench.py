@@ -176,7 +176,7 @@ def build_domain(cfg, precision, capi, solve=True, mesh_cache=None):
     if cfg.get("ion_sort_interval"):
         dom.set_species_sort_interval(1, cfg["ion_sort_interval"])
     for s in range(2):
-        dom.set_elastic(s, 1e14, 1e-19, mode=1)
+        dom.set_elastic(s, 1e14, 1e-19, mode=2)  # null-collision MCC
     if cfg.get("precond") == "multigrid":
         dom.set_preconditioner(capi.PRECOND_MULTIGRID)
     dom.set_potential(m["phi"])

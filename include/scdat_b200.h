@@ -97,7 +97,13 @@ typedef struct {
 /* Elastic background collision for one species: ElasticCollisionCrossSection
  * (Tools/Interactions/Collisions/src/CollisonTypes.cpp:60-78) against a neutral background.
  * mode 0: the reference two-draw test (CollisionAlgorithm.cpp:525-531 then :195-200);
- * mode 1: one draw against 1-exp(-nu*dt). */
+ * mode 1: one draw against 1-exp(-nu*dt);
+ * mode 2: null collision: with nu_max = n * sigma_max * vmax, where vmax is the species'
+ * largest speed at the end of the previous push, every particle no faster than vmax is
+ * selected with probability 1-exp(-nu_max*dt) by a cheap counter-based draw and then collides
+ * with probability nu/nu_max; faster particles (and all of them before the first push) take
+ * mode 1's draw.  The collision law is mode 1's to first order in nu*dt, and most particles
+ * skip the Philox draws. */
 typedef struct {
     double target_density;  /* m^-3 */
     double sigma_max;       /* m^2 */

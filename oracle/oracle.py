@@ -296,7 +296,7 @@ class Oracle:
         L.orc_poisson_cg.restype = C.c_int
         L.orc_lsq_efield.argtypes = [C.c_int64, _dp, _i64p, _i32p, _dp, C.c_double, _dp]
         L.orc_mcc.argtypes = [C.c_int64, _dp, _i32p, _u8p, _i64p, _dp, C.POINTER(Elastic), C.c_double,
-                              C.c_uint64, C.c_uint32, C.c_int]
+                              C.c_uint64, C.c_uint32, C.c_int, C.c_void_p]
         L.orc_mcc.restype = C.c_int64
         L.orc_boris.argtypes = [_dp, _dp, C.c_double, C.c_double, _dp]
         L.orc_boris.restype = None
@@ -418,13 +418,28 @@ class Oracle:
                               E)
         return E.reshape(-1, 3)
 
-    def mcc(self, v, species_idx, status, ids, species, procs, dt, seed, step, mode=0):
+    def mcc(self, v, species_idx, status, ids, species, procs, dt, seed, step, mode=0, vmax=None):
+        """vmax (mode 2): per species, the largest speed of the previous push (None: none yet)."""
         v = v.copy()
         sm = np.array([s.m for s in species])
         arr = (Elastic * len(procs))(*procs)
+        vm = None if vmax is None else np.ascontiguousarray(vmax, np.float64)
         hits = self.L.orc_mcc(v.shape[0], v.reshape(-1), species_idx.astype(np.int32), status.astype(np.uint8),
-                              ids.astype(np.int64), sm, arr, dt, seed, step, mode)
+                              ids.astype(np.int64), sm, arr, dt, seed, step, mode,
+                              None if vm is None else vm.ctypes.data_as(C.c_void_p))
         return v, int(hits)
+
+
+def push_speed_bound(v, species_idx, status, nspecies):
+    """The device's null-collision speed bound of each species after a push: the largest
+    squared speed of the active particles rounded to FP32, its FP32 square root."""
+    out = np.zeros(nspecies)
+    v2 = np.sum(np.asarray(v, np.float64) ** 2, axis=1).astype(np.float32)
+    for s in range(nspecies):
+        m = (species_idx == s) & (status == ACTIVE)
+        if m.any():
+            out[s] = float(np.sqrt(np.float32(v2[m].max()), dtype=np.float32))
+    return out
 
 
 # ---------------------------------------------------------------------------------------

@@ -847,9 +847,29 @@ static double orc_sigma_elastic(const orc_elastic* pr, double e_ev)
     return s > 0.0 ? s : 0.0;
 }
 
+/* splitmix64's output mix (Steele, Lea and Flood, OOPSLA 2014) and the null-collision
+ * selection draw for (seed; id, step), as the device computes them. */
+static uint64_t orc_mix64(uint64_t z)
+{
+    z ^= z >> 30;
+    z *= 0xBF58476D1CE4E5B9ull;
+    z ^= z >> 27;
+    z *= 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    return z;
+}
+
+static double orc_select_uniform(uint64_t seed, uint32_t id, uint32_t step)
+{
+    const uint64_t key = ((uint64_t)step << 32) | (uint64_t)id;
+    const uint64_t z = orc_mix64(orc_mix64(seed ^ 0x5CDA7B2005CDA7B2ull) + key * 0x9E3779B97F4A7C15ull);
+    return ((double)(z >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+}
+
+/* vmax (mode 2): per species, the largest speed of the previous push (0: none yet). */
 ORC_API int64_t orc_mcc(int64_t P, double* v, const int32_t* species, const uint8_t* status, const int64_t* pid,
                         const double* sm, const orc_elastic* proc, double dt, uint64_t seed, uint32_t step,
-                        int mode)
+                        int mode, const double* vmax)
 {
     int64_t hits = 0;
     const double two_pi = 2.0 * 3.14159265358979323846;
@@ -859,17 +879,32 @@ ORC_API int64_t orc_mcc(int64_t P, double* v, const int32_t* species, const uint
         if (!pr->enabled) continue;
         double m = sm[species[ip]];
         v3 vel = {v[3 * ip], v[3 * ip + 1], v[3 * ip + 2]};
-        double speed = v3mag(vel);
+        const double v2 = vel.x * vel.x + vel.y * vel.y + vel.z * vel.z;
+        double speed = sqrt(v2);
         double e_ev = 0.5 * m * speed * speed / ORC_QE;
         double nu = pr->n_target * orc_sigma_elastic(pr, e_ev) * speed;
         double u[2], u2[2];
-        orc_uniform2(seed, (uint64_t)pid[ip], step, 2u, u);
+        const double vm = (mode == 2 && vmax) ? vmax[species[ip]] : 0.0;
         int hit;
-        if (mode == 0) {
+        if (mode == 2 && vm > 0.0 && v2 <= vm * vm) {
+            /* null collision: selection with 1 - exp(-nu_max dt), then nu / nu_max */
+            const double numax = pr->n_target * pr->sigma_max * vm;
+            const double xmax = numax * dt;
+            const double us = orc_select_uniform(seed, (uint32_t)pid[ip], step);
+            if (us >= xmax + 1e-15 || !(us < 1.0 - exp(-xmax))) continue;
+            orc_uniform2(seed, (uint64_t)pid[ip], step, 2u, u);
+            hit = u[0] * numax < nu;
+        } else if (mode == 2) {
+            orc_uniform2(seed, (uint64_t)pid[ip], step, 2u, u);
+            const double x = nu * dt;
+            hit = !(u[0] >= x + 1e-15) && u[0] < 1.0 - exp(-x);
+        } else if (mode == 0) {
+            orc_uniform2(seed, (uint64_t)pid[ip], step, 2u, u);
             double p = nu * dt;
             p = p < 0.0 ? 0.0 : (p > 1.0 ? 1.0 : p);
             hit = (u[0] < p) && !(u[1] >= p);
         } else {
+            orc_uniform2(seed, (uint64_t)pid[ip], step, 2u, u);
             double p = 1.0 - exp(-nu * dt);
             hit = u[0] < p;
         }

@@ -35,6 +35,7 @@ struct FieldJob {
     // per-step accumulators
     unsigned long long *l0, *l1, *h;  // charge limbs [S*N]
     unsigned long long* ke_acc;       // kinetic energy of the push, exact fixed point (lo, hi)
+    unsigned* vmax;                   // [2 per species] maximum speeds (SpeciesDev::vmax)
     unsigned long long* led_active;
     unsigned long long* lsq_bad;
     // charge finalisation

@@ -46,6 +46,10 @@ __global__ void k_batch_zero(const FieldJob* __restrict__ jobs, const PushJob* _
             J.totq[1] = 0ull;
             *J.lsq_bad = 0ull;
         }
+        for (int s = threadIdx.x; s < J.S; s += blockDim.x) {  // the null-collision speed bound
+            J.vmax[2 * s] = J.vmax[2 * s + 1];
+            J.vmax[2 * s + 1] = 0u;
+        }
         if (blockIdx.y == 0)
             for (int j = threadIdx.x; j < npjobs; j += blockDim.x) {
                 *pjobs[j].D1.count = 0u;

@@ -141,6 +141,7 @@ int upload_jobs(scdat_batch* b)
         F.l1 = nullptr;
         F.h = nullptr;
         F.ke_acc = c->ke_acc.p;
+        F.vmax = c->vmax.p;
         F.led_active = &c->led.p->active;
         F.lsq_bad = &c->led.p->lsq_bad;
         F.uq = c->uq;

@@ -53,6 +53,7 @@ void launch_gather_mixed(int64_t n, const int64_t* active, const uint32_t* perm,
                          uint32_t nohint_key, const float4* in_mix, const uint32_t* in_id, float4* out_mix,
                          int32_t* out_tet, uint32_t* out_id, cudaStream_t st);
 void launch_scatter_values(int64_t n, const int64_t* idx, const double* v, double* dst, cudaStream_t st);
+void launch_rotate_vmax(int S, unsigned* v, cudaStream_t st);
 }  // namespace scdat
 
 using namespace scdat;
@@ -120,6 +121,7 @@ SpeciesDev species_dev(const scdat_ctx* ctx, int s)
     d.mcc_eref = S.mcc.e_ref_ev;
     d.mcc_alpha = S.mcc.alpha;
     d.mcc_eth = S.mcc.e_threshold_ev;
+    d.vmax = ctx->vmax.p ? ctx->vmax.p + 2 * s : nullptr;
     return d;
 }
 
@@ -221,6 +223,8 @@ int do_push(scdat_ctx* ctx, bool do_mcc)
     }
     CK(cudaMemsetAsync(ctx->ke_acc.p, 0, 2 * sizeof(unsigned long long), ctx->st));
     CK(cudaMemsetAsync(&ctx->led.p->active, 0, sizeof(unsigned long long), ctx->st));
+    ++ctx->launches;
+    launch_rotate_vmax(S, ctx->vmax.p, ctx->st);
     PushParams pp = push_params(ctx, do_mcc);
     StageEvents ev;
     if (ctx->timing) {
@@ -936,6 +940,8 @@ SCDAT_API int scdat_set_species(scdat_ctx* ctx, int32_t n_species, const scdat_s
     CK(ctx->acc_l1.alloc((size_t)(n_species * N)));
     CK(ctx->acc_h.alloc((size_t)(n_species * N)));
     CK(ctx->counts.alloc((size_t)n_species));
+    CK(ctx->vmax.alloc(2 * (size_t)n_species));
+    CK(cudaMemsetAsync(ctx->vmax.p, 0, 2 * sizeof(unsigned) * n_species, ctx->st));
     CK(cudaMallocHost((void**)&ctx->h_deferred, sizeof(unsigned) * n_species));
     std::memset(ctx->h_deferred, 0, sizeof(unsigned) * n_species);
     CK(cudaMemsetAsync(ctx->counts.p, 0, sizeof(int64_t) * n_species, ctx->st));
@@ -962,6 +968,8 @@ static int alloc_species(scdat_ctx* ctx, int s, int64_t n)
     S.cap = cap;
     S.n = n;
     CK(cudaMemcpyAsync(ctx->counts.p + s, &S.n, sizeof(int64_t), cudaMemcpyHostToDevice, ctx->st));
+    // new particles: no maximum speed yet (the next push's MCC takes the direct draw)
+    CK(cudaMemsetAsync(ctx->vmax.p + 2 * s, 0, 2 * sizeof(unsigned), ctx->st));
     // deferred lists of the multi-pass push: pass 1's list covers the largest species (a
     // stay-first pass 1 may defer every particle), pass 2's a quarter of it (a full list only
     // means the overflow finishes in pass 2)
@@ -1463,6 +1471,7 @@ SCDAT_API int scdat_set_elastic_mcc(scdat_ctx* ctx, int32_t species, const scdat
     if (!ctx) return SCDAT_ERR_ARG;
     ARG(species >= 0 && species < (int)ctx->species.size(), "bad species index");
     ARG(proc && proc->target_density >= 0.0 && proc->sigma_max >= 0.0, "bad collision process");
+    ARG(proc->mode >= 0 && proc->mode <= 2, "collision mode must be 0, 1 or 2");
     ctx->species[species].mcc = *proc;
     return SCDAT_OK;
 }

@@ -221,7 +221,31 @@ struct SpeciesDev {
     int32_t mcc_mode;
     int32_t pad;
     double mcc_n, mcc_sigma, mcc_eref, mcc_alpha, mcc_eth;
+    // null-collision MCC (mode 2): the species' largest speed at the end of the previous push
+    // ([0], float bits; 0 = none yet) and of the current one ([1], raised by the push)
+    unsigned* vmax;
 };
+
+// splitmix64's output mix (Steele, Lea and Flood, OOPSLA 2014), a bijection of 64-bit words.
+__host__ __device__ inline uint64_t mix64(uint64_t z)
+{
+    z ^= z >> 30;
+    z *= 0xBF58476D1CE4E5B9ull;
+    z ^= z >> 27;
+    z *= 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    return z;
+}
+
+// A (0,1) double with 53-bit resolution for (seed; id, step): the null-collision selection
+// draw, a counter-based stream distinct from the Philox streams (one multiply-mix chain
+// instead of ten Philox rounds, since every particle draws it every step).
+__host__ __device__ inline double select_uniform(uint64_t seed, uint32_t id, uint32_t step)
+{
+    const uint64_t key = ((uint64_t)step << 32) | (uint64_t)id;
+    const uint64_t z = mix64(mix64(seed ^ 0x5CDA7B2005CDA7B2ull) + key * 0x9E3779B97F4A7C15ull);
+    return ((double)(z >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+}
 
 struct PushParams {
     double dt;

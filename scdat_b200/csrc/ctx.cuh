@@ -140,6 +140,7 @@ struct scdat_ctx {
     DBuf<double> rho, phi, E, tmp_rho;
     DBuf<float> Ef;
     DBuf<unsigned long long> acc_l0, acc_l1, acc_h, totq;
+    DBuf<unsigned> vmax;  // [2 per species]: maximum speed of the previous / current push (float bits)
     // particles
     std::vector<SpeciesState> species;
     DBuf<int64_t> counts;

@@ -330,37 +330,62 @@ __device__ inline double sigma_elastic(const SpeciesDev& S, double e_ev)
 
 // MonteCarloCollisionHandler::processCollisions for one elastic process
 // (CollisionAlgorithm.cpp:500-538, 189-210) with Philox streams (seed; id, step, 2|3).
+// mode 0: the reference's two draws against p = nu dt; mode 1: one draw against
+// 1 - exp(-nu dt); mode 2: null collision (below).
 __device__ inline bool mcc_elastic(const SpeciesDev& S, const PushParams& pp, uint32_t pid, double& vx, double& vy,
                                    double& vz)
 {
     const double qe = 1.602176634e-19;
-    double speed = sqrt(vx * vx + vy * vy + vz * vz);
-    double e_ev = 0.5 * S.m * speed * speed / qe;
-    double nu = S.mcc_n * sigma_elastic(S, e_ev) * speed;
-    double u0, u1;
-    uniform2(pp.seed, pid, pp.step, 2u, u0, u1);
+    const double v2 = vx * vx + vy * vy + vz * vz;
     bool hit;
-    if (S.mcc_mode == 0) {
-        double p = fmin(fmax(nu * pp.dt, 0.0), 1.0);
-        hit = (u0 < p) && !(u1 >= p);
-    } else {
-        // p = 1 - exp(-x) <= x, and the computed p exceeds x by at most 2^-52 (exp within one
-        // ulp near 1, the subtraction exact), so u0 >= x + 1e-15 already decides "no hit"
-        // without the exponential; otherwise p is evaluated as before
-        const double x = nu * pp.dt;
-        if (u0 >= x + 1e-15) {
-            hit = false;
+    double speed;
+    if (S.mcc_mode == 2) {
+        // null collision: with nu_max = n sigma_max vmax (sigma <= sigma_max and speed <= vmax
+        // for every particle on this path), select with P = 1 - exp(-nu_max dt) by the cheap
+        // selection draw, then collide with probability nu / nu_max on the Philox stream.  A
+        // particle faster than vmax (and every particle before the first push has set vmax)
+        // takes the direct draw of mode 1.
+        const double vm = S.vmax ? (double)__uint_as_float(__ldg(S.vmax)) : 0.0;
+        double u0, u1;
+        if (vm > 0.0 && v2 <= vm * vm) {
+            const double numax = S.mcc_n * S.mcc_sigma * vm;
+            const double xmax = numax * pp.dt;
+            const double us = select_uniform(pp.seed, pid, pp.step);
+            // 1 - exp(-x) <= x, and the computed value exceeds x by at most 2^-52
+            if (us >= xmax + 1e-15 || !(us < 1.0 - exp(-xmax))) return false;
+            speed = sqrt(v2);
+            const double nu = S.mcc_n * sigma_elastic(S, 0.5 * S.m * speed * speed / qe) * speed;
+            uniform2(pp.seed, pid, pp.step, 2u, u0, u1);
+            hit = u0 * numax < nu;
         } else {
-            double p = 1.0 - exp(-x);
-            hit = u0 < p;
+            speed = sqrt(v2);
+            const double nu = S.mcc_n * sigma_elastic(S, 0.5 * S.m * speed * speed / qe) * speed;
+            uniform2(pp.seed, pid, pp.step, 2u, u0, u1);
+            const double x = nu * pp.dt;
+            hit = !(u0 >= x + 1e-15) && u0 < 1.0 - exp(-x);
+        }
+    } else {
+        speed = sqrt(v2);
+        const double nu = S.mcc_n * sigma_elastic(S, 0.5 * S.m * speed * speed / qe) * speed;
+        double u0, u1;
+        uniform2(pp.seed, pid, pp.step, 2u, u0, u1);
+        if (S.mcc_mode == 0) {
+            const double p = fmin(fmax(nu * pp.dt, 0.0), 1.0);
+            hit = (u0 < p) && !(u1 >= p);
+        } else {
+            // p = 1 - exp(-x) <= x, and the computed p exceeds x by at most 2^-52 (exp within one
+            // ulp near 1, the subtraction exact), so u0 >= x + 1e-15 already decides "no hit"
+            // without the exponential; otherwise p is evaluated as before
+            const double x = nu * pp.dt;
+            hit = (u0 >= x + 1e-15) ? false : (u0 < 1.0 - exp(-x));
         }
     }
     if (!hit) return false;
     double w0, w1;
     uniform2(pp.seed, pid, pp.step, 3u, w0, w1);
-    double theta = acos(-1.0 + 2.0 * w0);
-    double phi = 6.283185307179586476925286766559 * w1;
-    double st = sin(theta);
+    const double theta = acos(-1.0 + 2.0 * w0);
+    const double phi = 6.283185307179586476925286766559 * w1;
+    const double st = sin(theta);
     vx = speed * st * cos(phi);
     vy = speed * st * sin(phi);
     vz = speed * cos(theta);
@@ -392,6 +417,7 @@ enum { kDone = 0, kCapped = 1, kLost = 2 };
 struct PushStats {
     double ke;
     unsigned nsub, ev;
+    float v2;  // largest squared speed of the chunk's particles still active after their push
 };
 enum : unsigned { kEvLost = 1u, kEvActive = 2u, kEvHit = 4u };
 
@@ -404,6 +430,7 @@ constexpr double kKeUnit = 8.673617379884035e-19;     // 2^-60
 struct WarpStats {
     Fx128 ke;
     unsigned long long n[4];
+    unsigned v2max;  // float bits of the largest squared speed (non-negative floats order as integers)
 };
 
 __device__ __forceinline__ WarpStats& warp_slot()
@@ -415,7 +442,7 @@ __device__ __forceinline__ WarpStats& warp_slot()
 // start of a push kernel; every lane calls it
 __device__ __forceinline__ void warp_stats_begin()
 {
-    if ((threadIdx.x & 31) == 0) warp_slot() = WarpStats{Fx128{0ull, 0ll}, {0ull, 0ull, 0ull, 0ull}};
+    if ((threadIdx.x & 31) == 0) warp_slot() = WarpStats{Fx128{0ull, 0ll}, {0ull, 0ull, 0ull, 0ull}, 0u};
     __syncwarp();
 }
 
@@ -437,6 +464,7 @@ __device__ __forceinline__ void warp_chunk_end(PushStats& c)
     const unsigned lost = __popc(__ballot_sync(0xffffffffu, c.ev & kEvLost));
     const unsigned hit = __popc(__ballot_sync(0xffffffffu, c.ev & kEvHit));
     const unsigned act = __popc(__ballot_sync(0xffffffffu, c.ev & kEvActive));
+    const unsigned v2 = __reduce_max_sync(0xffffffffu, __float_as_uint(c.v2));
     if ((threadIdx.x & 31) == 0) {
         WarpStats& w = warp_slot();
         fx_add(w.ke, Fx128{lo, hi});
@@ -444,14 +472,17 @@ __device__ __forceinline__ void warp_chunk_end(PushStats& c)
         w.n[1] += lost;
         w.n[2] += hit;
         w.n[3] += act;
+        w.v2max = max(w.v2max, v2);
     }
-    c = PushStats{0.0, 0u, 0u};
+    c = PushStats{0.0, 0u, 0u, 0.0f};
 }
 
 // Flush the warp's totals into a ledger and its kinetic-energy accumulator (lo, hi words);
 // every lane calls it, after warp_chunk_end.  Integer sums only, so the totals do not depend
 // on the schedule.
-__device__ __forceinline__ void warp_stats_flush(LedgerDev* L, unsigned long long* ke_acc)
+// vmax: the species' maximum-speed slots (SpeciesDev::vmax, may be null); the current push's
+// slot [1] is raised to the warp's largest speed.
+__device__ __forceinline__ void warp_stats_flush(LedgerDev* L, unsigned long long* ke_acc, unsigned* vmax = nullptr)
 {
     if ((threadIdx.x & 31) == 0) {
         WarpStats& w = warp_slot();
@@ -460,7 +491,8 @@ __device__ __forceinline__ void warp_stats_flush(LedgerDev* L, unsigned long lon
         if (w.n[2]) atomicAdd(&L->mcc_hits, w.n[2]);
         if (w.n[3]) atomicAdd(&L->active, w.n[3]);
         fx_atomic_add(ke_acc, ke_acc + 1, w.ke);
-        w = WarpStats{Fx128{0ull, 0ll}, {0ull, 0ull, 0ull, 0ull}};
+        if (vmax && w.v2max) atomicMax(vmax + 1, __float_as_uint(sqrtf(__uint_as_float(w.v2max))));
+        w = WarpStats{Fx128{0ull, 0ll}, {0ull, 0ull, 0ull, 0ull}, 0u};
     }
     __syncwarp();
 }

@@ -180,6 +180,7 @@ __device__ __forceinline__ void finish_d(const MeshView& M, const ParticleStore&
     c.ke += ke;  // updateStatistics counts every stored particle (PICCycle.cpp:941-966)
     if (tet_out >= 0) {
         c.ev |= kEvActive;
+        if (S.mcc_mode == 2) c.v2 = fmaxf(c.v2, (float)(f.vx * f.vx + f.vy * f.vy + f.vz * f.vz));  // the null-collision speed bound
         if (pp.do_mcc && S.mcc_enabled && mcc_elastic(S, pp, P.id[i], f.vx, f.vy, f.vz)) c.ev |= kEvHit;
     }
     P.x[i] = f.px; P.y[i] = f.py; P.z[i] = f.pz;
@@ -247,7 +248,7 @@ __global__ void __launch_bounds__(256) k_push_f64(const __grid_constant__ MeshVi
             warp_chunk_end(c);
         }
     }
-    warp_stats_flush(L, ke_acc);
+    warp_stats_flush(L, ke_acc, S.vmax);
 }
 
 // Passes 2 and 3 over a deferred list (see k_push_mixed_more).
@@ -287,7 +288,7 @@ __global__ void __launch_bounds__(256) k_push_f64_more(const __grid_constant__ M
         }
         warp_chunk_end(c);
     }
-    warp_stats_flush(L, ke_acc);
+    warp_stats_flush(L, ke_acc, S.vmax);
 }
 
 // Standalone MCC pass (executeBackgroundMccStep, CollisionPicAdapter.cpp:338-434).

@@ -329,6 +329,7 @@ __device__ __forceinline__ void finish_f(const MeshView& M, const ParticleStore&
     c.ke += ke;
     if (tet_out >= 0) {
         c.ev |= kEvActive;
+        if (S.mcc_mode == 2) c.v2 = fmaxf(c.v2, (float)(dvx * dvx + dvy * dvy + dvz * dvz));  // the null-collision speed bound
         if (pp.do_mcc && S.mcc_enabled && mcc_elastic(S, pp, P.id[i], dvx, dvy, dvz)) {
             c.ev |= kEvHit;
             f.vx = (float)dvx; f.vy = (float)dvy; f.vz = (float)dvz;
@@ -557,7 +558,7 @@ __global__ void __launch_bounds__(256, 6) k_push_mixed(const __grid_constant__ M
         for (int64_t base = b0; base < b0 + 32 * kRun && base < n; base += 32)
             push1_warp(M, P, S, pp, D, A, L, base, n, c);
     }
-    warp_stats_flush(L, ke_acc);
+    warp_stats_flush(L, ke_acc, S.vmax);
 }
 
 // Stay-first pass 1 (same work distribution as k_push_mixed); no walk code, so it needs far
@@ -578,7 +579,7 @@ __global__ void __launch_bounds__(256, 6) k_push_mixed_stay(const __grid_constan
         for (int64_t base = b0; base < b0 + 32 * kRun && base < n; base += 32)
             push1_stay_warp(M, P, S, pp, D, A, L, base, n, c);
     }
-    warp_stats_flush(L, ke_acc);
+    warp_stats_flush(L, ke_acc, S.vmax);
 }
 
 // Passes 2 and 3.
@@ -596,7 +597,7 @@ __global__ void __launch_bounds__(256, 4) k_push_mixed_more(const __grid_constan
         if (base >= n) break;
         push_more_warp(M, P, S, pp, Din, Dout, cap, A, L, base, n, c);
     }
-    warp_stats_flush(L, ke_acc);
+    warp_stats_flush(L, ke_acc, S.vmax);
 }
 
 // ---- batched step: all (scenario, species) jobs in one launch per pass -----------------
@@ -655,7 +656,7 @@ __global__ void __launch_bounds__(256, 4) k_push_mixed_batch(const PushJob* __re
                 hi = mid;
         }
         if (lo != cur) {
-            if (cur >= 0) warp_stats_flush(jobs[cur].L, jobs[cur].ke_acc);
+            if (cur >= 0) warp_stats_flush(jobs[cur].L, jobs[cur].ke_acc, jobs[cur].S.vmax);
             cur = lo;
         }
         const PushJob& J = jobs[cur];
@@ -674,7 +675,7 @@ __global__ void __launch_bounds__(256, 4) k_push_mixed_batch(const PushJob* __re
             push_more_warp(J.M, J.P, J.S, J.pp, J.D2, DeferList{}, 0, J.A, J.L, base, n, c);
         }
     }
-    if (cur >= 0) warp_stats_flush(jobs[cur].L, jobs[cur].ke_acc);
+    if (cur >= 0) warp_stats_flush(jobs[cur].L, jobs[cur].ke_acc, jobs[cur].S.vmax);
 }
 
 // nodal E -> tet records of every scenario (tets block map)

@@ -104,6 +104,18 @@ __global__ void k_scatter_values(int64_t n, const int64_t* __restrict__ idx, con
         dst[idx[i]] = v[i];
 }
 
+// Start of a push: each species' maximum speed of the previous push becomes the one the
+// null-collision MCC uses ([2s] <- [2s+1]), and the current slot starts from zero.
+__global__ void k_rotate_vmax(int S, unsigned* v)
+{
+    for (int s = threadIdx.x; s < S; s += blockDim.x) {
+        v[2 * s] = v[2 * s + 1];
+        v[2 * s + 1] = 0u;
+    }
+}
+
+void launch_rotate_vmax(int S, unsigned* v, cudaStream_t st) { k_rotate_vmax<<<1, 32, 0, st>>>(S, v); }
+
 void launch_scatter_values(int64_t n, const int64_t* idx, const double* v, double* dst, cudaStream_t st)
 {
     int grid = (int)std::min<int64_t>((n + 255) / 256, 148 * 8);

@@ -55,24 +55,28 @@ def oracle_cycle(o, mesh, sp, parts, nsteps, dt, face_bc, phi0, neighbors=True, 
     return dict(st, rho=rho, phi=phi, E=E, ledger=ledger, surface_charge=sc, substeps=substeps)
 
 
-def oracle_mcc_run(o, mesh, sp, parts, nsteps, dt, face_bc, n_t, sigma, seed, rtol=1e-15):
+def oracle_mcc_run(o, mesh, sp, parts, nsteps, dt, face_bc, n_t, sigma, seed, rtol=1e-15, mode=0):
     """The oracle's PIC-MCC run in the reference's order: each step the cycle (push, boundary
     events, field), then elastic MCC on the Philox streams of (seed, particle id, step), then
     the absorbed particles leave the container (Collision::executeBackgroundMccStep,
-    CollisionPicAdapter.cpp:338-434).  Returns the active particles, the summed ledger, the
-    collisions and the last fields."""
+    CollisionPicAdapter.cpp:338-434).  Mode 2 (null collision) takes each species' speed bound
+    from the previous push, as the device does.  Returns the active particles, the summed
+    ledger, the collisions and the last fields."""
     procs = [O.Elastic(n_t, sigma, 1.0, 0.0, 0.0, 1, 0) for _ in sp]
     cur = {k: v.copy() for k, v in parts.items()}
     phi, ledger, hits = mesh.phi_bc.copy(), np.zeros((7, 8)), 0
     out = None
+    vmax = None
     for k in range(nsteps):
         out = oracle_cycle(o, mesh, sp, cur, 1, dt, face_bc, phi, rtol=rtol)
         ledger += out["ledger"]
         phi = out["phi"]
         v = out["v"]
         if n_t > 0:
-            v, h = o.mcc(out["v"], cur["species"], out["status"], cur["id"], sp, procs, dt, seed, k, mode=0)
+            v, h = o.mcc(out["v"], cur["species"], out["status"], cur["id"], sp, procs, dt, seed, k, mode=mode,
+                         vmax=vmax)
             hits += h
+        vmax = O.push_speed_bound(out["v"], cur["species"], out["status"], len(sp))
         act = out["status"] == O.ACTIVE
         cur = {key: val[act] for key, val in cur.items()}
         cur.update(x=out["x"][act], v=v[act], tet=out["tet"][act])

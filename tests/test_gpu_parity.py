@@ -142,7 +142,8 @@ def test_mcc_matches_oracle_streams(lib, orc, mode):
     dom.close()
 
 
-def test_full_mcc_run_matches_oracle(lib, orc):
+@pytest.mark.parametrize("mode", [0, 2])
+def test_full_mcc_run_matches_oracle(lib, orc, mode):
     """Several full steps with elastic MCC (fused into the push) against the oracle's run in the
     reference's order (cycle, then MCC, then inactive particles dropped) on the same Philox
     streams: the same collisions, statuses and ledger counts, and states, fields and ledger
@@ -154,11 +155,11 @@ def test_full_mcc_run_matches_oracle(lib, orc):
     vth = np.sqrt(O.QE / O.ME)
     parts["v"][parts["species"] == 0, 0] += 2.0 * vth  # drift into the +x face
     dt, n_t, sigma, seed, nsteps, face_bc = 2e-8, 4e20, 1e-19, 777, 4, (1,) * 6
-    ref = oracle_mcc_run(orc, mesh, sp, parts, nsteps, dt, face_bc, n_t, sigma, seed)
+    ref = oracle_mcc_run(orc, mesh, sp, parts, nsteps, dt, face_bc, n_t, sigma, seed, mode=mode)
     dom = gpu_domain(mesh, dt, face_bc=face_bc, pcg_rtol=1e-15, pcg_max_iter=20000, body_tally=False, seed=seed)
     gpu_load_particles(dom, sp, parts)
     for s in range(len(sp)):
-        dom.set_elastic(s, n_t, sigma, mode=0)
+        dom.set_elastic(s, n_t, sigma, mode=mode)
     dom.set_potential(mesh.phi_bc)
     dom.step(nsteps)
     st = gpu_state(dom, len(sp), len(parts["tet"]))

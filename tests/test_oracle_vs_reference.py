@@ -256,3 +256,37 @@ def test_whipple_yield_matches_reference(ref):
             bar = np.maximum(1e-12, 1e-15 / np.maximum(q * q / 2.0, 1e-300))
             assert np.all(np.abs(mine - theirs) <= bar * np.abs(theirs)), (peak_yield, peak_e)
             assert np.all(bar[e >= 0.1 * max(1.0, peak_e)] < 1e-12 * 1.5)  # the plain bar above 0.1 Emax
+
+
+def test_null_collision_law(orc):
+    """Null-collision MCC (mode 2) against the direct draw (mode 1) on 400k Maxwellian
+    electrons at nu dt ~ 1e-2: each mode's collision count within 5 sigma of its own expected
+    value (sum of the per-particle probabilities: 1 - exp(-nu dt), and
+    (1 - exp(-nu_max dt)) nu / nu_max), the two laws equal to first order in nu dt, speeds kept;
+    particles faster than the bound take the direct draw."""
+    rng = np.random.default_rng(8)
+    n = 400_000
+    sp = [O.Species(-O.QE, O.ME, 1.0, 0, 1.0)]
+    v = rng.normal(0.0, np.sqrt(O.QE / O.ME), (n, 3))
+    spd = np.linalg.norm(v, axis=1)
+    idx = np.zeros(n, np.int32)
+    status = np.zeros(n, np.uint8)
+    ids = np.arange(n, dtype=np.int64)
+    n_t, sigma, dt = 4e19, 1e-19, 4e-9
+    proc = [O.Elastic(n_t, sigma, 1.0, 0.0, 0.0, 1, 0)]
+    nu = n_t * sigma * spd
+    for vbound in (spd.max(), np.quantile(spd, 0.9)):
+        numax = n_t * sigma * vbound
+        slow = spd <= vbound
+        p2 = np.where(slow, (1.0 - np.exp(-numax * dt)) * nu / numax, 1.0 - np.exp(-nu * dt))
+        p1 = 1.0 - np.exp(-nu * dt)
+        for mode, p in ((1, p1), (2, p2)):
+            v2, hits = orc.mcc(v, idx, status, ids, sp, proc, dt, 77, 3, mode=mode, vmax=np.array([vbound]))
+            mu, sd = p.sum(), np.sqrt((p * (1 - p)).sum())
+            assert abs(hits - mu) < 5 * sd, (mode, vbound, hits, mu, sd)
+            np.testing.assert_allclose(np.linalg.norm(v2, axis=1), spd, rtol=1e-12)
+            assert np.count_nonzero(np.any(v2 != v, axis=1)) == hits
+        assert abs(p2.sum() - p1.sum()) < 0.02 * p1.sum()  # same law to O(nu dt)
+    # the two modes draw from different streams, so their collision sets differ
+    _, h1 = orc.mcc(v, idx, status, ids, sp, proc, dt, 77, 3, mode=1)
+    assert h1 > 1000
