@@ -187,13 +187,33 @@ __device__ __forceinline__ void deposit_traj_f(const MeshView& M, const SpeciesD
                 }
             }
         } else {
-            for (int sg = 0; sg < nseg; ++sg) {
-                float tau = ((float)sg + 0.5f) / (float)nseg;
-                float lq[4] = {ls[0] + tau * dl[0], ls[1] + tau * dl[1], ls[2] + tau * dl[2], ls[3] + tau * dl[3]};
-                if (inside_f(lq)) {
-                    for (int k = 0; k < 4; ++k) sum[k] += lq[k];
-                    any = true;
+            // The segment cloud's points tau_k = (k + 1/2) / nseg lie on a line, and
+            // lambda_i(tau) = ls_i + tau dl_i is affine, so the points inside the tet (every
+            // lambda_i in [-1e-8, 1 + 1e-8]) are those with tau in one interval [lo, hi]: their
+            // count n and the sum of their lambdas, n ls + (sum of their tau) dl, follow in closed
+            // form instead of point by point.
+            const float e = 1e-8f;
+            float lo = 0.0f, hi = 1.0f;
+            bool empty = false;
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                if (dl[i] != 0.0f) {
+                    const float inv = 1.0f / dl[i];
+                    const float a = (-e - ls[i]) * inv, b = (1.0f + e - ls[i]) * inv;
+                    lo = fmaxf(lo, fminf(a, b));
+                    hi = fminf(hi, fmaxf(a, b));
+                } else if (!(ls[i] >= -e && ls[i] <= 1.0f + e)) {
+                    empty = true;
                 }
+            }
+            const int ka = max(0, (int)ceilf(lo * (float)nseg - 0.5f));
+            const int kb = min(nseg - 1, (int)floorf(hi * (float)nseg - 0.5f));
+            if (!empty && kb >= ka) {
+                const float n = (float)(kb - ka + 1);
+                const float st = 0.5f * n * (float)(ka + kb + 1) / (float)nseg;
+#pragma unroll
+                for (int k = 0; k < 4; ++k) sum[k] = n * ls[k] + st * dl[k];
+                any = true;
             }
         }
     }
