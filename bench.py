@@ -53,7 +53,29 @@ CONFIGS = {
     "surface256": dict(cells=(256, 256, 128), body=((112, 144), (112, 144), (56, 72)), ppc=16, density=1e9, te=5.0,
                        ti=5.0, precision=1, rtol=1e-10, sort_interval=4, ion_sort_interval=16, eps_r=3.0,
                        thickness=1e-3),
+    # the large surface-charging run's plasma and dielectric faces on a quarter-size box, run for
+    # thousands of steps: the floating-potential error of the mixed form against FP64
+    "surface_long": dict(cells=(64, 64, 32), body=((28, 36), (28, 36), (14, 18)), ppc=16, density=1e9, te=5.0,
+                         ti=5.0, precision=1, rtol=1e-10, sort_interval=4, ion_sort_interval=16, eps_r=3.0,
+                         thickness=1e-3),
 }
+
+
+def round_velocities_fp32(dom):
+    """Round every particle velocity to FP32, as the precision form stores them: a perturbation
+    of all particles at the level of the precision form's initial rounding, run in FP64."""
+    for s in range(dom.nspecies):
+        p = dom.get_particles(s)
+        dom.set_particles(s, p["x"], p["v"].astype(np.float32).astype(np.float64), p["tet"], p["id"])
+
+
+def nudge_one_velocity(dom, s=0):
+    """Move one particle's x-velocity by one ulp (FP64) -- a perturbation at the level of the
+    arithmetic's own rounding, to measure how far two runs of one form drift apart."""
+    p = dom.get_particles(s)
+    v = p["v"].copy()
+    v[0, 0] = np.nextafter(v[0, 0], np.inf)
+    dom.set_particles(s, p["x"], v, p["tet"], p["id"])
 EPS0 = 8.8541878128e-12
 
 
@@ -196,9 +218,11 @@ def alg_bytes_push(dom, precision, particles):
     return particles * b_p + dom.T * t_b + dom.N * n_b
 
 
-# DRAM bytes per stored particle of one step's push launches (all passes, both species), from
-# an ncu capture of the push scaled per particle; None: not measured for the form.
-PUSH_DRAM_BYTES_PER_PARTICLE = {1: 339.2, 0: None}
+# DRAM bytes per stored particle of one step's push launches (all passes, both species): an ncu
+# capture (dram__bytes_read.sum + dram__bytes_write.sum) of one step's six push launches on a
+# 64^3-cell box at 64 ppc per species (31.9 M particles, 6.15 GB), divided by the particles; the
+# full workload has the same density and access pattern.  None: not measured for the form.
+PUSH_DRAM_BYTES_PER_PARTICLE = {1: 193.0, 0: None}
 
 
 def cg_iteration_bytes(dom, precision):
@@ -521,6 +545,19 @@ def run_batched(args, cfg):
     errs = []
     for d, p64 in zip(doms, phi64):
         errs.append(float(np.abs(d.fields()[1] - p64).max() / max(np.abs(p64).max(), 1e-300)))
+    # the worst scenario's FP64 form against itself with one velocity moved by one ulp, over the
+    # same steps: how far two FP64 runs drift apart on their own
+    # and against itself started from FP32-rounded velocities (the precision form's initial
+    # rounding, FP64 arithmetic after it)
+    kw = int(np.argmax(errs))
+    worst = dict(index=kw, error=errs[kw], scenario={k: scen[kw][k] for k in ("n", "bias", "density", "te", "ti", "ppc")})
+    for name, perturb in (("fp64_vs_fp64_nudged", nudge_one_velocity), ("fp64_vs_fp64_v32", round_velocities_fp32)):
+        cdom, _ = build_domain(scen[kw], 0, capi)
+        perturb(cdom)
+        for _ in range(total):
+            cdom.step(1)
+        worst[name] = float(np.abs(cdom.fields()[1] - phi64[kw]).max() / max(np.abs(phi64[kw]).max(), 1e-300))
+        cdom.close()
     parts = int(sum(d.count(s) for d in doms for s in range(d.nspecies)))
     # end to end through the C ABI with host buffers: per step, each scenario's Dirichlet
     # potentials in from pinned memory, the potentials and statistics back
@@ -566,7 +603,8 @@ def run_batched(args, cfg):
                    "l2": "inputs larger than L2 (particle state > 126 MB)", "parallelism": f"replicas x{world}"},
         "fp64_form": {"value": fp64_ps / (fp64_ms / 1e3), "unit": "particle-steps/s", "steps": args.steps,
                       "ms_per_step": fp64_ms / args.steps, "note": "plain FP64 form, scenarios one at a time"},
-        "phi_rel_err_vs_fp64": {"max": max(errs), "median": float(np.median(errs)), "after_steps": total},
+        "phi_rel_err_vs_fp64": {"max": max(errs), "median": float(np.median(errs)), "after_steps": total,
+                                "per_scenario": errs, "worst": worst},
         "gpu_launches": int(launches),
         "clocks": clk,
         "e2e": {"value": e2e_val, "unit": "particle-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
@@ -578,7 +616,7 @@ def run_batched(args, cfg):
         print(json.dumps(out))
 
 
-def build_surface_domain(cfg, precision, capi):
+def build_surface_domain(cfg, precision, capi, seed=4242):
     nx, ny, nz = cfg["cells"]
     h = float(np.sqrt(EPS0 * cfg["te"] / (cfg["density"] * QE)))
     dt = 0.1 / float(np.sqrt(cfg["density"] * QE * QE / (EPS0 * ME)))
@@ -593,8 +631,8 @@ def build_surface_domain(cfg, precision, capi):
 
     w = cfg["density"] * h ** 3 / cfg["ppc"]
     dom.set_species([Sp(-QE, ME, w), Sp(QE, MP, w)])
-    dom.seed_box(0, (nx, ny, nz), h, body, cfg["ppc"], cfg["te"], 4242)
-    dom.seed_box(1, (nx, ny, nz), h, body, cfg["ppc"], cfg["ti"], 4242)
+    dom.seed_box(0, (nx, ny, nz), h, body, cfg["ppc"], cfg["te"], seed)
+    dom.seed_box(1, (nx, ny, nz), h, body, cfg["ppc"], cfg["ti"], seed)
     if cfg.get("ion_sort_interval"):
         dom.set_species_sort_interval(1, cfg["ion_sort_interval"])
     dom.set_potential(m["phi"])
@@ -624,11 +662,23 @@ def run_surface(args, cfg):
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=900))
     res = {}
     clk = None
-    for prec in (0, 1):
-        dom, dt = build_surface_domain(cfg, prec, capi)
+    long_run = args.config == "surface_long"
+    every = max(1, (args.warmup + args.steps) // 20)  # face-potential samples of the long run
+    # (precision, control): the long run adds the FP64 form against itself with one velocity
+    # nudged by an ulp, started from FP32-rounded velocities, and from an independent seed
+    runs = [(0, None), (1, None)] + ([(0, "nudged"), (0, "v32"), (0, "seed")] if long_run else [])
+    for prec, nudged in runs:
+        dom, dt = build_surface_domain(cfg, prec, capi, seed=4243 if nudged == "seed" else 4242)
+        if nudged == "nudged":
+            nudge_one_velocity(dom)
+        elif nudged == "v32":
+            round_velocities_fp32(dom)
         stream = torch.cuda.ExternalStream(dom.stream())
-        for _ in range(args.warmup):
+        series = []
+        for k in range(args.warmup):
             dom.step(1)
+            if long_run and (k + 1) % every == 0:
+                series.append(dom.surface_state()["V"].tolist())
         torch.cuda.synchronize()
         if prec == 1 and dist:
             dist.barrier()
@@ -638,36 +688,55 @@ def run_surface(args, cfg):
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ev0.record(stream)
         ps = 0
-        for _ in range(args.steps):
+        for k in range(args.steps):
             dom.step(1)
             ps += dom.stats()["active_particles"]
+            if long_run and (args.warmup + k + 1) % every == 0:
+                series.append(dom.surface_state()["V"].tolist())
         ev1.record(stream)
         torch.cuda.synchronize()
         if prec == 1:
             clk = clocks.stop()
         ms = ev0.elapsed_time(ev1)
         srf = dom.surface_state()
-        res[prec] = dict(ms=ms, ps=ps, V=srf["V"], Q=srf["Q"], particles=int(sum(dom.count(s) for s in range(2))),
-                         tets=dom.T, dt=dt, collected=int(np.asarray(srf["counts"]).sum()))
+        res[(prec, nudged)] = dict(ms=ms, ps=ps, V=srf["V"], Q=srf["Q"], series=series,
+                                   particles=int(sum(dom.count(s) for s in range(2))), tets=dom.T, dt=dt,
+                                   collected=int(np.asarray(srf["counts"]).sum()))
         dom.close()
-    v64, v32 = res[0]["V"], res[1]["V"]
-    err = float(np.abs(v32 - v64).max() / max(np.abs(v64).max(), 1e-300))
-    t_local = res[1]["ms"] / 1e3
-    t_max, total_ps = reduce_over_ranks(dist, t_local, res[1]["ps"])
+
+    def rel(a, b):
+        a, b = np.asarray(a), np.asarray(b)
+        return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+    r64, r32 = res[(0, None)], res[(1, None)]
+    v64, v32 = r64["V"], r32["V"]
+    err = rel(v32, v64)
+    t_local = r32["ms"] / 1e3
+    t_max, total_ps = reduce_over_ranks(dist, t_local, r32["ps"])
+    fp = {"mixed_V": v32.tolist(), "fp64_V": v64.tolist(), "rel_err_vs_fp64": err,
+          "after_steps": args.warmup + args.steps,
+          "particles_collected": {"mixed": r32["collected"], "fp64": r64["collected"]}}
+    if long_run:
+        fp["series_every_steps"] = every
+        fp["series_rel_err_vs_fp64"] = [rel(a, b) for a, b in zip(r32["series"], r64["series"])]
+        for ctl in ("nudged", "v32", "seed"):
+            rn = res[(0, ctl)]
+            fp[f"fp64_{ctl}_vs_fp64"] = rel(rn["V"], v64)
+            fp["particles_collected"][f"fp64_{ctl}"] = rn["collected"]
+            fp[f"series_fp64_{ctl}_vs_fp64"] = [rel(a, b) for a, b in zip(rn["series"], r64["series"])]
+        fp["series_fp64_mean_V"] = [float(np.mean(b)) for b in r64["series"]]
     out = {
         "metric": "PIC particle-steps/s on 1 B200 (mixed/batched vs plain FP64 at equal error)",
         "value": total_ps / t_max, "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_max * 1e3 / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded, no dataset)",
-        "config": {"workload": "surface256", "cells": list(cfg["cells"]), "tets": res[1]["tets"],
-                   "particles": res[1]["particles"], "dt": res[1]["dt"], "precision": "mixed",
+        "config": {"workload": args.config, "cells": list(cfg["cells"]), "tets": r32["tets"],
+                   "particles": r32["particles"], "dt": r32["dt"], "precision": "mixed",
                    "surface": "6 floating dielectric faces (eps_r 3, 1 mm), FP64 charge and potential",
                    "l2": "inputs larger than L2 (particle state > 126 MB)", "parallelism": f"replicas x{world}"},
-        "fp64_form": {"value": res[0]["ps"] / (res[0]["ms"] / 1e3), "unit": "particle-steps/s",
-                      "ms_per_step": res[0]["ms"] / args.steps},
-        "floating_potential": {"mixed_V": v32.tolist(), "fp64_V": v64.tolist(), "rel_err_vs_fp64": err,
-                               "after_steps": args.warmup + args.steps,
-                               "particles_collected": {"mixed": res[1]["collected"], "fp64": res[0]["collected"]}},
+        "fp64_form": {"value": r64["ps"] / (r64["ms"] / 1e3), "unit": "particle-steps/s",
+                      "ms_per_step": r64["ms"] / args.steps},
+        "floating_potential": fp,
         "clocks": clk,
     }
     if dist:
@@ -819,7 +888,7 @@ def main():
     ap.add_argument("--no-graph-form", dest="graph_form", action="store_false")
     args = ap.parse_args()
     cfg = dict(CONFIGS[args.config])
-    if args.config in ("batched64", "surface256"):
+    if args.config in ("batched64", "surface256", "surface_long"):
         if args.impl == "reference":
             run_reference(args, dict(CONFIGS["precision128"]))
         elif args.config == "batched64":

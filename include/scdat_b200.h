@@ -350,11 +350,14 @@ SCDAT_API int scdat_batch_kernel_launches(scdat_batch* b, int64_t* launches);
 
 /* PicMccSurfaceCurrentSampler::sampleWithDerivative (Toolkit/Surface Charging/src/
  * PicMccSurfaceCurrentSampler.cpp:641-670): three contexts holding the same scenario (mesh,
- * species, particles, seed) run window_steps steps with the body nodes held at V - d, V and
+ * species, particles, seed) run window_steps steps with the surface nodes held at V - d, V and
  * V + d, d = max(0.1, |probe_delta_v|) as in the reference, as one batch when all three are
- * mixed-precision (one at a time otherwise).  Returns the centre window's collection current
- * densities (charge per second per area into the body: electrons negative, ions positive,
- * secondaries leaving positive) and the central difference of the net density over 2d. */
+ * mixed-precision (one at a time otherwise).  The collected charge is that of ledger row
+ * `ledger_row`: 0..5 a domain face XMin..ZMax (the reference samples its plate's ZMin face,
+ * PicMccSurfaceCurrentSampler.cpp:587-588), 6 the body box.  Returns the centre window's
+ * collection current densities (charge per second per area into the surface: electrons
+ * negative, ions positive, secondaries leaving positive) and the central difference of the net
+ * density over 2d. */
 typedef struct {
     double surface_potential_v;
     double electron_collection_a_per_m2;
@@ -365,9 +368,9 @@ typedef struct {
     int32_t valid;
     int32_t window_steps;
 } scdat_current_sample;
-SCDAT_API int scdat_sample_with_derivative(scdat_ctx* const* ctx3, int64_t n_body, const int64_t* body_nodes,
-                                           double surface_potential_v, double probe_delta_v, int32_t window_steps,
-                                           double area_m2, scdat_current_sample* out);
+SCDAT_API int scdat_sample_with_derivative(scdat_ctx* const* ctx3, int64_t n_surface, const int64_t* surface_nodes,
+                                           int32_t ledger_row, double surface_potential_v, double probe_delta_v,
+                                           int32_t window_steps, double area_m2, scdat_current_sample* out);
 
 /* ---- Adjoint window (no reference counterpart) ----
  * Runs `steps` FP64 steps from the current state (which must follow a scdat_solve_field; MCC

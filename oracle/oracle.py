@@ -479,6 +479,12 @@ class Reference:
         L.ref_parse_cross_section_set.restype = C.c_int
         L.ref_estimate_densities.argtypes = [C.c_int64, _i32p, _dp, _dp, _u8p, C.c_double, _dp, _dp]
         L.ref_estimate_densities.restype = None
+        L.ref_sampler_mesh.argtypes = [C.c_double, C.c_double, C.c_double, C.c_int, C.c_int64, _dp, C.c_int64, _i32p,
+                                       _i64p]
+        L.ref_sampler_mesh.restype = C.c_int
+        L.ref_sampler_sample.argtypes = [C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, C.c_uint] + \
+            [C.c_double] * 8 + [C.c_int, _dp]
+        L.ref_sampler_sample.restype = C.c_int
         self._meshes = {}
 
     def mesh(self, mesh: BoxMesh, neighbors=True):
@@ -599,6 +605,28 @@ class Reference:
         out = np.zeros(len(e))
         self.L.ref_whipple_yield(float(peak_yield), float(peak_energy_ev), len(e), e, out)
         return out
+
+    def sampler_mesh(self, area_m2, aspect, gap_m, z_layers):
+        """The surface current sampler's plate mesh (GeometryMeshGenerator, as createSamplingMesh
+        builds it for a sampler with no linked boundary faces): node coordinates and tets."""
+        cap = 100000
+        xyz = np.zeros((cap, 3))
+        tet = np.zeros((cap, 4), np.int32)
+        cnt = np.zeros(2, np.int64)
+        assert self.L.ref_sampler_mesh(float(area_m2), float(aspect), float(gap_m), int(z_layers), cap, xyz, cap, tet,
+                                       cnt) == 0
+        return xyz[:cnt[0]].copy(), tet[:cnt[1]].copy()
+
+    def sampler_sample(self, area_m2, gap_m, z_layers, ppe, window_steps, seed, ne, ni, te_ev, ti_ev, ion_amu,
+                       surface_v, reference_v, probe_dv, enable_mcc=False):
+        """PicMccSurfaceCurrentSampler::sampleWithDerivative: electron, ion, emitted and net
+        collection current densities [A/m^2], d(net)/dV, valid, deposition segments, seed used."""
+        out = np.zeros(8)
+        self.L.ref_sampler_sample(float(area_m2), float(gap_m), int(z_layers), int(ppe), int(window_steps), int(seed),
+                                  float(ne), float(ni), float(te_ev), float(ti_ev), float(ion_amu), float(surface_v),
+                                  float(reference_v), float(probe_dv), int(bool(enable_mcc)), out)
+        keys = ("electron", "ion", "emitted", "net", "derivative", "valid", "segments", "seed")
+        return dict(zip(keys, out))
 
     def parse_cross_section_set(self, text):
         """Collision::parseCollisionCrossSectionSetId: -1 unknown, else the set's index."""

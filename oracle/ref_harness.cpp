@@ -10,6 +10,8 @@
 //   Collision::executeBackgroundMccStep         Tools/Interactions/Collisions/include/CollisionPicAdapter.h:64-75
 //   SurfaceCircuitCoupling::advanceImplicit     Tools/Coupling/src/SurfaceCircuitCoupling.cpp:866-1126
 //   evaluateLegacySecondaryElectronYield        Tools/Material/src/SurfaceMaterialModel.cpp:620-636
+//   PicMccSurfaceCurrentSampler::sampleWithDerivative
+//                                               Toolkit/Surface Charging/src/PicMccSurfaceCurrentSampler.cpp:641-670
 // Only the parity tests and the CPU reference arm of the benchmark load it.
 #include "PICcore/include/PICCycle.h"
 #include "Mesh/include/MeshParsing.h"
@@ -18,8 +20,11 @@
 #include "Coupling/include/SurfaceCircuitCoupling.h"
 #include "Material/include/MaterialProperty.h"
 #include "Material/include/SurfaceMaterialModel.h"
+#include "PicMccSurfaceCurrentSampler.h"
 
+#include <algorithm>
 #include <chrono>
+#include <cmath>
 #include <cstdint>
 #ifdef USE_OPENMP
 #include <omp.h>
@@ -463,6 +468,81 @@ void ref_estimate_densities(int64_t n, const int32_t* type, const double* charge
     out3[0] = d.neutral_density_m3;
     out3[1] = d.ion_density_m3;
     out3[2] = d.electron_density_m3;
+}
+
+// The sampler's plate mesh for a sampler with no linked boundary faces: the options that
+// createSamplingMesh derives from its config (PicMccSurfaceCurrentSampler.cpp:195-245: length and
+// width from the area and aspect ratio, the gap as thickness, one cell across, max(4, z_layers)
+// layers) through the reference's own GeometryMeshGenerator.  counts = {nodes, tets}; returns 1
+// when a capacity is too small.
+int ref_sampler_mesh(double area_m2, double aspect, double gap_m, int z_layers, int64_t cap_nodes, double* xyz,
+                     int64_t cap_tets, int32_t* tet4, int64_t* counts)
+{
+    SM::GeometryDimensions dims;
+    dims.shape = SM::GeometryShape::PLATE;
+    const double ar = std::clamp(aspect, 0.25, 4.0);
+    const double a = std::max(1.0e-12, area_m2);
+    dims.length = std::sqrt(a * ar);
+    dims.width = std::sqrt(a / ar);
+    dims.thickness = std::max(1.0e-6, gap_m);
+    SM::MeshGenerationOptions opt;
+    opt.nx = 1;
+    opt.ny = std::max<std::size_t>(1, (std::size_t)std::ceil(1.0 / std::max(0.5, ar)));
+    opt.nz = std::max<std::size_t>(4, (std::size_t)std::max(0, z_layers));
+    opt.tetrahedralize = true;
+    auto mesh = SM::GeometryMeshGenerator::generateFromDimensions(dims, opt);
+    if (!mesh) return 2;
+    const auto& nodes = mesh->getNodes();
+    const auto& els = mesh->getElements();
+    counts[0] = (int64_t)nodes.size();
+    counts[1] = (int64_t)els.size();
+    if (counts[0] > cap_nodes || counts[1] > cap_tets) return 1;
+    for (std::size_t i = 0; i < nodes.size(); ++i) {
+        const auto p = nodes[i]->getPosition();
+        xyz[3 * i] = p.x(); xyz[3 * i + 1] = p.y(); xyz[3 * i + 2] = p.z();
+    }
+    for (std::size_t e = 0; e < els.size(); ++e) {
+        const auto& en = els[e]->getNodes();
+        if (en.size() != 4) return 3;
+        for (int k = 0; k < 4; ++k) tet4[4 * e + k] = (int32_t)en[k]->getId();
+    }
+    return 0;
+}
+
+// PicMccSurfaceCurrentSampler::sampleWithDerivative on a config with the given plate, plasma
+// (electron and ion densities and temperatures, ion mass), particles per element, window,
+// seed and potentials.  out = {electron, ion, emitted, net collection current densities,
+// d(net)/dV, valid, deposition segments, the seed the sampler used}.
+int ref_sampler_sample(double area_m2, double gap_m, int z_layers, int ppe, int window_steps, unsigned seed,
+                       double ne, double ni, double te_ev, double ti_ev, double ion_amu, double surface_v,
+                       double reference_v, double probe_dv, int enable_mcc, double* out)
+{
+    SCDAT::Toolkit::SurfaceCharging::PicMccSurfaceSamplerConfig c;
+    c.surface_area_m2 = area_m2;
+    c.gap_distance_m = gap_m;
+    c.z_layers = (std::size_t)std::max(0, z_layers);
+    c.particles_per_element = (std::size_t)std::max(1, ppe);
+    c.window_steps = (std::size_t)std::max(1, window_steps);
+    c.seed = seed;
+    c.plasma.electron_density_m3 = ne;
+    c.plasma.ion_density_m3 = ni;
+    c.plasma.electron_temperature_ev = te_ev;
+    c.plasma.ion_temperature_ev = ti_ev;
+    c.plasma.ion_mass_amu = ion_amu;
+    c.surface_potential_v = surface_v;
+    c.plasma_reference_potential_v = reference_v;
+    c.enable_mcc = enable_mcc != 0;
+    SCDAT::Toolkit::SurfaceCharging::PicMccSurfaceCurrentSampler sampler;
+    const auto r = sampler.sampleWithDerivative(c, probe_dv);
+    out[0] = r.electron_collection_current_density_a_per_m2;
+    out[1] = r.ion_collection_current_density_a_per_m2;
+    out[2] = r.emitted_electron_current_density_a_per_m2;
+    out[3] = r.net_collection_current_density_a_per_m2;
+    out[4] = r.current_derivative_a_per_m2_per_v;
+    out[5] = r.valid ? 1.0 : 0.0;
+    out[6] = (double)r.deposition_segments;
+    out[7] = (double)r.seed_used;
+    return r.valid ? 0 : 1;
 }
 
 }  // extern "C"

@@ -141,8 +141,8 @@ def load():
     L.scdat_export_layer_profile_csv.argtypes = [vp, C.c_char_p, C.c_int32]
     L.scdat_export_nodes_csv.argtypes = [vp, C.c_char_p]
     L.scdat_adjoint_window.argtypes = [vp, C.POINTER(AdjointRequestC), C.POINTER(AdjointResultC)]
-    L.scdat_sample_with_derivative.argtypes = [C.POINTER(vp), C.c_int64, vp, C.c_double, C.c_double, C.c_int32,
-                                               C.c_double, C.POINTER(CurrentSampleC)]
+    L.scdat_sample_with_derivative.argtypes = [C.POINTER(vp), C.c_int64, vp, C.c_int32, C.c_double, C.c_double,
+                                               C.c_int32, C.c_double, C.POINTER(CurrentSampleC)]
     L.scdat_batch_kernel_launches.argtypes = [vp, C.POINTER(C.c_int64)]
     L.scdat_set_particles.argtypes = [vp, C.c_int32, C.c_int64, vp, vp, vp, vp]
     L.scdat_seed_box_particles.argtypes = [vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_double, vp, vp,
@@ -562,13 +562,18 @@ class Batch:
             pass
 
 
-def sample_with_derivative(domains, body_nodes, surface_potential_v, probe_delta_v, window_steps, area_m2):
-    """scdat_sample_with_derivative over three Domains holding the same scenario."""
+LEDGER_BODY = 6  # ledger rows 0..5 are the domain faces XMin..ZMax
+
+
+def sample_with_derivative(domains, surface_nodes, surface_potential_v, probe_delta_v, window_steps, area_m2,
+                           ledger_row=LEDGER_BODY):
+    """scdat_sample_with_derivative over three Domains holding the same scenario; the collected
+    charge is that of `ledger_row` (a face 0..5, or the body box)."""
     L = load()
     arr = (C.c_void_p * 3)(*[d.h for d in domains])
-    nodes = np.ascontiguousarray(body_nodes, np.int64)
+    nodes = np.ascontiguousarray(surface_nodes, np.int64)
     out = CurrentSampleC()
-    rc = L.scdat_sample_with_derivative(arr, nodes.shape[0], _p(nodes), float(surface_potential_v),
+    rc = L.scdat_sample_with_derivative(arr, nodes.shape[0], _p(nodes), int(ledger_row), float(surface_potential_v),
                                         float(probe_delta_v), int(window_steps), float(area_m2), C.byref(out))
     if rc != 0:
         raise ScdatError(rc, L.scdat_last_error(domains[1].h).decode())

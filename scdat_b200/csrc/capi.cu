@@ -25,8 +25,8 @@ void launch_push_f64(const MeshView& M, const ParticleStore& P, const SpeciesDev
                      unsigned* ctr, int grid, cudaStream_t st);
 void launch_mcc_f64(const ParticleStore& P, const SpeciesDev& S, const PushParams& pp, LedgerDev* L, int grid,
                     cudaStream_t st);
-void launch_push_mixed(const MeshView& M, const ParticleStore& P, const SpeciesDev& S, const PushParams& pp,
-                       const DeferList& D1, const DeferList& D2, ChargeAcc A, LedgerDev* L,
+void launch_push_mixed(const MeshView& M, const ParticleStore& P, const SortedSource& R, const SpeciesDev& S,
+                       const PushParams& pp, const DeferList& D1, const DeferList& D2, ChargeAcc A, LedgerDev* L,
                        unsigned long long* ke_acc, unsigned* ctr, int grid, bool stay_first, cudaStream_t st);
 void launch_mcc_mixed(const ParticleStore& P, const SpeciesDev& S, const PushParams& pp, LedgerDev* L, int grid,
                       cudaStream_t st);
@@ -90,7 +90,7 @@ double pow2_ceil(double v)
 
 namespace scdat {
 
-ParticleStore store_of(scdat_ctx* ctx, int s)
+static ParticleStore store_view(scdat_ctx* ctx, int s)
 {
     SpeciesState& S = ctx->species[s];
     ParticleStore P{};
@@ -101,6 +101,30 @@ ParticleStore store_of(scdat_ctx* ctx, int s)
     P.id = S.id.p;
     P.count = ctx->counts.p + s;
     return P;
+}
+
+// Apply a re-sort still pending on species s (mixed form): one gather of the store through the
+// permutation, the tet of each kept particle being its sorted key.
+int settle_store(scdat_ctx* ctx, int s)
+{
+    SpeciesState& S = ctx->species[s];
+    if (!S.perm_pending) return SCDAT_OK;
+    S.perm_pending = false;
+    ++ctx->launches;
+    launch_gather_mixed(S.n, ctx->counts.p + s, S.perm.p, S.skey.p, (uint32_t)ctx->hm.T, S.mix.p, S.id.p, S.mix2.p,
+                        S.tet2.p, S.id2.p, ctx->st);
+    S.mix.swap(S.mix2);
+    S.tet.swap(S.tet2);
+    S.id.swap(S.id2);
+    CK(cudaGetLastError());
+    return SCDAT_OK;
+}
+
+// The store of species s for any use other than the push (which reads a pending re-sort itself).
+ParticleStore store_of(scdat_ctx* ctx, int s)
+{
+    settle_store(ctx, s);
+    return store_view(ctx, s);
 }
 
 SpeciesDev species_dev(const scdat_ctx* ctx, int s)
@@ -235,7 +259,17 @@ int do_push(scdat_ctx* ctx, bool do_mcc)
     for (int s = 0; s < S; ++s) {
         if (ctx->species[s].cap == 0) continue;
         ctx->push_particles += ctx->species[s].n;
-        ParticleStore P = store_of(ctx, s);
+        SpeciesState& Ss = ctx->species[s];
+        ParticleStore P = store_view(ctx, s);
+        SortedSource R{};
+        if (Ss.perm_pending) {
+            // pass 1 gathers the re-sorted store itself: it reads through the permutation and
+            // writes the sorted order into the second buffers, which every pass then uses
+            R = SortedSource{Ss.perm.p, Ss.skey.p, (uint32_t)ctx->hm.T, Ss.mix.p, Ss.id.p};
+            P.mix = Ss.mix2.p;
+            P.tet = Ss.tet2.p;
+            P.id = Ss.id2.p;
+        }
         SpeciesDev sd = species_dev(ctx, s);
         // defer-list counts [0, 1] and the three passes' work counters [2, 5)
         CK(cudaMemsetAsync(ctx->dcount.p, 0, 5 * sizeof(unsigned), ctx->st));
@@ -246,8 +280,14 @@ int do_push(scdat_ctx* ctx, bool do_mcc)
                                    : ChargeAcc{ctx->acc_l0.p + s * N, ctx->acc_l1.p + s * N, ctx->acc_h.p + s * N};
         if (ctx->mixed) {
             const bool stay = stay_first_now(ctx, s);
-            launch_push_mixed(ctx->mv, P, sd, pp, d1, d2, acc, ctx->led.p, ctx->ke_acc.p, ctx->dcount.p + 2,
+            launch_push_mixed(ctx->mv, P, R, sd, pp, d1, d2, acc, ctx->led.p, ctx->ke_acc.p, ctx->dcount.p + 2,
                               ctx->grid_push, stay, ctx->st);
+            if (Ss.perm_pending) {
+                Ss.perm_pending = false;
+                Ss.mix.swap(Ss.mix2);
+                Ss.tet.swap(Ss.tet2);
+                Ss.id.swap(Ss.id2);
+            }
             if (stay) {
                 // pass 1's deferred count, read by the next push's choice (the field solve in
                 // between synchronises the stream)
@@ -639,6 +679,8 @@ int do_sort(scdat_ctx* ctx, int s)
     SpeciesState& S = ctx->species[s];
     const int64_t n = S.n;
     if (n == 0) return SCDAT_OK;
+    int rc = settle_store(ctx, s);  // the keys are read from the store in its current order
+    if (rc) return rc;
     const uint32_t inactive = (uint32_t)ctx->hm.T;  // keys: tet, T (no hint), T+1 (inactive)
     int bits = 1;
     while (((uint64_t)1 << bits) <= (uint64_t)inactive + 1) ++bits;
@@ -648,23 +690,23 @@ int do_sort(scdat_ctx* ctx, int s)
         CK(cudaEventCreate(&ev.e1));
         CK(cudaEventRecord(ev.e0, ctx->st));
     }
-    ctx->launches += 2;  // keys + one gather of the whole store (the radix sort itself is CUB's)
+    // the mixed form sorts into the species' own permutation and key buffers and leaves the
+    // gather to the next pass 1 (or to settle_store)
+    uint32_t* kout = ctx->mixed ? S.skey.p : ctx->kout.p;
+    uint32_t* vout = ctx->mixed ? S.perm.p : ctx->vout.p;
+    ctx->launches += ctx->mixed ? 1 : 2;  // keys (+ the FP64 form's gather); the radix sort itself is CUB's
     launch_sort_keys(n, S.tet.p, inactive, ctx->kin.p, ctx->vin.p, ctx->nact.p, ctx->st);
     size_t tmp = 0;
-    CK(cub::DeviceRadixSort::SortPairs(nullptr, tmp, ctx->kin.p, ctx->kout.p, ctx->vin.p, ctx->vout.p, (int)n, 0, bits,
-                                       ctx->st));
+    CK(cub::DeviceRadixSort::SortPairs(nullptr, tmp, ctx->kin.p, kout, ctx->vin.p, vout, (int)n, 0, bits, ctx->st));
     if (tmp > ctx->cub_tmp.n) CK(ctx->cub_tmp.alloc(tmp));
-    CK(cub::DeviceRadixSort::SortPairs(ctx->cub_tmp.p, tmp, ctx->kin.p, ctx->kout.p, ctx->vin.p, ctx->vout.p, (int)n,
-                                       0, bits, ctx->st));
-    const uint32_t* perm = ctx->vout.p;
-    if (ctx->scratchi.n < S.tet.n) CK(ctx->scratchi.alloc(S.tet.n));
-    if (ctx->scratchu.n < S.id.n) CK(ctx->scratchu.alloc(S.id.n));
+    CK(cub::DeviceRadixSort::SortPairs(ctx->cub_tmp.p, tmp, ctx->kin.p, kout, ctx->vin.p, vout, (int)n, 0, bits,
+                                       ctx->st));
     if (ctx->mixed) {
-        if (ctx->shadow_mix.n < S.mix.n) CK(ctx->shadow_mix.alloc(S.mix.n));
-        launch_gather_mixed(n, ctx->nact.p, perm, ctx->kout.p, inactive, S.mix.p, S.id.p, ctx->shadow_mix.p,
-                            ctx->scratchi.p, ctx->scratchu.p, ctx->st);
-        S.mix.swap(ctx->shadow_mix);
+        S.perm_pending = true;
     } else {
+        const uint32_t* perm = ctx->vout.p;
+        if (ctx->scratchi.n < S.tet.n) CK(ctx->scratchi.alloc(S.tet.n));
+        if (ctx->scratchu.n < S.id.n) CK(ctx->scratchu.alloc(S.id.n));
         DBuf<double>* da[6] = {&S.x, &S.y, &S.z, &S.vx, &S.vy, &S.vz};
         GatherArrays<double> in{}, out{};
         for (int a = 0; a < 6; ++a) {
@@ -676,9 +718,9 @@ int do_sort(scdat_ctx* ctx, int s)
         out.tet = ctx->scratchi.p; out.id = ctx->scratchu.p;
         launch_gather_store<double>(n, ctx->nact.p, perm, in, out, ctx->st);
         for (int a = 0; a < 6; ++a) da[a]->swap(ctx->shadow64[a]);
+        S.tet.swap(ctx->scratchi);
+        S.id.swap(ctx->scratchu);
     }
-    S.tet.swap(ctx->scratchi);
-    S.id.swap(ctx->scratchu);
     CK(cudaGetLastError());
     if (ctx->timing) {
         CK(cudaEventRecord(ev.e1, ctx->st));
@@ -956,8 +998,14 @@ static int alloc_species(scdat_ctx* ctx, int s, int64_t n)
 {
     SpeciesState& S = ctx->species[s];
     int64_t cap = std::max<int64_t>(n, 1);
+    S.perm_pending = false;
     if (ctx->mixed) {
         CK(S.mix.alloc(2 * (size_t)cap));
+        CK(S.mix2.alloc(2 * (size_t)cap));
+        CK(S.tet2.alloc((size_t)cap));
+        CK(S.id2.alloc((size_t)cap));
+        CK(S.perm.alloc((size_t)cap));
+        CK(S.skey.alloc((size_t)cap));
         for (DBuf<double>* a : {&S.x, &S.y, &S.z, &S.vx, &S.vy, &S.vz}) a->release();
     } else {
         for (DBuf<double>* a : {&S.x, &S.y, &S.z, &S.vx, &S.vy, &S.vz}) CK(a->alloc((size_t)cap));
@@ -1002,7 +1050,6 @@ static int alloc_species(scdat_ctx* ctx, int s, int64_t n)
     for (int a = 0; a < 6; ++a) {
         if (!ctx->mixed && ctx->shadow64[a].n < need) CK(ctx->shadow64[a].alloc(need));
     }
-    if (ctx->mixed && ctx->shadow_mix.n < 2 * need) CK(ctx->shadow_mix.alloc(2 * need));
     if (ctx->scratchi.n < need) CK(ctx->scratchi.alloc(need));
     if (ctx->scratchu.n < need) CK(ctx->scratchu.alloc(need));
     int bits = 1;
@@ -1223,6 +1270,10 @@ SCDAT_API int scdat_get_particles(scdat_ctx* ctx, int32_t species, int64_t capac
     if (n_out) *n_out = n;
     ARG(capacity >= n, "capacity smaller than the particle count");
     if (n == 0) return SCDAT_OK;
+    {
+        int rc = settle_store(ctx, species);
+        if (rc) return rc;
+    }
     std::vector<double> cx((size_t)n), cy((size_t)n), cz((size_t)n), wx((size_t)n), wy((size_t)n), wz((size_t)n);
     std::vector<int32_t> t((size_t)n);
     std::vector<uint32_t> id((size_t)n);
@@ -1633,12 +1684,13 @@ SCDAT_API int scdat_get_species_charge(scdat_ctx* ctx, int32_t species, double* 
 }
 
 SCDAT_API int scdat_sample_with_derivative(scdat_ctx* const* c3, int64_t n_body, const int64_t* body_nodes,
-                                           double v, double probe_delta_v, int32_t window_steps, double area_m2,
-                                           scdat_current_sample* out)
+                                           int32_t row, double v, double probe_delta_v, int32_t window_steps,
+                                           double area_m2, scdat_current_sample* out)
 {
     if (!c3 || !out || !c3[0] || !c3[1] || !c3[2]) return SCDAT_ERR_ARG;
     scdat_ctx* ctx = c3[1];
-    ARG(n_body > 0 && body_nodes && window_steps > 0 && area_m2 > 0.0, "need body nodes, a window and an area");
+    ARG(n_body > 0 && body_nodes && window_steps > 0 && area_m2 > 0.0, "need surface nodes, a window and an area");
+    ARG(row >= 0 && row <= 6, "ledger row out of range (0..5 faces, 6 body)");
     std::memset(out, 0, sizeof(*out));
     const double d = std::max(0.1, std::fabs(probe_delta_v));
     const double pot[3] = {v - d, v, v + d};
@@ -1651,7 +1703,7 @@ SCDAT_API int scdat_sample_with_derivative(scdat_ctx* const* c3, int64_t n_body,
         double led[7 * 8];
         rc = scdat_get_ledger(c3[k], led);
         if (rc) return rc;
-        std::memcpy(before[k], led + 8 * 6, sizeof(before[k]));
+        std::memcpy(before[k], led + 8 * row, sizeof(before[k]));
     }
     const bool mixed = c3[0]->mixed && c3[1]->mixed && c3[2]->mixed;
     if (mixed) {
@@ -1672,7 +1724,7 @@ SCDAT_API int scdat_sample_with_derivative(scdat_ctx* const* c3, int64_t n_body,
         double led[7 * 8];
         int rc = scdat_get_ledger(c3[k], led);
         if (rc) return rc;
-        std::memcpy(after[k], led + 8 * 6, sizeof(after[k]));
+        std::memcpy(after[k], led + 8 * row, sizeof(after[k]));
         const double span = window_steps * c3[k]->prm.dt * area_m2;
         const double je = (after[k][0] - before[k][0]) / span, ji = (after[k][1] - before[k][1]) / span,
                      jm = -(after[k][2] - before[k][2]) / span;

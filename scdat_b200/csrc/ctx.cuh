@@ -75,6 +75,13 @@ struct SpeciesState {
     DBuf<float4> mix;  // mixed form: two float4 per particle (see ParticleStore)
     DBuf<int32_t> tet;
     DBuf<uint32_t> id;
+    // Mixed form: a re-sort leaves its permutation and sorted keys here and the next pass 1
+    // reads the store through them, writing the sorted store into mix2/tet2/id2 (then swapped
+    // in); anything else that needs the store first runs the gather (settle_store).
+    DBuf<float4> mix2;
+    DBuf<int32_t> tet2;
+    DBuf<uint32_t> id2, perm, skey;
+    bool perm_pending = false;
 };
 
 // The start and end events of one timed stage.  An early error return destroys them; commit()
@@ -150,7 +157,6 @@ struct scdat_ctx {
     DBuf<uint32_t> kin, kout, vin, vout;
     DBuf<unsigned char> cub_tmp;
     DBuf<double> shadow64[6];  // re-sort targets, swapped with the store's arrays
-    DBuf<float4> shadow_mix;
     DBuf<int32_t> scratchi;
     DBuf<uint32_t> scratchu;
     DBuf<int64_t> nact;
@@ -215,6 +221,7 @@ struct scdat_ctx {
 namespace scdat {
 // helpers of capi.cu used by the batched step
 ParticleStore store_of(scdat_ctx* ctx, int s);
+int settle_store(scdat_ctx* ctx, int s);
 SpeciesDev species_dev(const scdat_ctx* ctx, int s);
 PushParams push_params(const scdat_ctx* ctx, bool do_mcc);
 int check_flags(scdat_ctx* ctx);

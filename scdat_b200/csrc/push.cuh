@@ -18,6 +18,18 @@ struct ParticleStore {
     const int64_t* count;  // device-resident particle count of this species
 };
 
+// A re-sort whose gather the mixed form's pass 1 does itself: particle i of the sorted order is
+// record perm[i] of the old arrays (mix, id) and its tet is the sorted key (a key of nohint_key
+// or above: no hint); pass 1 writes it to position i of its ParticleStore.  perm == nullptr:
+// nothing pending, pass 1 reads the store in place.
+struct SortedSource {
+    const uint32_t* perm;
+    const uint32_t* keys;
+    uint32_t nohint_key;
+    const float4* mix;
+    const uint32_t* id;
+};
+
 __device__ __forceinline__ void mix_load(const ParticleStore& P, int64_t i, float& x, float& y, float& z, float& vx,
                                          float& vy, float& vz)
 {

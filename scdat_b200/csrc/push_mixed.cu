@@ -370,18 +370,36 @@ __device__ __forceinline__ void defer_store_f(const ParticleStore& P, const Defe
     P.tet[i] = f.cur;
 }
 
+// Pass 1's load of particle i: from the store in place, or through a pending re-sort (R), whose
+// particle id it copies into the store at once (the fused MCC reads it there).  Every particle
+// a re-sort keeps is active, and pass 1 writes each of them back (finished or deferred).
+__device__ __forceinline__ void load_first(const ParticleStore& P, const SortedSource& R, int64_t i, FlightF& f)
+{
+    if (R.perm) {
+        const uint32_t j = __ldg(R.perm + i);
+        const uint32_t key = __ldg(R.keys + i);
+        f.cur = key < R.nohint_key ? (int)key : kTetNoHint;
+        const float4 a = __ldg(R.mix + 2 * (int64_t)j), b = __ldg(R.mix + 2 * (int64_t)j + 1);
+        f.rx = a.x; f.ry = a.y; f.rz = a.z; f.vx = a.w;
+        f.vy = b.x; f.vz = b.y;
+        P.id[i] = __ldg(R.id + j);
+    } else {
+        f.cur = P.tet[i];
+        mix_load(P, i, f.rx, f.ry, f.rz, f.vx, f.vy, f.vz);
+    }
+}
+
 // Pass 1 for the 32 particles [base, base + 32) of one warp: at most kCap1 sub-steps, the
 // unfinished ones appended to D.
-__device__ __forceinline__ void push1_warp(const MeshView& M, const ParticleStore& P, const SpeciesDev& S,
-                                           const PushParams& pp, const DeferList& D, ChargeAcc A, LedgerDev* L,
-                                           int64_t base, int64_t n, PushStats& c)
+__device__ __forceinline__ void push1_warp(const MeshView& M, const ParticleStore& P, const SortedSource& R,
+                                           const SpeciesDev& S, const PushParams& pp, const DeferList& D, ChargeAcc A,
+                                           LedgerDev* L, int64_t base, int64_t n, PushStats& c)
 {
     const int64_t i = base + (threadIdx.x & 31);
     int st = -1;
     FlightF f;
     if (i < n) {
-        f.cur = P.tet[i];
-        mix_load(P, i, f.rx, f.ry, f.rz, f.vx, f.vy, f.vz);
+        load_first(P, R, i, f);
         if (f.cur <= kTetAbsorbed) {
             // updateStatistics sums every particle the container still holds (PICCycle.cpp:941-966)
             double ux = f.vx, uy = f.vy, uz = f.vz;
@@ -484,16 +502,15 @@ __device__ __forceinline__ int advance_stay_f(const MeshView& M, const SpeciesDe
 // Stay-first pass 1 for the 32 particles [base, base + 32): one sub-step for those that stay in
 // their tet; everything else (leaving the tet, more time left, no location hint) goes to D,
 // whose capacity covers the whole species, so nothing overflows.
-__device__ __forceinline__ void push1_stay_warp(const MeshView& M, const ParticleStore& P, const SpeciesDev& S,
-                                                const PushParams& pp, const DeferList& D, ChargeAcc A, LedgerDev* L,
-                                                int64_t base, int64_t n, PushStats& c)
+__device__ __forceinline__ void push1_stay_warp(const MeshView& M, const ParticleStore& P, const SortedSource& R,
+                                                const SpeciesDev& S, const PushParams& pp, const DeferList& D,
+                                                ChargeAcc A, LedgerDev* L, int64_t base, int64_t n, PushStats& c)
 {
     const int64_t i = base + (threadIdx.x & 31);
     int st = -1;
     FlightF f;
     if (i < n) {
-        f.cur = P.tet[i];
-        mix_load(P, i, f.rx, f.ry, f.rz, f.vx, f.vy, f.vz);
+        load_first(P, R, i, f);
         if (f.cur <= kTetAbsorbed) {
             double ux = f.vx, uy = f.vy, uz = f.vz;
             c.ke += 0.5 * S.m * (ux * ux + uy * uy + uz * uz);
@@ -506,10 +523,14 @@ __device__ __forceinline__ void push1_stay_warp(const MeshView& M, const Particl
     }
     const unsigned slot = warp_append(st == kCapped, D.count);
     if (st == kCapped) {
-        if (slot < D.cap)
+        if (slot < D.cap) {
             defer_store_f(P, D, slot, i, f);
-        else
+        } else {
+            // the step fails with this flag; the particle is stored as it stands
             atomicOr(&L->flags, (unsigned long long)kFlagDeferOverflow);
+            mix_store(P, i, f.rx, f.ry, f.rz, f.vx, f.vy, f.vz);
+            P.tet[i] = f.cur;
+        }
     } else if (st >= 0) {
         finish_f(M, P, S, pp, L, i, f, st, c);
     }
@@ -565,6 +586,7 @@ __device__ __forceinline__ void push_more_warp(const MeshView& M, const Particle
 // 6 blocks of 256 per SM (40 registers): the extra warps hide more of the walk's load latency
 // than the extra spills cost (4 blocks: 46.2 ms, 5: 47.7, 6: 45.3, 8: 47.5 per step at 128^3)
 __global__ void __launch_bounds__(256, 6) k_push_mixed(const __grid_constant__ MeshView M, ParticleStore P,
+                                                    const __grid_constant__ SortedSource R,
                                                     const __grid_constant__ SpeciesDev S,
                                                     const __grid_constant__ PushParams pp, DeferList D, ChargeAcc A,
                                                     LedgerDev* L, unsigned long long* ke_acc, unsigned* ctr)
@@ -576,7 +598,7 @@ __global__ void __launch_bounds__(256, 6) k_push_mixed(const __grid_constant__ M
         const int64_t b0 = (int64_t)next_chunk(ctr) * (32 * kRun);
         if (b0 >= n) break;
         for (int64_t base = b0; base < b0 + 32 * kRun && base < n; base += 32)
-            push1_warp(M, P, S, pp, D, A, L, base, n, c);
+            push1_warp(M, P, R, S, pp, D, A, L, base, n, c);
     }
     warp_stats_flush(L, ke_acc, S.vmax);
 }
@@ -585,6 +607,7 @@ __global__ void __launch_bounds__(256, 6) k_push_mixed(const __grid_constant__ M
 // fewer registers: 6 blocks of 256 per SM at 40 registers spill 64 bytes a thread, against 456
 // for the walking pass 1.
 __global__ void __launch_bounds__(256, 6) k_push_mixed_stay(const __grid_constant__ MeshView M, ParticleStore P,
+                                                         const __grid_constant__ SortedSource R,
                                                          const __grid_constant__ SpeciesDev S,
                                                          const __grid_constant__ PushParams pp, DeferList D,
                                                          ChargeAcc A, LedgerDev* L, unsigned long long* ke_acc,
@@ -597,7 +620,7 @@ __global__ void __launch_bounds__(256, 6) k_push_mixed_stay(const __grid_constan
         const int64_t b0 = (int64_t)next_chunk(ctr) * (32 * kRun);
         if (b0 >= n) break;
         for (int64_t base = b0; base < b0 + 32 * kRun && base < n; base += 32)
-            push1_stay_warp(M, P, S, pp, D, A, L, base, n, c);
+            push1_stay_warp(M, P, R, S, pp, D, A, L, base, n, c);
     }
     warp_stats_flush(L, ke_acc, S.vmax);
 }
@@ -683,7 +706,7 @@ __global__ void __launch_bounds__(256, 4) k_push_mixed_batch(const PushJob* __re
         if (PASS == 1) {
             const int64_t n = *J.P.count, b0 = (g - spre[cur]) * (32 * kRun);
             for (int64_t base = b0; base < b0 + 32 * kRun && base < n; base += 32)
-                push1_warp(J.M, J.P, J.S, J.pp, J.D1, J.A, J.L, base, n, c);
+                push1_warp(J.M, J.P, SortedSource{}, J.S, J.pp, J.D1, J.A, J.L, base, n, c);
             continue;
         }
         const int64_t base = (g - spre[cur]) * 32;
@@ -766,14 +789,14 @@ __global__ void k_refresh_trec(int64_t T, const int4* __restrict__ tet, const do
         refresh_trec_part(g >> 2, (int)(g & 3), tet, E, trec);
 }
 
-void launch_push_mixed(const MeshView& M, const ParticleStore& P, const SpeciesDev& S, const PushParams& pp,
-                       const DeferList& D1, const DeferList& D2, ChargeAcc A, LedgerDev* L,
+void launch_push_mixed(const MeshView& M, const ParticleStore& P, const SortedSource& R, const SpeciesDev& S,
+                       const PushParams& pp, const DeferList& D1, const DeferList& D2, ChargeAcc A, LedgerDev* L,
                        unsigned long long* ke_acc, unsigned* ctr, int grid, bool stay_first, cudaStream_t st)
 {
     if (stay_first)
-        k_push_mixed_stay<<<grid, 256, 0, st>>>(M, P, S, pp, D1, A, L, ke_acc, ctr);
+        k_push_mixed_stay<<<grid, 256, 0, st>>>(M, P, R, S, pp, D1, A, L, ke_acc, ctr);
     else
-        k_push_mixed<<<grid, 256, 0, st>>>(M, P, S, pp, D1, A, L, ke_acc, ctr);
+        k_push_mixed<<<grid, 256, 0, st>>>(M, P, R, S, pp, D1, A, L, ke_acc, ctr);
     k_push_mixed_more<<<grid, 256, 0, st>>>(M, P, S, pp, D1, D2, kCap2, A, L, ke_acc, ctr + 1);
     DeferList none{};
     k_push_mixed_more<<<grid, 256, 0, st>>>(M, P, S, pp, D2, none, 0, A, L, ke_acc, ctr + 2);

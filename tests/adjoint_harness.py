@@ -65,3 +65,45 @@ def central_difference(window, params, rel=1e-4):
         dn[k] -= h
         out.append((window.run(*up)["J"] - window.run(*dn)["J"]) / (2 * h))
     return np.array(out)
+
+
+class BoxWindow:
+    """The differentiation configuration at its size: a Kuhn box of n^3 cells (0.05 m) with a
+    central body of n/4 cells per edge carrying the floating dielectric circuit, electrons and
+    H+ at 1e10 m^-3 seeded on the device (the same Philox draws for every parameter set, so a
+    change of Te rescales the electron velocities), Sternglass secondaries (Emax 300 eV);
+    J = wV . mean face potential + wI . net current collected by the body over the window."""
+
+    def __init__(self, n=48, ppc=32, steps=50, checkpoint=10, wV=1.0, wI=0.0, seed=4321):
+        from scdat_b200 import capi
+
+        self.n, self.ppc, self.steps, self.checkpoint, self.wV, self.wI, self.seed = n, ppc, steps, checkpoint, wV, wI, seed
+        self.h, self.dt, self.density, self.ti, self.e_max = 0.05, 2e-8, 1e10, 1.0, 300.0
+        q = n // 4
+        lo = (n - q) // 2
+        self.body = ((lo, lo + q),) * 3
+        self.blo = tuple(b[0] * self.h for b in self.body)
+        self.bhi = tuple(b[1] * self.h for b in self.body)
+        self.mesh = capi.kuhn_box_mesh((n, n, n), self.h, body=self.body, bias=-1.0)
+
+    def run(self, bias, te, dmax):
+        from scdat_b200 import capi
+
+        m = self.mesh
+        phi = np.where(m["phi"] != 0.0, bias, 0.0)
+        dom = capi.Domain(m["xyz"], m["tet"], m["dirichlet"], self.dt, face_bc=(1,) * 6, pcg_rtol=1e-14,
+                          pcg_max_iter=20000)
+        try:
+            dom.set_species(O.plasma_species(self.density, te, self.ti, self.h, self.ppc))
+            dom.seed_box(0, (self.n,) * 3, self.h, self.body, self.ppc, te, self.seed)
+            dom.seed_box(1, (self.n,) * 3, self.h, self.body, self.ppc, self.ti, self.seed)
+            dom.set_surface_circuit(self.blo, self.bhi, eps_r=3.0, thickness=1e-3, v0=bias)
+            dom.set_secondary_emission(1, dmax, self.e_max)
+            dom.set_potential(phi)
+            dom.solve_field(allow_not_converged=True)
+            gI = self.wI / (self.steps * self.dt)
+            r = dom.adjoint_window(self.steps, self.checkpoint, g_V=[self.wV / 6.0] * 6, g_Q=[gI] * 6, te_ev=te)
+            r["collected"] = int(np.asarray(dom.surface_state()["counts"]).sum())
+            return r
+        finally:
+            dom.close()

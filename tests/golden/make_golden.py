@@ -5,9 +5,11 @@ Run in a checkout where the reference tree is present and oracle/_ref was built
 
     python tests/golden/make_golden.py            # the small cases
     python tests/golden/make_golden.py config0    # config0_ref.npz, the 32^3 configuration
+    python tests/golden/make_golden.py sampler    # sampler_ref.npz, the surface current sampler
 
 Every fixture is produced by the reference's own classes (CrossTetrahedron, PoissonSolver,
-PICCycle) through oracle/ref_harness.cpp on identical, seeded mesh and particle state.
+PICCycle, PicMccSurfaceCurrentSampler) through oracle/ref_harness.cpp on identical, seeded mesh
+and particle state (the sampler seeds its own particles; its fixture holds its mesh and output).
 The inputs are regenerated from the recorded seeds by oracle.py's builders.
 """
 import os
@@ -81,11 +83,38 @@ def make_config0(o, r):
     print("config0", mesh.N, mesh.T, parts["x"].shape[0], sub["x"].shape[0])
 
 
+# PicMccSurfaceCurrentSampler scenario: a 1 cm^2 plate 1 mm below the plasma boundary, 8 layers,
+# a low-density Ar plasma (Debye length well above the gap, so the field is the applied one),
+# MCC off, the sampler's default window and seed.
+SAMPLER = dict(area_m2=1e-4, aspect=1.0, gap_m=1e-3, z_layers=8, ppe=2000, window_steps=12, seed=20260408,
+               ne=1e12, ni=1e12, te_ev=5.0, ti_ev=0.2, ion_amu=40.0, reference_v=0.0, probe_dv=0.5)
+SAMPLER_POTENTIALS = (-2.0, 0.0)
+
+
+def make_sampler(r):
+    c = SAMPLER
+    xyz, tet = r.sampler_mesh(c["area_m2"], c["aspect"], c["gap_m"], c["z_layers"])
+    rows = []
+    for v in SAMPLER_POTENTIALS:
+        out = r.sampler_sample(c["area_m2"], c["gap_m"], c["z_layers"], c["ppe"], c["window_steps"], c["seed"],
+                               c["ne"], c["ni"], c["te_ev"], c["ti_ev"], c["ion_amu"], v, c["reference_v"],
+                               c["probe_dv"])
+        assert out["valid"] == 1.0
+        rows.append([out[k] for k in ("electron", "ion", "emitted", "net", "derivative", "segments")])
+    np.savez_compressed(os.path.join(HERE, "sampler_ref.npz"), xyz=xyz, tet=tet,
+                        potentials=np.array(SAMPLER_POTENTIALS), samples=np.array(rows))
+    print("sampler", xyz.shape[0], tet.shape[0], np.array(rows))
+
+
 def main():
     o = O.Oracle()
     r = O.Reference()
     if len(sys.argv) > 1 and sys.argv[1] == "config0":
         make_config0(O.Oracle(fast_locate=True), r)
+        r.close()
+        return
+    if len(sys.argv) > 1 and sys.argv[1] == "sampler":
+        make_sampler(r)
         r.close()
         return
     for case in CASES:

@@ -278,6 +278,40 @@ def test_deterministic_and_sort_invariant(lib, precision):
     assert out[0][5]["total_energy"] == out[1][5]["total_energy"]
 
 
+def test_resort_gather_in_push_matches_gather_on_read(lib):
+    """The precision form's re-sort leaves its gather to the next pass 1, which reads the store
+    through the permutation; a read of the store in between (here the particles, every step)
+    gathers it at once instead.  Both orders give bitwise the same run, with the stay-first ion
+    pass and the walking pass both reading through a pending re-sort."""
+    from scdat_b200 import capi
+
+    mesh = O.kuhn_box((8, 8, 8), 0.05, body=((3, 5), (3, 5), (3, 5)), bias=-10.0)
+    sp = O.plasma_species(1e10, 1.0, 1.0, 0.05, 6)
+    parts = O.seed_particles(mesh, sp, 6, 7)
+    out = []
+    for read_between, ion_mode in ((False, capi.PUSH_STAY_FIRST), (True, capi.PUSH_STAY_FIRST),
+                                   (False, capi.PUSH_WALKING)):
+        dom = gpu_domain(mesh, 2e-8, face_bc=(2, 2, 2, 2, 1, 1), precision=1, sort_interval=1)
+        gpu_load_particles(dom, sp, parts)
+        dom.set_push_mode(1, ion_mode)
+        dom.set_potential(mesh.phi_bc)
+        dom.solve_field()
+        for _ in range(5):
+            dom.step(1)
+            if read_between:
+                gpu_state(dom, len(sp), len(parts["tet"]))
+        dom.compact()  # a re-sort with no push after it: read back through the gather
+        rho, phi, E = dom.fields()
+        out.append((rho, phi, gpu_state(dom, len(sp), len(parts["tet"])), dom.ledger(), dom.stats()))
+        dom.close()
+    for k in (1, 2):
+        assert np.array_equal(out[0][0], out[k][0]) and np.array_equal(out[0][1], out[k][1])
+        for key in ("x", "v", "tet", "status"):
+            assert np.array_equal(out[0][2][key], out[k][2][key], equal_nan=True), key
+        assert np.array_equal(out[0][3], out[k][3])
+        assert out[0][4]["total_energy"] == out[k][4]["total_energy"]
+
+
 def test_mixed_precision_error_bounded(lib):
     """Precision form against the FP64 form on the same inputs (errors reported and bounded)."""
     mesh, sp, parts, dt, nsteps, face_bc = make_inputs("box6_body")
