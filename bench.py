@@ -4,9 +4,9 @@ MCC + Poisson solve + nodal field) on a synthetic Kuhn-box plasma, through the C
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config NAME]
 
 Workloads (all synthetic, seeded; the reference publishes no dataset):
-  precision128  128^3 hex cells x 6 tets (12.6M tets), h = 1.6 m / 128, central 32^3-cell
+  precision128  128^3 hex cells x 6 tets (12.4M tets outside the body), h = 1.6 m / 128, central 32^3-cell
                 conducting body at -10 V, outer faces 0 V, electrons + H+ at n = 1e10 m^-3,
-                Te = Ti = 1 eV, 64 particles per cell per species (~268M), dt = 2e-8 s,
+                Te = Ti = 1 eV, 64 particles per cell per species (~264M), dt = 2e-8 s,
                 FP32 cell-relative push, fixed-point deposit, FP32-SpMV PCG under FP64
                 refinement to 1e-10, elastic MCC (sigma 1e-19 m^2, n_n 1e14 m^-3), electrons
                 re-sorted by tet every step (they cross ~0.7 cells per step), ions every 16
@@ -24,6 +24,11 @@ Workloads (all synthetic, seeded; the reference publishes no dataset):
                 collected charge into FP64 potentials, n = 1e9 m^-3, Te = Ti = 5 eV, 16 ppc,
                 dt = 0.1 / omega_pe; mixed form, with the FP64 form's face potentials after the
                 same steps as the error reference
+  surface_long  the same plasma and dielectric faces on a 64 x 64 x 32-cell box (8 x 8 x 4
+                body) run for thousands of steps: the face-potential error of the mixed form
+                against FP64 every 100 steps, beside FP64 controls (one velocity moved by one
+                ulp, every velocity rounded to FP32, an independent seed) that size the
+                run-to-run divergence of the chaotic particle dynamics
 Every rank runs an independent replica ("replicas only": the path has no exchange step).
 """
 from __future__ import annotations
@@ -76,6 +81,8 @@ def nudge_one_velocity(dom, s=0):
     v = p["v"].copy()
     v[0, 0] = np.nextafter(v[0, 0], np.inf)
     dom.set_particles(s, p["x"], v, p["tet"], p["id"])
+
+
 EPS0 = 8.8541878128e-12
 
 
@@ -218,11 +225,12 @@ def alg_bytes_push(dom, precision, particles):
     return particles * b_p + dom.T * t_b + dom.N * n_b
 
 
-# DRAM bytes per stored particle of one step's push launches (all passes, both species): an ncu
-# capture (dram__bytes_read.sum + dram__bytes_write.sum) of one step's six push launches on a
-# 64^3-cell box at 64 ppc per species (31.9 M particles, 6.15 GB), divided by the particles; the
-# full workload has the same density and access pattern.  None: not measured for the form.
-PUSH_DRAM_BYTES_PER_PARTICLE = {1: 193.0, 0: None}
+# DRAM bytes per stored particle of one step's push launches (all passes, both species; the
+# electrons' pass 1 includes the gather of their re-sort): an ncu capture (dram__bytes_read.sum +
+# dram__bytes_write.sum) of one step's six push launches on a 64^3-cell box at 64 ppc per species
+# (31.9 M particles, 9.52 GB), divided by the particles; the full workload has the same density
+# and access pattern.  None: not measured for the form.
+PUSH_DRAM_BYTES_PER_PARTICLE = {1: 298.6, 0: None}
 
 
 def cg_iteration_bytes(dom, precision):

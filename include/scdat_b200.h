@@ -191,6 +191,12 @@ SCDAT_API int scdat_seed_tet_particles(scdat_ctx* ctx, int32_t species, int64_t 
 SCDAT_API int scdat_export_layer_profile_csv(scdat_ctx* ctx, const char* path, int32_t n_layers);
 /* Every node: position, potential, charge and field. */
 SCDAT_API int scdat_export_nodes_csv(scdat_ctx* ctx, const char* path);
+/* CSVExporter::exportDataSet (Tools/Output/src/CSVExporter.cpp:11-47) on a columnar data set:
+ * n_rows axis values and n_series named series of n_rows values each, written in series-name
+ * order (the reference's std::map), the parent directory created first.  Host code only: needs
+ * no context and no GPU; the two exports above write through it. */
+SCDAT_API int scdat_export_columns_csv(const char* path, const char* axis_name, int64_t n_rows, const double* axis,
+                                       int32_t n_series, const char* const* names, const double* const* values);
 
 /* ParticleContainer iteration (ParticleManager.h:113-126): copy one species back. */
 SCDAT_API int scdat_get_particle_count(scdat_ctx* ctx, int32_t species, int64_t* n);

@@ -485,6 +485,9 @@ class Reference:
         L.ref_sampler_sample.argtypes = [C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, C.c_uint] + \
             [C.c_double] * 8 + [C.c_int, _dp]
         L.ref_sampler_sample.restype = C.c_int
+        L.ref_csv_export.argtypes = [C.c_char_p, C.c_char_p, C.c_int64, _dp, C.c_int, C.POINTER(C.c_char_p),
+                                     C.POINTER(C.c_void_p)]
+        L.ref_csv_export.restype = C.c_int
         self._meshes = {}
 
     def mesh(self, mesh: BoxMesh, neighbors=True):
@@ -627,6 +630,15 @@ class Reference:
                                   float(reference_v), float(probe_dv), int(bool(enable_mcc)), out)
         keys = ("electron", "ion", "emitted", "net", "derivative", "valid", "segments", "seed")
         return dict(zip(keys, out))
+
+    def csv_export(self, path, axis_name, axis, series):
+        """CSVExporter::exportDataSet of {name: values} over the axis; True on success."""
+        names = list(series)
+        vals = [np.ascontiguousarray(series[k], np.float64) for k in names]
+        cn = (C.c_char_p * max(1, len(names)))(*[k.encode() for k in names])
+        cv = (C.c_void_p * max(1, len(names)))(*[v.ctypes.data for v in vals])
+        a = np.ascontiguousarray(axis, np.float64)
+        return self.L.ref_csv_export(str(path).encode(), axis_name.encode(), len(a), a, len(names), cn, cv) == 0
 
     def parse_cross_section_set(self, text):
         """Collision::parseCollisionCrossSectionSetId: -1 unknown, else the set's index."""

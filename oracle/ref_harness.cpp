@@ -12,6 +12,7 @@
 //   evaluateLegacySecondaryElectronYield        Tools/Material/src/SurfaceMaterialModel.cpp:620-636
 //   PicMccSurfaceCurrentSampler::sampleWithDerivative
 //                                               Toolkit/Surface Charging/src/PicMccSurfaceCurrentSampler.cpp:641-670
+//   CSVExporter::exportDataSet                  Tools/Output/src/CSVExporter.cpp:11-47
 // Only the parity tests and the CPU reference arm of the benchmark load it.
 #include "PICcore/include/PICCycle.h"
 #include "Mesh/include/MeshParsing.h"
@@ -21,6 +22,7 @@
 #include "Material/include/MaterialProperty.h"
 #include "Material/include/SurfaceMaterialModel.h"
 #include "PicMccSurfaceCurrentSampler.h"
+#include "Output/include/CSVExporter.h"
 
 #include <algorithm>
 #include <chrono>
@@ -543,6 +545,19 @@ int ref_sampler_sample(double area_m2, double gap_m, int z_layers, int ppe, int 
     out[6] = (double)r.deposition_segments;
     out[7] = (double)r.seed_used;
     return r.valid ? 0 : 1;
+}
+
+// CSVExporter::exportDataSet of a columnar data set (axis values and named series of n rows
+// each); 0 on success.
+int ref_csv_export(const char* path, const char* axis_name, int64_t n, const double* axis, int m,
+                   const char* const* names, const double* const* values)
+{
+    SCDAT::Output::ColumnarDataSet ds;
+    ds.axis_name = axis_name;
+    ds.axis_values.assign(axis, axis + n);
+    for (int s = 0; s < m; ++s) ds.scalar_series[names[s]] = std::vector<double>(values[s], values[s] + n);
+    SCDAT::Output::CSVExporter ex;
+    return ex.exportDataSet(path, ds).isSuccess() ? 0 : 1;
 }
 
 }  // extern "C"

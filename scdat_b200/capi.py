@@ -98,7 +98,7 @@ EXPORTS = ["scdat_default_params", "scdat_create", "scdat_destroy", "scdat_last_
            "scdat_batch_last_step_ms", "scdat_batch_stream", "scdat_batch_kernel_launches",
            "scdat_set_surface_circuit", "scdat_get_surface_state", "scdat_set_secondary_emission",
            "scdat_sample_with_derivative", "scdat_adjoint_window", "scdat_seed_tet_particles",
-           "scdat_export_layer_profile_csv", "scdat_export_nodes_csv"]
+           "scdat_export_layer_profile_csv", "scdat_export_nodes_csv", "scdat_export_columns_csv"]
 
 _LIB = None
 
@@ -140,6 +140,8 @@ def load():
     L.scdat_seed_tet_particles.argtypes = [vp, C.c_int32, C.c_int64, vp, C.c_int32, C.c_double, vp, C.c_uint64]
     L.scdat_export_layer_profile_csv.argtypes = [vp, C.c_char_p, C.c_int32]
     L.scdat_export_nodes_csv.argtypes = [vp, C.c_char_p]
+    L.scdat_export_columns_csv.argtypes = [C.c_char_p, C.c_char_p, C.c_int64, vp, C.c_int32, C.POINTER(C.c_char_p),
+                                           C.POINTER(vp)]
     L.scdat_adjoint_window.argtypes = [vp, C.POINTER(AdjointRequestC), C.POINTER(AdjointResultC)]
     L.scdat_sample_with_derivative.argtypes = [C.POINTER(vp), C.c_int64, vp, C.c_int32, C.c_double, C.c_double,
                                                C.c_int32, C.c_double, C.POINTER(CurrentSampleC)]
@@ -563,6 +565,20 @@ class Batch:
 
 
 LEDGER_BODY = 6  # ledger rows 0..5 are the domain faces XMin..ZMax
+
+
+def export_columns_csv(path, axis_name, axis, series):
+    """scdat_export_columns_csv (CSVExporter::exportDataSet) of {name: values} over the axis."""
+    L = load()
+    names = list(series)
+    vals = [np.ascontiguousarray(series[k], np.float64) for k in names]
+    a = np.ascontiguousarray(axis, np.float64)
+    assert all(v.shape == a.shape for v in vals)
+    cn = (C.c_char_p * max(1, len(names)))(*[k.encode() for k in names])
+    cv = (C.c_void_p * max(1, len(names)))(*[v.ctypes.data for v in vals])
+    rc = L.scdat_export_columns_csv(str(path).encode(), axis_name.encode(), a.shape[0], _p(a), len(names), cn, cv)
+    if rc != 0:
+        raise ScdatError(rc, "scdat_export_columns_csv failed")
 
 
 def sample_with_derivative(domains, surface_nodes, surface_potential_v, probe_delta_v, window_steps, area_m2,

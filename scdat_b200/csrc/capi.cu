@@ -15,6 +15,8 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <filesystem>
+#include <map>
 #include <memory>
 #include <string>
 #include <vector>
@@ -855,19 +857,21 @@ int create_ctx(const scdat_mesh_desc* mesh, const scdat_params* params, scdat_ct
     mv.tet = ctx->tet.p;
     mv.nbr = ctx->nbr.p;
     if (ctx->mixed) {
-        // static words of the 128-byte tet records: J^-1 and node ids (E refreshed later)
+        // static words of the 256-byte tet records: J^-1, node ids, neighbours and the origin
+        // shifts to them (E refreshed after each field solve)
         std::vector<float> rec((size_t)(64 * m.T), 0.0f);
         for (int64_t t = 0; t < m.T; ++t) {
             float* r = &rec[64 * t];
             for (int k = 0; k < 9; ++k) r[k] = ctx->hg.geomf[12 * t + k];
-            for (int k = 0; k < 4; ++k) std::memcpy(&r[21 + k], &m.tet[4 * t + k], sizeof(int32_t));
-            for (int k = 0; k < 4; ++k) std::memcpy(&r[25 + k], &m.nbr[4 * t + k], sizeof(int32_t));
+            for (int k = 0; k < 4; ++k) std::memcpy(&r[24 + k], &m.tet[4 * t + k], sizeof(int32_t));
+            for (int k = 0; k < 4; ++k) std::memcpy(&r[28 + k], &m.nbr[4 * t + k], sizeof(int32_t));
             const int64_t o = m.tet[4 * t];
             for (int k = 0; k < 4; ++k) {
-                int32_t nb = m.nbr[4 * t + k];
+                const int32_t nb = m.nbr[4 * t + k];
+                std::memcpy(&r[35 + 4 * k], &nb, sizeof(int32_t));  // the walk's (shift, neighbour) float4
                 if (nb < 0) continue;
                 const int64_t on = m.tet[4 * (int64_t)nb];
-                for (int a = 0; a < 3; ++a) r[32 + 3 * k + a] = (float)(m.xyz[3 * o + a] - m.xyz[3 * on + a]);
+                for (int a = 0; a < 3; ++a) r[32 + 4 * k + a] = (float)(m.xyz[3 * o + a] - m.xyz[3 * on + a]);
             }
         }
         CK(ctx->trec.upload(rec.data(), rec.size(), st));
@@ -1136,26 +1140,46 @@ SCDAT_API int scdat_seed_tet_particles(scdat_ctx* ctx, int32_t species, int64_t 
     return SCDAT_OK;
 }
 
-// ResultExporter / CSVExporter columnar layout (Tools/Output/src/CSVExporter.cpp:11-47): a header
-// "axis,series..." with the series in name order, then one row per axis value, %.8e.
-static int write_columns(scdat_ctx* ctx, const char* path, const std::string& axis, const std::vector<double>& av,
-                         const std::vector<std::pair<std::string, std::vector<double>>>& series)
+// ResultExporter / CSVExporter columnar layout (Tools/Output/src/CSVExporter.cpp:11-47): the
+// parent directory created, a header "axis,series..." with the series in name order (a later
+// series of an equal name replaces an earlier one, as std::map assignment does), then one row
+// per axis value, %.8e.  err: the reason on failure.
+static int write_columns_csv(const char* path, const char* axis, int64_t n_rows, const double* av, int32_t n_series,
+                             const char* const* names, const double* const* values, std::string& err)
 {
+    std::map<std::string, const double*> series;
+    for (int32_t s = 0; s < n_series; ++s) series[names[s]] = values[s];
+    std::error_code ec;
+    const std::filesystem::path p(path);
+    std::filesystem::create_directories(p.parent_path().empty() ? std::filesystem::path(".") : p.parent_path(), ec);
     FILE* f = std::fopen(path, "w");
     if (!f) {
-        ctx->err = std::string("cannot open ") + path;
+        err = std::string("Failed to open csv output: ") + path;
         return SCDAT_ERR_ARG;
     }
-    std::fprintf(f, "%s", axis.c_str());
+    std::fprintf(f, "%s", axis);
     for (auto& s : series) std::fprintf(f, ",%s", s.first.c_str());
     std::fprintf(f, "\n");
-    for (size_t r = 0; r < av.size(); ++r) {
+    for (int64_t r = 0; r < n_rows; ++r) {
         std::fprintf(f, "%.8e", av[r]);
         for (auto& s : series) std::fprintf(f, ",%.8e", s.second[r]);
         std::fprintf(f, "\n");
     }
     std::fclose(f);
     return SCDAT_OK;
+}
+
+static int write_columns(scdat_ctx* ctx, const char* path, const std::string& axis, const std::vector<double>& av,
+                         const std::vector<std::pair<std::string, std::vector<double>>>& series)
+{
+    std::vector<const char*> names;
+    std::vector<const double*> vals;
+    for (auto& s : series) {
+        names.push_back(s.first.c_str());
+        vals.push_back(s.second.data());
+    }
+    return write_columns_csv(path, axis.c_str(), (int64_t)av.size(), av.data(), (int32_t)series.size(), names.data(),
+                             vals.data(), ctx->err);
 }
 
 SCDAT_API int scdat_export_layer_profile_csv(scdat_ctx* ctx, const char* path, int32_t n_layers)
@@ -1250,6 +1274,18 @@ SCDAT_API int scdat_export_nodes_csv(scdat_ctx* ctx, const char* path)
                           {"x_m", x},
                           {"y_m", y},
                           {"z_m", z}});
+}
+
+SCDAT_API int scdat_export_columns_csv(const char* path, const char* axis_name, int64_t n_rows, const double* axis,
+                                       int32_t n_series, const char* const* names, const double* const* values)
+{
+    if (!path || !axis_name || n_rows < 0 || n_series < 0 || (n_rows > 0 && !axis) ||
+        (n_series > 0 && (!names || !values)))
+        return SCDAT_ERR_ARG;
+    for (int32_t s = 0; s < n_series; ++s)
+        if (!names[s] || (n_rows > 0 && !values[s])) return SCDAT_ERR_ARG;
+    std::string err;
+    return write_columns_csv(path, axis_name, n_rows, axis, n_series, names, values, err);
 }
 
 SCDAT_API int scdat_get_particle_count(scdat_ctx* ctx, int32_t species, int64_t* n)

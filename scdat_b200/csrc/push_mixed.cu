@@ -1,13 +1,14 @@
 // push_mixed.cu -- the precision form of the particle step.
 //
 // Particles store FP32 positions relative to the origin node (local vertex 0) of their tet
-// and FP32 velocities (28 bytes with the tet id, against 52 in FP64).  Every tet has one
-// 128-byte record: FP32 inverse Jacobian, the nodal E of its 4 nodes as E0 and three
-// differences (refreshed after every field solve) and its node ids, so a sub-step reads one
-// cache line.  Gather, adaptive sub-step, Boris and the in-tet test run in FP32; a move into
-// a face neighbour is re-based in FP32 from the FP64 node difference; anything farther (walk,
-// grid lookup, boundary events) reconstructs the FP64 absolute position and uses the FP64
-// locate.  Deposit weights are FP32 barycentrics promoted to FP64 before the exact
+// and FP32 velocities (a 32-byte record, plus the tet and particle ids).  Every tet has one
+// 256-byte record: in its first line the FP32 inverse Jacobian, the nodal E of its 4 nodes as
+// E0 and three differences (refreshed after every field solve), its node ids and neighbours,
+// so a sub-step inside the tet reads one cache line; in its second, per face the FP32 origin
+// shift to the neighbour with the neighbour's id, which the walk reads.  Gather, adaptive
+// sub-step, Boris and the in-tet test run in FP32; a move into a face neighbour is re-based in
+// FP32 by the stored shift; a walk that meets a boundary face or runs long reconstructs the FP64
+// absolute position and uses the FP64 locate.  Deposit weights are FP32 barycentrics promoted to FP64 before the exact
 // fixed-point accumulation (one 64-bit word per node, fx_red_word).
 //
 // Sub-steps run in passes so that warps stay converged: pass 1 gives every particle at most
@@ -29,8 +30,14 @@ __device__ __forceinline__ bool inside_f(const float l[4])
 }
 
 // record layout (64 words): [0..8] J^-1, [9..11] E0, [12..20] E1-E0, E2-E0, E3-E0,
-// [21..24] node ids, [25..28] face neighbours, [29..31] unused | [32..43] origin minus the
-// origin of each face neighbour (FP32), [44..63] unused
+// [21..23] unused, [24..27] node ids, [28..31] face neighbours | [32..47] per face f the origin
+// minus the neighbour's origin (FP32) and the neighbour id, one float4 each (the walk reads one
+// 16-byte load per step for both), [48..63] unused
+
+__device__ __forceinline__ int4 node_ids(const MeshView& M, int t)
+{
+    return __ldg(reinterpret_cast<const int4*>(M.trec + 64 * (int64_t)t) + 6);
+}
 
 // Rewrite words 9..20 of record t (E0 and the three differences) from the nodal field, keeping
 // J^-1 and the node ids that share those 16-byte lines.  Four lanes share a record, lane q
@@ -121,10 +128,10 @@ static __device__ __noinline__ Reloc relocate_f(const MeshView& M, int cur, floa
         if (l[1] < lm) { lm = l[1]; f = 1; }
         if (l[2] < lm) { lm = l[2]; f = 2; }
         if (l[3] < lm) f = 3;
-        const float* rec = M.trec + 64 * (int64_t)t;
-        int nt = __float_as_int(__ldg(rec + 25 + f));
+        const float4 sh = __ldg(reinterpret_cast<const float4*>(M.trec + 64 * (int64_t)t) + 8 + f);
+        const int nt = __float_as_int(sh.w);
         if (nt < 0) break;
-        float dx = __ldg(rec + 32 + 3 * f), dy = __ldg(rec + 33 + 3 * f), dz = __ldg(rec + 34 + 3 * f);
+        const float dx = sh.x, dy = sh.y, dz = sh.z;
         qx += dx; qy += dy; qz += dz;
         ox += dx; oy += dy; oz += dz;
         t = nt;
@@ -142,15 +149,13 @@ static __device__ __noinline__ Reloc relocate_f(const MeshView& M, int cur, floa
     return Reloc{tt, (float)(px - on.x), (float)(py - on.y), (float)(pz - on.z), sx + dx, sy + dy, sz + dz};
 }
 
-// Deposit along start -> end (both FP32 offsets from the origin of t) into t: the sample
-// points that lie in t (the sub-step changed tet), summed in FP32 per node, then converted
-// once to fixed point.
+// Deposit along start -> end (both FP32 offsets from the origin of t) into t, whose inverse
+// Jacobian the caller holds in j: the sample points that lie in t (the sub-step changed tet),
+// summed in FP32 per node, then converted once to fixed point.
 __device__ __forceinline__ void deposit_traj_f(const MeshView& M, const SpeciesDev& S, const PushParams& pp, int t,
-                                               float sx, float sy, float sz, float rx, float ry, float rz,
-                                               ChargeAcc A)
+                                               const float j[9], float sx, float sy, float sz, float rx, float ry,
+                                               float rz, ChargeAcc A)
 {
-    float j[9];
-    load_j(M, t, j);
     float sum[4] = {0.f, 0.f, 0.f, 0.f};
     double cw = S.cw_seg;
     bool any = false;
@@ -218,9 +223,10 @@ __device__ __forceinline__ void deposit_traj_f(const MeshView& M, const SpeciesD
         }
     }
     if (!any) return;
-    const int* nd = reinterpret_cast<const int*>(M.trec + 64 * (int64_t)t + 21);
+    const int4 nd4 = node_ids(M, t);
+    const int nd[4] = {nd4.x, nd4.y, nd4.z, nd4.w};
     for (int k = 0; k < 4; ++k) {
-        int node = __ldg(nd + k);
+        int node = nd[k];
         fx_red_word(A, node, (cw * (double)sum[k]) * pp.inv_uq);
     }
 }
@@ -285,14 +291,15 @@ __device__ __forceinline__ int advance_f(const MeshView& M, const SpeciesDev& S,
                 if (in) {
                     float tx = f.rx - sx, ty = f.ry - sy, tz = f.rz - sz;
                     bool tiny = sqrtf(tx * tx + ty * ty + tz * tz) < 1e-15f;
+                    const int4 nd4 = __ldg(reinterpret_cast<const int4*>(rec) + 6);
+                    const int nd[4] = {nd4.x, nd4.y, nd4.z, nd4.w};
 #pragma unroll
                     for (int q = 0; q < 4; ++q) {
                         float lk = tiny ? l[q] : (pp.dep_kernel == 0 ? le[q] : 0.5f * (l[q] + le[q]));
-                        const int nd = __float_as_int(__ldg(reinterpret_cast<const float*>(rec) + 21 + q));
-                        fx_red_word(A, nd, (qw * (double)lk) * pp.inv_uq);
+                        fx_red_word(A, nd[q], (qw * (double)lk) * pp.inv_uq);
                     }
                 } else {
-                    deposit_traj_f(M, S, pp, f.cur, sx, sy, sz, f.rx, f.ry, f.rz, A);
+                    deposit_traj_f(M, S, pp, f.cur, J, sx, sy, sz, f.rx, f.ry, f.rz, A);
                 }
             }
 #pragma unroll
@@ -307,7 +314,7 @@ __device__ __forceinline__ int advance_f(const MeshView& M, const SpeciesDev& S,
             f.cur = nt;
             rec = reinterpret_cast<const float4*>(M.trec + 64 * (int64_t)nt);
             load_j(M, nt, J);
-            if (pp.deposit) deposit_traj_f(M, S, pp, nt, sx, sy, sz, f.rx, f.ry, f.rz, A);
+            if (pp.deposit) deposit_traj_f(M, S, pp, nt, J, sx, sy, sz, f.rx, f.ry, f.rz, A);
             baryj(J, f.rx, f.ry, f.rz, l);
             in = inside_f(l);
         }
@@ -485,11 +492,12 @@ __device__ __forceinline__ int advance_stay_f(const MeshView& M, const SpeciesDe
         const double qw = S.q * S.w;
         const float tx = rx - f.rx, ty = ry - f.ry, tz = rz - f.rz;
         const bool tiny = sqrtf(tx * tx + ty * ty + tz * tz) < 1e-15f;
+        const int4 nd4 = __ldg(reinterpret_cast<const int4*>(rec) + 6);
+        const int nd[4] = {nd4.x, nd4.y, nd4.z, nd4.w};
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             const float lk = tiny ? l[q] : (pp.dep_kernel == 0 ? le[q] : 0.5f * (l[q] + le[q]));
-            const int nd = __float_as_int(__ldg(reinterpret_cast<const float*>(rec) + 21 + q));
-            fx_red_word(A, nd, (qw * (double)lk) * pp.inv_uq);
+            fx_red_word(A, nd[q], (qw * (double)lk) * pp.inv_uq);
         }
     }
     f.rx = rx; f.ry = ry; f.rz = rz;
@@ -603,10 +611,12 @@ __global__ void __launch_bounds__(256, 6) k_push_mixed(const __grid_constant__ M
     warp_stats_flush(L, ke_acc, S.vmax);
 }
 
-// Stay-first pass 1 (same work distribution as k_push_mixed); no walk code, so it needs far
-// fewer registers: 6 blocks of 256 per SM at 40 registers spill 64 bytes a thread, against 456
-// for the walking pass 1.
-__global__ void __launch_bounds__(256, 6) k_push_mixed_stay(const __grid_constant__ MeshView M, ParticleStore P,
+// Stay-first pass 1 (same work distribution as k_push_mixed); no walk code, so at 4 blocks of
+// 256 per SM it fits in 62 registers without spilling.  Its launch is bound by L1 wavefronts
+// (scattered record loads, one atomic per lane and node), so the spills of a denser launch cost
+// more than its extra warps gain: 4 blocks 37.66 ms of push per step at 128^3, 5 blocks
+// 38.5, 6 blocks (40 registers, 200 bytes of spill stores) 38.83.
+__global__ void __launch_bounds__(256, 4) k_push_mixed_stay(const __grid_constant__ MeshView M, ParticleStore P,
                                                          const __grid_constant__ SortedSource R,
                                                          const __grid_constant__ SpeciesDev S,
                                                          const __grid_constant__ PushParams pp, DeferList D,

@@ -290,3 +290,37 @@ def test_null_collision_law(orc):
     # the two modes draw from different streams, so their collision sets differ
     _, h1 = orc.mcc(v, idx, status, ids, sp, proc, dt, 77, 3, mode=1)
     assert h1 > 1000
+
+
+def test_csv_export_matches_reference_exporter(ref, tmp_path):
+    """scdat_export_columns_csv against the reference's own CSVExporter::exportDataSet
+    (Tools/Output/src/CSVExporter.cpp:11-47) on the same columnar data: byte-identical files,
+    series in name order, the parent directories created, signed zeros, extreme exponents and
+    non-finite values written alike; a repeated name keeps its last series, as std::map does."""
+    from scdat_b200 import build, capi
+
+    build.build()  # host code: runs without a GPU
+    rng = np.random.default_rng(11)
+    n = 57
+    axis = np.linspace(-0.5, 1.25, n)
+    series = {"potential_v": rng.normal(0.0, 3.0, n), "electron_density_m3": 10 ** rng.uniform(6, 18, n),
+              "Z_upper": rng.normal(0.0, 1e-300, n), "a_first": rng.uniform(-1, 1, n) * 1e300,
+              "electric_field_z_v_per_m": rng.normal(0.0, 1e3, n)}
+    series["potential_v"][[0, 3, 5]] = [-0.0, np.inf, np.nan]
+    series["a_first"][7] = -np.inf
+    for k, (name, vals) in enumerate([("index", series), ("z_m", {"only": axis * 2.0}), ("node", {})]):
+        ours, theirs = tmp_path / f"ours{k}" / "sub" / "t.csv", tmp_path / f"ref{k}" / "sub" / "t.csv"
+        capi.export_columns_csv(ours, name, axis, vals)
+        assert ref.csv_export(theirs, name, axis, vals)
+        assert ours.read_bytes() == theirs.read_bytes()
+    # a repeated name: ours is given the pair list, the reference's map keeps the last assignment
+    L = capi.load()
+    import ctypes as C
+
+    a = np.ascontiguousarray(axis)
+    v1, v2 = np.ones(n), np.full(n, 2.0)
+    names = (C.c_char_p * 2)(b"dup", b"dup")
+    vals = (C.c_void_p * 2)(v1.ctypes.data, v2.ctypes.data)
+    assert L.scdat_export_columns_csv(str(tmp_path / "dup.csv").encode(), b"x", n, a.ctypes.data, 2, names, vals) == 0
+    assert ref.csv_export(tmp_path / "dup_ref.csv", "x", axis, {"dup": v2})
+    assert (tmp_path / "dup.csv").read_bytes() == (tmp_path / "dup_ref.csv").read_bytes()
