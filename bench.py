@@ -228,9 +228,9 @@ def alg_bytes_push(dom, precision, particles):
 # DRAM bytes per stored particle of one step's push launches (all passes, both species; the
 # electrons' pass 1 includes the gather of their re-sort): an ncu capture (dram__bytes_read.sum +
 # dram__bytes_write.sum) of one step's six push launches on a 64^3-cell box at 64 ppc per species
-# (31.9 M particles, 9.52 GB), divided by the particles; the full workload has the same density
+# (31.9 M particles, 7.16 GB), divided by the particles; the full workload has the same density
 # and access pattern.  None: not measured for the form.
-PUSH_DRAM_BYTES_PER_PARTICLE = {1: 298.6, 0: None}
+PUSH_DRAM_BYTES_PER_PARTICLE = {1: 224.6, 0: None}
 
 
 def cg_iteration_bytes(dom, precision):

@@ -7,9 +7,10 @@
 // so a sub-step inside the tet reads one cache line; in its second, per face the FP32 origin
 // shift to the neighbour with the neighbour's id, which the walk reads.  Gather, adaptive
 // sub-step, Boris and the in-tet test run in FP32; a move into a face neighbour is re-based in
-// FP32 by the stored shift; a walk that meets a boundary face or runs long reconstructs the FP64
-// absolute position and uses the FP64 locate.  Deposit weights are FP32 barycentrics promoted to FP64 before the exact
-// fixed-point accumulation (one 64-bit word per node, fx_red_word).
+// FP32 by the stored shift; a walk that meets a boundary face or runs long reconstructs the
+// FP64 absolute position and uses the FP64 locate.  Deposit weights are FP32 barycentrics
+// promoted to FP64 before the exact fixed-point accumulation (one 64-bit word per node,
+// fx_red_word).
 //
 // Sub-steps run in passes so that warps stay converged: pass 1 gives every particle at most
 // kCap1 sub-steps and appends the unfinished ones to a list; pass 2 gives those up to kCap2
@@ -89,16 +90,6 @@ __device__ __forceinline__ double3 origin(const MeshView& M, int t)
 {
     int o = __ldg(&M.tet[t].x);
     return make_double3(__ldg(M.xyz + 3 * o), __ldg(M.xyz + 3 * o + 1), __ldg(M.xyz + 3 * o + 2));
-}
-
-__device__ __forceinline__ void dep_point_f(Fx128 acc[4], bool& any, const float l[4], double cw, double inv_uq)
-{
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        Fx128 f = fx_from_double((cw * (double)l[i]) * inv_uq);
-        fx_add(acc[i], f);
-    }
-    any = true;
 }
 
 // Result of a relocation: the new tet (or -1), the offset r and the carried start offset s
@@ -591,9 +582,11 @@ __device__ __forceinline__ void push_more_warp(const MeshView& M, const Particle
 
 // Pass 1: every stored particle.  Warps take runs of kRun 32-particle chunks from the launch's
 // work counter until none are left, so no warp idles while another still has work.
-// 6 blocks of 256 per SM (40 registers): the extra warps hide more of the walk's load latency
-// than the extra spills cost (4 blocks: 46.2 ms, 5: 47.7, 6: 45.3, 8: 47.5 per step at 128^3)
-__global__ void __launch_bounds__(256, 6) k_push_mixed(const __grid_constant__ MeshView M, ParticleStore P,
+// 5 blocks of 256 per SM (48 registers): with the record's vector loads and the folded re-sort
+// gather, the fewer spills now pay more than the sixth block's warps (push per step at 128^3:
+// 5 blocks 35.97 ms, 6 blocks 36.92, 4 blocks 40.2; the walk inlined: 36.11 at 6 blocks,
+// 37.56 at 5).
+__global__ void __launch_bounds__(256, 5) k_push_mixed(const __grid_constant__ MeshView M, ParticleStore P,
                                                     const __grid_constant__ SortedSource R,
                                                     const __grid_constant__ SpeciesDev S,
                                                     const __grid_constant__ PushParams pp, DeferList D, ChargeAcc A,
