@@ -241,12 +241,19 @@ typedef struct {
 } scdat_surface_circuit;
 SCDAT_API int scdat_set_surface_circuit(scdat_ctx* ctx, const scdat_surface_circuit* sc);
 /* Secondary emission of electrons collected by the body (needs the surface circuit):
- * model 1 is Sternglass's universal yield 7.4 dmax (E/Emax) exp(-2 sqrt(E/Emax)), model 2 the
- * reference's legacyWhippleYield (Tools/Material/src/SurfaceMaterialModel.cpp:231-244), 0 off.
+ * model 1 is Sternglass's universal yield 7.4 dmax (E/Emax) exp(-2 sqrt(E/Emax)); models 2, 3
+ * and 4 the reference's legacy yields as evaluateLegacySecondaryElectronYield computes them
+ * (Tools/Material/src/SurfaceMaterialModel.cpp:619-637): 2 legacyWhippleYield (:231-244),
+ * 3 legacySimsYield (:246-273), 4 legacyKatzYield (:275-302); 0 off.
  * The emitted charge delta |q| w of each collected electron returns to its face as current and
  * is recorded in ledger row 6 as emitted electron charge (no secondary macro-particles are
  * created). */
 SCDAT_API int scdat_set_secondary_emission(scdat_ctx* ctx, int32_t model, double delta_max, double e_max_ev);
+/* The shape parameters of the legacy yields: the Sims exponent n (the reference's default 1.6;
+ * values below 1.05 act as 1.05, as in the reference) and the Katz range coefficients
+ * {r1, n1, r2, n2} (NULL: the reference's defaults {0.85, 0.35, 0.12, 1.05}, the material
+ * scalars katz_r1, katz_n1, katz_r2, katz_n2). */
+SCDAT_API int scdat_set_secondary_yield_params(scdat_ctx* ctx, double sims_exponent_n, const double* katz);
 /* Face potentials [6], collected charge [6], last-step current [6] and the number of particles
  * collected so far [6]; any pointer may be NULL. */
 SCDAT_API int scdat_get_surface_state(scdat_ctx* ctx, double* V, double* Q, double* I, int64_t* counts);

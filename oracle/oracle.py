@@ -13,6 +13,7 @@ from __future__ import annotations
 
 import contextlib
 import ctypes as C
+import math
 import os
 import subprocess
 from dataclasses import dataclass, field
@@ -475,6 +476,8 @@ class Reference:
         L.ref_circuit_advance.restype = C.c_int
         L.ref_whipple_yield.argtypes = [C.c_double, C.c_double, C.c_int, _dp, _dp]
         L.ref_whipple_yield.restype = None
+        L.ref_legacy_yield.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, C.c_void_p, C.c_int, _dp, _dp]
+        L.ref_legacy_yield.restype = None
         L.ref_parse_cross_section_set.argtypes = [C.c_char_p]
         L.ref_parse_cross_section_set.restype = C.c_int
         L.ref_estimate_densities.argtypes = [C.c_int64, _i32p, _dp, _dp, _u8p, C.c_double, _dp, _dp]
@@ -640,6 +643,15 @@ class Reference:
         a = np.ascontiguousarray(axis, np.float64)
         return self.L.ref_csv_export(str(path).encode(), axis_name.encode(), len(a), a, len(names), cn, cv) == 0
 
+    def legacy_yield(self, model, peak_yield, peak_energy_ev, e_ev, sims_n=1.6, katz=None):
+        """evaluateLegacySecondaryElectronYield, model "whipple", "sims" or "katz"."""
+        e = np.ascontiguousarray(e_ev, np.float64)
+        out = np.zeros(len(e))
+        k = None if katz is None else np.ascontiguousarray(katz, np.float64)
+        self.L.ref_legacy_yield({"whipple": 0, "sims": 1, "katz": 2}[model], float(peak_yield), float(peak_energy_ev),
+                                float(sims_n), None if k is None else k.ctypes.data, len(e), e, out)
+        return out
+
     def parse_cross_section_set(self, text):
         """Collision::parseCollisionCrossSectionSetId: -1 unknown, else the set's index."""
         return int(self.L.ref_parse_cross_section_set(text.encode()))
@@ -676,12 +688,46 @@ def body_face_of(x, blo, bhi):
     return np.argmin(d, axis=1)
 
 
-def see_yield(model, dmax, emax, e_ev):
-    """Secondary-electron yield: 1 Sternglass 7.4 dmax (E/Emax) exp(-2 sqrt(E/Emax)); 2 the
-    reference's legacyWhippleYield (Tools/Material/src/SurfaceMaterialModel.cpp:231-244)."""
+def sims_xm(n):
+    """The root xm of the Sims yield for exponent n, by legacySimsYield's own grid search
+    (Tools/Material/src/SurfaceMaterialModel.cpp:252-263)."""
+    for i in range(1, 10001):
+        x = 0.5 + i * (2.5 - 0.5) / 10000.0
+        if abs(x - (1.0 - 1.0 / n) * (math.exp(x) - 1.0)) <= 1.0e-3:
+            return x
+    return 2.5
+
+
+def see_yield(model, dmax, emax, e_ev, sims_n=1.6, katz=(0.85, 0.35, 0.12, 1.05)):
+    """Secondary-electron yield: 1 Sternglass 7.4 dmax (E/Emax) exp(-2 sqrt(E/Emax)); the
+    reference's legacy yields (Tools/Material/src/SurfaceMaterialModel.cpp): 2 legacyWhippleYield
+    (:231-244), 3 legacySimsYield (:246-273), 4 legacyKatzYield (:275-302)."""
     e = np.asarray(e_ev, float)
     out = np.zeros_like(e)
     ok = (e > 0) & (dmax > 0)
+    if model == 3:
+        n = max(1.05, sims_n)
+        xm = sims_xm(n)
+        ep = max(1.0, emax)
+        ok &= e > 10.0
+        x = xm * (e[ok] / ep) ** n
+        good = (x > 1e-12) & (abs(1.0 - math.exp(-xm)) >= 1e-12)
+        xs = np.where(good, x, 1.0)
+        out[ok] = np.where(good, dmax / (1.0 - math.exp(-xm)) * (ep / e[ok]) ** (n - 1.0) * 2.0
+                           * (xs + np.exp(-xs) - 1.0) / xs, 0.0)
+        return out
+    if model == 4:
+        ok = (e > 1e-9) & (dmax > 0)
+        ep = max(1.0, emax)
+        r1, n1, r2, n2 = katz
+        ek, pk = e[ok] * 1e-3, ep * 1e-3
+        rng = r1 * ek ** n1 + r2 * ek ** n2
+        prng = r1 * pk ** n1 + r2 * pk ** n2
+        good = (rng > 1e-12) & (prng > 1e-12)
+        att = np.exp(-(rng / prng - 1.0) ** 2)
+        roll = 1.0 / (1.0 + (e[ok] / max(1.0, 3.0 * ep)) ** 0.7)
+        out[ok] = np.where(good, dmax * att * (0.55 + 0.45 * roll), 0.0)
+        return out
     if model == 1:
         r = e[ok] / emax
         out[ok] = 7.4 * dmax * r * np.exp(-2.0 * np.sqrt(r))

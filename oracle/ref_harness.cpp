@@ -443,6 +443,26 @@ void ref_whipple_yield(double peak_yield, double peak_energy_ev, int n, const do
             mat, SCDAT::Material::LegacySecondaryYieldModel::Whipple, e_ev[k]);
 }
 
+// evaluateLegacySecondaryElectronYield for model 0 Whipple, 1 Sims (exponent sims_n), 2 Katz
+// (range coefficients katz4 = r1, n1, r2, n2 as material scalars; NULL: the material defaults).
+void ref_legacy_yield(int model, double peak_yield, double peak_energy_ev, double sims_n, const double* katz4, int n,
+                      const double* e_ev, double* out)
+{
+    SCDAT::Material::MaterialProperty mat;
+    mat.setSecondaryElectronYield(peak_yield);
+    mat.setScalarProperty("secondary_yield_peak_energy_ev", peak_energy_ev);
+    if (katz4) {
+        mat.setScalarProperty("katz_r1", katz4[0]);
+        mat.setScalarProperty("katz_n1", katz4[1]);
+        mat.setScalarProperty("katz_r2", katz4[2]);
+        mat.setScalarProperty("katz_n2", katz4[3]);
+    }
+    const auto m = model == 0 ? SCDAT::Material::LegacySecondaryYieldModel::Whipple
+                   : model == 1 ? SCDAT::Material::LegacySecondaryYieldModel::Sims
+                                : SCDAT::Material::LegacySecondaryYieldModel::Katz;
+    for (int k = 0; k < n; ++k) out[k] = SCDAT::Material::evaluateLegacySecondaryElectronYield(mat, m, e_ev[k], sims_n);
+}
+
 // Collision::parseCollisionCrossSectionSetId: -1 for an unknown name, else the set's index.
 int ref_parse_cross_section_set(const char* text)
 {

@@ -97,6 +97,7 @@ EXPORTS = ["scdat_default_params", "scdat_create", "scdat_destroy", "scdat_last_
            "scdat_batch_step", "scdat_batch_set_tuning", "scdat_batch_get_tuning", "scdat_batch_autotune",
            "scdat_batch_last_step_ms", "scdat_batch_stream", "scdat_batch_kernel_launches",
            "scdat_set_surface_circuit", "scdat_get_surface_state", "scdat_set_secondary_emission",
+           "scdat_set_secondary_yield_params",
            "scdat_sample_with_derivative", "scdat_adjoint_window", "scdat_seed_tet_particles",
            "scdat_export_layer_profile_csv", "scdat_export_nodes_csv", "scdat_export_columns_csv"]
 
@@ -137,6 +138,7 @@ def load():
     L.scdat_set_surface_circuit.argtypes = [vp, C.POINTER(SurfaceCircuitC)]
     L.scdat_get_surface_state.argtypes = [vp, vp, vp, vp, vp]
     L.scdat_set_secondary_emission.argtypes = [vp, C.c_int32, C.c_double, C.c_double]
+    L.scdat_set_secondary_yield_params.argtypes = [vp, C.c_double, vp]
     L.scdat_seed_tet_particles.argtypes = [vp, C.c_int32, C.c_int64, vp, C.c_int32, C.c_double, vp, C.c_uint64]
     L.scdat_export_layer_profile_csv.argtypes = [vp, C.c_char_p, C.c_int32]
     L.scdat_export_nodes_csv.argtypes = [vp, C.c_char_p]
@@ -371,8 +373,14 @@ class Domain:
         self._ck(self.L.scdat_set_surface_circuit(self.h, C.byref(sc)))
 
     def set_secondary_emission(self, model, delta_max=2.0, e_max_ev=300.0):
-        """model: 0 off, 1 Sternglass, 2 Whipple (the reference's legacy form)."""
+        """model: 0 off, 1 Sternglass, 2 Whipple, 3 Sims, 4 Katz (the reference's legacy forms)."""
         self._ck(self.L.scdat_set_secondary_emission(self.h, int(model), float(delta_max), float(e_max_ev)))
+
+    def set_secondary_yield_params(self, sims_exponent_n=1.6, katz=None):
+        """Sims exponent and Katz range coefficients (r1, n1, r2, n2; None: the defaults)."""
+        k = None if katz is None else np.ascontiguousarray(katz, np.float64)
+        assert k is None or k.shape == (4,)
+        self._ck(self.L.scdat_set_secondary_yield_params(self.h, float(sims_exponent_n), _p(k)))
 
     def surface_state(self):
         V, Q, I = np.zeros(6), np.zeros(6), np.zeros(6)

@@ -182,6 +182,9 @@ PushParams push_params(const scdat_ctx* ctx, bool do_mcc)
     pp.see_model = ctx->see_model;
     pp.see_dmax = ctx->see_dmax;
     pp.see_emax_ev = ctx->see_emax;
+    pp.see_sims_n = ctx->see_sims_n;
+    pp.see_sims_xm = ctx->see_sims_xm;
+    for (int k = 0; k < 4; ++k) pp.see_katz[k] = ctx->see_katz[k];
     for (int a = 0; a < 3; ++a) {
         pp.blo[a] = ctx->body_lo[a];
         pp.bhi[a] = ctx->body_hi[a];
@@ -1521,10 +1524,40 @@ SCDAT_API int scdat_set_surface_circuit(scdat_ctx* ctx, const scdat_surface_circ
     return SCDAT_OK;
 }
 
+// The Sims yield's xm for exponent n, as legacySimsYield finds it (SurfaceMaterialModel.cpp:252-263):
+// the first of 10000 grid points x in (0.5, 2.5] within 1e-3 of (1 - 1/n)(e^x - 1), else 2.5.
+static double sims_xm(double n)
+{
+    double xm = 2.5;
+    for (int i = 1; i < 10001; ++i) {
+        const double x = 0.5 + (double)i * (2.5 - 0.5) / 10000.0;
+        const double y = (1.0 - 1.0 / n) * (std::exp(x) - 1.0);
+        if (std::fabs(x - y) <= 1.0e-3) {
+            xm = x;
+            break;
+        }
+    }
+    return xm;
+}
+
+SCDAT_API int scdat_set_secondary_yield_params(scdat_ctx* ctx, double sims_exponent_n, const double* katz)
+{
+    if (!ctx) return SCDAT_ERR_ARG;
+    ARG(std::isfinite(sims_exponent_n), "non-finite Sims exponent");
+    if (katz)
+        for (int k = 0; k < 4; ++k) ARG(std::isfinite(katz[k]), "non-finite Katz coefficient");
+    ctx->see_sims_n = std::max(1.05, sims_exponent_n);
+    ctx->see_sims_xm = sims_xm(ctx->see_sims_n);
+    const double dflt[4] = {0.85, 0.35, 0.12, 1.05};
+    for (int k = 0; k < 4; ++k) ctx->see_katz[k] = katz ? katz[k] : dflt[k];
+    return SCDAT_OK;
+}
+
 SCDAT_API int scdat_set_secondary_emission(scdat_ctx* ctx, int32_t model, double delta_max, double e_max_ev)
 {
     if (!ctx) return SCDAT_ERR_ARG;
-    ARG(model >= 0 && model <= 2, "model: 0 off, 1 Sternglass, 2 Whipple");
+    ARG(model >= 0 && model <= 4, "model: 0 off, 1 Sternglass, 2 Whipple, 3 Sims, 4 Katz");
+    if (ctx->see_sims_xm == 0.0) ctx->see_sims_xm = sims_xm(ctx->see_sims_n);
     ARG(model == 0 || (delta_max >= 0.0 && e_max_ev > 0.0), "yield needs delta_max >= 0 and e_max > 0");
     ctx->see_model = model;
     ctx->see_dmax = delta_max;

@@ -264,9 +264,11 @@ struct PushParams {
     // surface circuit: particles lost into the body box [blo, bhi] are tallied per face
     int32_t patches;
     int32_t see_model;       // secondary emission of electrons collected by the body: 0 off,
-                             // 1 Sternglass, 2 Whipple (legacyWhippleYield)
+                             // 1 Sternglass, 2 Whipple, 3 Sims, 4 Katz (the legacy yields)
     double blo[3], bhi[3];
     double see_dmax, see_emax_ev;
+    double see_sims_n, see_sims_xm;  // Sims: exponent (>= 1.05) and the root xm it implies
+    double see_katz[4];              // Katz: range coefficients r1, n1, r2, n2
 };
 
 }  // namespace scdat

@@ -174,6 +174,8 @@ struct scdat_ctx {
     bool surface = false;
     int see_model = 0;
     double see_dmax = 0.0, see_emax = 300.0;
+    double see_sims_n = 1.6, see_sims_xm = 0.0;  // xm set with the exponent
+    double see_katz[4] = {0.85, 0.35, 0.12, 1.05};
     double body_lo[3] = {0, 0, 0}, body_hi[3] = {0, 0, 0};
     DBuf<SurfaceDev> surf;
     DBuf<int32_t> surf_node;

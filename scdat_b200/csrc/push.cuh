@@ -241,6 +241,25 @@ __device__ inline double see_yield(const PushParams& pp, double e_ev)
         const double r = e_ev / pp.see_emax_ev;
         return 7.4 * pp.see_dmax * r * exp(-2.0 * sqrt(r));
     }
+    if (pp.see_model == 3) {  // legacySimsYield (SurfaceMaterialModel.cpp:246-273)
+        if (e_ev <= 10.0) return 0.0;
+        const double ep = fmax(1.0, pp.see_emax_ev), n = pp.see_sims_n, xm = pp.see_sims_xm;
+        const double x = xm * pow(e_ev / ep, n);
+        if (x <= 1.0e-12 || fabs(1.0 - exp(-xm)) < 1.0e-12) return 0.0;
+        return pp.see_dmax / (1.0 - exp(-xm)) * pow(ep / e_ev, n - 1.0) * 2.0 * (x + exp(-x) - 1.0) / x;
+    }
+    if (pp.see_model == 4) {  // legacyKatzYield (SurfaceMaterialModel.cpp:275-302)
+        if (e_ev <= 1.0e-9) return 0.0;
+        const double ep = fmax(1.0, pp.see_emax_ev);
+        const double ek = e_ev * 1.0e-3, pk = ep * 1.0e-3;
+        const double* k = pp.see_katz;
+        const double range = k[0] * pow(ek, k[1]) + k[2] * pow(ek, k[3]);
+        const double peak_range = k[0] * pow(pk, k[1]) + k[2] * pow(pk, k[3]);
+        if (range <= 1.0e-12 || peak_range <= 1.0e-12) return 0.0;
+        const double att = exp(-pow(range / peak_range - 1.0, 2.0));
+        const double roll = 1.0 / (1.0 + pow(e_ev / fmax(1.0, 3.0 * ep), 0.7));
+        return pp.see_dmax * att * (0.55 + 0.45 * roll);
+    }
     const double ep = fmax(1.0, pp.see_emax_ev);
     const double q = 2.28 * pow(e_ev / ep, 1.35);
     if (q <= 1.0e-12) return 0.0;

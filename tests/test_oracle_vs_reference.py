@@ -324,3 +324,31 @@ def test_csv_export_matches_reference_exporter(ref, tmp_path):
     assert L.scdat_export_columns_csv(str(tmp_path / "dup.csv").encode(), b"x", n, a.ctypes.data, 2, names, vals) == 0
     assert ref.csv_export(tmp_path / "dup_ref.csv", "x", axis, {"dup": v2})
     assert (tmp_path / "dup.csv").read_bytes() == (tmp_path / "dup_ref.csv").read_bytes()
+
+
+@pytest.mark.parametrize("model", ["sims", "katz"])
+def test_legacy_sims_katz_yields_match_reference(ref, model):
+    """The oracle's (and the device's) Sims and Katz secondary yields against the reference's
+    evaluateLegacySecondaryElectronYield over 0-20 keV, several peak yields and energies, and
+    several Sims exponents (below the 1.05 floor too) and Katz range coefficients."""
+    e = np.concatenate([[0.0, 1e-12, 1e-9, 0.5, 9.999, 10.0, 10.001], np.geomspace(1e-3, 50.0, 60),
+                        np.linspace(50.0, 2e4, 400)])
+    shapes = [dict(sims_n=n) for n in (0.9, 1.05, 1.35, 1.6, 2.2)] if model == "sims" else \
+        [dict(katz=k) for k in ((0.85, 0.35, 0.12, 1.05), (1.2, 0.5, 0.05, 1.4), (0.4, 0.2, 0.3, 0.9))]
+    num = 3 if model == "sims" else 4
+    for peak_yield in (0.0, 0.7, 2.0, 3.5):
+        for peak_e in (0.3, 50.0, 300.0, 800.0):
+            for sh in shapes:
+                mine = O.see_yield(num, peak_yield, peak_e, e, **sh)
+                theirs = ref.legacy_yield(model, peak_yield, peak_e, e, **sh)
+                assert np.array_equal(mine == 0.0, theirs == 0.0), (peak_yield, peak_e, sh)
+                if model == "sims":
+                    # the numerator x + e^-x - 1 ~ x^2/2 cancels for small x = xm (E/Emax)^n, so
+                    # an ulp of exp grows by ~2/x^2: the bar is 1e-12 or that condition number
+                    # times a few ulps, whichever is larger
+                    n = max(1.05, sh["sims_n"])
+                    x = O.sims_xm(n) * (e / max(1.0, peak_e)) ** n
+                    bar = np.maximum(1e-12, 1e-15 * 2.0 / np.maximum(x * x, 1e-300))
+                else:
+                    bar = np.full_like(e, 1e-12)
+                assert np.all(np.abs(mine - theirs) <= bar * np.abs(theirs)), (peak_yield, peak_e, sh)
