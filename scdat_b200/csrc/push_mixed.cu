@@ -628,7 +628,8 @@ __global__ void __launch_bounds__(256, 4) k_push_mixed_stay(const __grid_constan
     warp_stats_flush(L, ke_acc, S.vmax);
 }
 
-// Passes 2 and 3.
+// Passes 2 and 3, 4 blocks of 256 per SM (64 registers; push per step at 128^3: 4 blocks 36.32
+// ms, 3 blocks 36.46, 5 blocks 36.55).
 __global__ void __launch_bounds__(256, 4) k_push_mixed_more(const __grid_constant__ MeshView M, ParticleStore P,
                                                          const __grid_constant__ SpeciesDev S,
                                                          const __grid_constant__ PushParams pp, DeferList Din,
