@@ -62,6 +62,28 @@ def test_single_scenario_batch_is_bitwise_the_single_step(lib):
     assert steps == 3
 
 
+def test_batch_over_a_pending_resort_is_bitwise_the_single_step(lib):
+    """A context whose last step re-sorted (the precision form leaves that re-sort's gather to
+    the next push) joins a batch, which gathers the store first: two more steps in the batch
+    give bitwise what four steps of the context alone give, where the third step's push read
+    the store through the permutation."""
+    from scdat_b200 import capi
+
+    dom, sp, parts = _scenario(0)
+    dom.step(4)
+    ref = _state(dom, sp, parts)
+    dom.close()
+    dom, sp, parts = _scenario(0)
+    dom.step(2)  # sort_interval 2: re-sorted after the second step
+    b = capi.Batch([dom])
+    b.step(2)
+    got = _state(dom, sp, parts)
+    b.close()
+    dom.close()
+    for key in ("rho", "phi", "E", "ledger", "x", "v", "tet", "status"):
+        assert np.array_equal(np.nan_to_num(got[key]), np.nan_to_num(ref[key])), key
+
+
 def test_batch_of_uneven_scenarios_matches_single_steps(lib):
     from scdat_b200 import capi
 
