@@ -553,10 +553,9 @@ def run_batched(args, cfg):
     errs = []
     for d, p64 in zip(doms, phi64):
         errs.append(float(np.abs(d.fields()[1] - p64).max() / max(np.abs(p64).max(), 1e-300)))
-    # the worst scenario's FP64 form against itself with one velocity moved by one ulp, over the
-    # same steps: how far two FP64 runs drift apart on their own
-    # and against itself started from FP32-rounded velocities (the precision form's initial
-    # rounding, FP64 arithmetic after it)
+    # controls on the worst scenario, each an FP64 run over the same steps against the FP64 run:
+    # one velocity moved by one ulp (how far two FP64 runs drift apart on their own), and every
+    # velocity rounded to FP32 (the precision form's initial rounding, FP64 arithmetic after it)
     kw = int(np.argmax(errs))
     worst = dict(index=kw, error=errs[kw], scenario={k: scen[kw][k] for k in ("n", "bias", "density", "te", "ti", "ppc")})
     for name, perturb in (("fp64_vs_fp64_nudged", nudge_one_velocity), ("fp64_vs_fp64_v32", round_velocities_fp32)):
