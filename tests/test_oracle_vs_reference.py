@@ -352,3 +352,25 @@ def test_legacy_sims_katz_yields_match_reference(ref, model):
                 else:
                     bar = np.full_like(e, 1e-12)
                 assert np.all(np.abs(mine - theirs) <= bar * np.abs(theirs)), (peak_yield, peak_e, sh)
+
+
+def test_sampler_fixture_is_the_reference_sampler(ref):
+    """tests/golden/sampler_ref.npz (the GPU sampler test's reference) is what the reference's
+    PicMccSurfaceCurrentSampler gives here: its plate mesh and its sampleWithDerivative output
+    at both potentials, reproduced exactly from the recorded configuration and seed."""
+    import os
+
+    from golden.make_golden import SAMPLER, SAMPLER_POTENTIALS
+
+    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "sampler_ref.npz"))
+    c = SAMPLER
+    xyz, tet = ref.sampler_mesh(c["area_m2"], c["aspect"], c["gap_m"], c["z_layers"])
+    assert np.array_equal(xyz, g["xyz"]) and np.array_equal(tet, g["tet"])
+    assert np.array_equal(g["potentials"], np.array(SAMPLER_POTENTIALS))
+    for v, row in zip(SAMPLER_POTENTIALS, g["samples"]):
+        out = ref.sampler_sample(c["area_m2"], c["gap_m"], c["z_layers"], c["ppe"], c["window_steps"], c["seed"],
+                                 c["ne"], c["ni"], c["te_ev"], c["ti_ev"], c["ion_amu"], v, c["reference_v"],
+                                 c["probe_dv"])
+        assert out["valid"] == 1.0
+        got = [out[k] for k in ("electron", "ion", "emitted", "net", "derivative", "segments")]
+        assert np.array_equal(np.array(got), row), v
