@@ -5,6 +5,7 @@ import pytest
 
 import oracle as O
 from conftest import rel_err
+from golden.make_golden import CASES
 from pic_helpers import oracle_cycle, oracle_mcc_run
 
 
@@ -374,3 +375,51 @@ def test_sampler_fixture_is_the_reference_sampler(ref):
         assert out["valid"] == 1.0
         got = [out[k] for k in ("electron", "ion", "emitted", "net", "derivative", "segments")]
         assert np.array_equal(np.array(got), row), v
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_golden_fixtures_are_the_reference(ref, name):
+    """Each small-case fixture in tests/golden (the GPU parity tests' reference values) is what
+    the reference's own code gives here from the recorded inputs: Laplace solve, frozen-field
+    push, charged solve and the full cycle, reproduced exactly."""
+    import os
+
+    from golden.make_golden import make_inputs
+
+    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", f"{name}.npz"))
+    mesh, sp, parts, dt, nsteps, face_bc = make_inputs(name)
+    phi_l, E_l = ref.poisson(mesh, np.zeros(mesh.N), mesh.phi_bc)
+    push = ref.push(mesh, E_l, parts, sp, dt)
+    phi_q, E_q = ref.poisson(mesh, push["rho"], mesh.phi_bc)
+    cyc = ref.cycle(mesh, parts, sp, nsteps, dt, face_bc, phi_l)
+    pairs = {"phi_laplace": phi_l, "E_laplace": E_l, "push_x": push["x"], "push_v": push["v"],
+             "push_tet": push["tet"], "push_lost": push["lost"], "push_rho": push["rho"],
+             "push_substeps": push["substeps"], "phi_charge": phi_q, "E_charge": E_q, "cyc_x": cyc["x"],
+             "cyc_v": cyc["v"], "cyc_id": cyc["id"], "cyc_status": cyc["status"], "cyc_rho": cyc["rho"],
+             "cyc_phi": cyc["phi"], "cyc_E": cyc["E"], "cyc_ledger": cyc["ledger"], "cyc_stats": cyc["stats"]}
+    for key, val in pairs.items():
+        assert np.array_equal(np.asarray(val), g[key], equal_nan=True), key
+
+
+def test_config0_fixture_is_the_reference(ref):
+    """tests/golden/config0_ref.npz is the reference's push of the first benchmark
+    configuration's subsample in the reference's LSQ field of the Laplace potential, reproduced
+    exactly here from the recorded inputs."""
+    import os
+
+    from golden.make_golden import CONFIG0_STRIDE, config0_laplace, make_config0_inputs, subsample
+
+    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "config0_ref.npz"))
+    mesh, sp, parts, dt = make_config0_inputs()
+    o = O.Oracle(fast_locate=True)
+    try:
+        _, phi = config0_laplace(o, mesh)
+    finally:
+        o.close()
+    E = ref.lsq(mesh, phi)
+    push = ref.push(mesh, E, subsample(parts, CONFIG0_STRIDE), sp, dt)
+    nz = np.nonzero(push["rho"])[0]
+    assert g["phi_sum"] == np.sum(phi) and g["E_abs_sum"] == np.sum(np.abs(E))
+    for key in ("x", "v", "tet", "lost", "substeps"):
+        assert np.array_equal(np.asarray(push[key]), g["push_" + key]), key
+    assert np.array_equal(nz, g["rho_nodes"]) and np.array_equal(push["rho"][nz], g["rho_vals"])
