@@ -423,3 +423,28 @@ def test_config0_fixture_is_the_reference(ref):
     for key in ("x", "v", "tet", "lost", "substeps"):
         assert np.array_equal(np.asarray(push[key]), g["push_" + key]), key
     assert np.array_equal(nz, g["rho_nodes"]) and np.array_equal(push["rho"][nz], g["rho_vals"])
+
+
+def test_push_edge_cases_match_reference(orc, ref):
+    """Edge inputs through both the oracle and the reference's CrossTetrahedron: no particles
+    (no charge, no sub-steps), a particle outside the mesh with no location hint (lost at once,
+    state untouched, nothing deposited), and one exactly on a shared vertex of the box."""
+    mesh = O.kuhn_box((3, 3, 3), 0.05)
+    sp = O.plasma_species(1e10, 1.0, 1.0, 0.05, 2)
+    E = np.zeros((mesh.N, 3))
+
+    def parts(x, v, s, t):
+        return dict(x=np.asarray(x, float).reshape(-1, 3), v=np.asarray(v, float).reshape(-1, 3),
+                    species=np.asarray(s, np.int32), tet=np.asarray(t, np.int32),
+                    id=np.arange(len(s), dtype=np.int64))
+
+    cases = [parts([], [], [], []),
+             parts([[0.2, 0.05, 0.05]], [[1.0, 0.0, 0.0]], [1], [-1]),
+             parts([[0.05, 0.05, 0.05]], [[10.0, -5.0, 2.0]], [0], [-1])]
+    for p in cases:
+        a, b = orc.push(mesh, E, p, sp, 2e-8), ref.push(mesh, E, p, sp, 2e-8)
+        assert np.array_equal(a["lost"], b["lost"]) and np.array_equal(a["tet"], b["tet"])
+        assert np.array_equal(a["x"], b["x"]) and np.array_equal(a["v"], b["v"])
+        assert np.abs(a["rho"] - b["rho"]).max(initial=0.0) <= 1e-12 * np.abs(b["rho"]).max(initial=1e-300)
+        assert a["substeps"] == b["substeps"]
+    assert np.abs(orc.push(mesh, E, cases[0], sp, 2e-8)["rho"]).max() == 0.0
