@@ -448,3 +448,20 @@ def test_push_edge_cases_match_reference(orc, ref):
         assert np.abs(a["rho"] - b["rho"]).max(initial=0.0) <= 1e-12 * np.abs(b["rho"]).max(initial=1e-300)
         assert a["substeps"] == b["substeps"]
     assert np.abs(orc.push(mesh, E, cases[0], sp, 2e-8)["rho"]).max() == 0.0
+
+
+@pytest.mark.parametrize("cells", [(1, 1, 1), (2, 2, 2), (2, 1, 3)])
+def test_poisson_degenerate_meshes_match_reference(orc, ref, cells):
+    """Meshes with no unknown (every node Dirichlet) or a single one: the oracle's solve and LSQ
+    field against the reference's PoissonSolver and PICCycle field, with random boundary values
+    and charge."""
+    mesh = O.kuhn_box(cells, 0.05, bias=0.0)
+    rng = np.random.default_rng(1)
+    phi_bc = mesh.phi_bc + rng.normal(0.0, 1.0, mesh.N) * (mesh.dirichlet == 1)
+    rho = rng.normal(0.0, 1e-12, mesh.N)
+    A = orc.assemble(mesh)
+    phi, _, _ = orc.poisson(mesh, A, rho, phi_bc)
+    E = orc.lsq(mesh, A, phi)
+    ref_phi, ref_E = ref.poisson(mesh, rho, phi_bc)
+    assert np.abs(phi - ref_phi).max() <= 1e-12 * np.abs(ref_phi).max()
+    assert rel_err(E, ref_E) < 1e-12
